@@ -1,0 +1,41 @@
+"""diffsoup_b200: B200-native differentiable triangle-soup rasterize-and-shade.
+
+Drop-in for the rasterize/shade API of kenji-tojo/diffsoup
+(python/diffsoup/__init__.py:11-25): the same public names with the same
+signatures and tensor layouts, backed by hand-written sm_100a kernels in
+libdiffsoup_b200.so.  `step` adds the batched, graph-captured training step.
+"""
+
+from __future__ import annotations
+
+from . import _core
+from ._core import __version__
+from .rasterize import (
+    count_triangle_ids,
+    edge_grad,
+    encode_view_dir,
+    encode_view_dir_sh2,
+    opacity_aux_loss,
+)
+from .multires import (
+    ColorMLP,
+    accumulate_to_level,
+    build_multires_triangle_color,
+    feats_at_level,
+    multires_triangle_color,
+    rasterize_multires_triangle_alpha,
+)
+
+__all__ = [
+    "ColorMLP",
+    "accumulate_to_level",
+    "build_multires_triangle_color",
+    "count_triangle_ids",
+    "edge_grad",
+    "encode_view_dir",
+    "encode_view_dir_sh2",
+    "feats_at_level",
+    "multires_triangle_color",
+    "opacity_aux_loss",
+    "rasterize_multires_triangle_alpha",
+]

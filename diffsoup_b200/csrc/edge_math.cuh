@@ -1,0 +1,217 @@
+// diffsoup_b200/csrc/edge_math.cuh -- per-pixel edge-gradient estimator and
+// per-fragment opacity auxiliary gradient (kenji-tojo/diffsoup
+// src/cuda/rasterize.cu:489-971), shared by the operator kernels and the
+// fused training step.
+#pragma once
+
+#include "geometry.cuh"
+
+namespace dsb {
+
+// Segment (x0,y0)-(x1,y1) against (x2,y2)-(x3,y3) (rasterize.cu:493-544).
+__device__ __forceinline__ bool segment_intersect2d(float x0, float y0, float x1, float y1, float x2, float y2,
+                                                    float x3, float y3, float& ix, float& iy) {
+    const float eps = 1e-7f;
+    const float rx = x1 - x0, ry = y1 - y0, sx = x3 - x2, sy = y3 - y2;
+    const float denom = rx * sy - ry * sx;
+    const float qpx = x2 - x0, qpy = y2 - y0;
+    if (fabsf(denom) <= eps) {
+        const float cr = qpx * ry - qpy * rx;
+        if (fabsf(cr) > eps) return false;
+        const float rr = rx * rx + ry * ry;
+        if (rr < eps) return false;
+        const float t0 = ((x2 - x0) * rx + (y2 - y0) * ry) / rr;
+        const float t1 = ((x3 - x0) * rx + (y3 - y0) * ry) / rr;
+        const float tmin = fminf(t0, t1), tmax = fmaxf(t0, t1);
+        if (tmax < -eps || tmin > 1.f + eps) return false;
+        const float t = fmaxf(0.f, fminf(1.f, 0.5f * (fmaxf(0.f, tmin) + fminf(1.f, tmax))));
+        ix = x0 + t * rx; iy = y0 + t * ry;
+        return true;
+    }
+    const float t = (qpx * sy - qpy * sx) / denom;
+    const float u = (qpx * ry - qpy * rx) / denom;
+    if (t < -eps || t > 1.f + eps || u < -eps || u > 1.f + eps) return false;
+    ix = x0 + t * rx; iy = y0 + t * ry;
+    return true;
+}
+
+// Which triangle edge the pixel-pair segment crosses, and the perspective-
+// correct edge weights at the crossing (rasterize.cu:546-604).
+__device__ __forceinline__ bool find_edge_intersection(const float4 P[3], float x0, float y0, float x1, float y1,
+                                                       int& i0, int& i1, float& s0, float& s1) {
+    float rx[3], ry[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { rx[k] = P[k].x / P[k].w; ry[k] = P[k].y / P[k].w; }
+    float ix = 0.f, iy = 0.f;
+    if (segment_intersect2d(x0, y0, x1, y1, rx[0], ry[0], rx[1], ry[1], ix, iy)) { i0 = 0; i1 = 1; }
+    else if (segment_intersect2d(x0, y0, x1, y1, rx[1], ry[1], rx[2], ry[2], ix, iy)) { i0 = 1; i1 = 2; }
+    else if (segment_intersect2d(x0, y0, x1, y1, rx[2], ry[2], rx[0], ry[0], ix, iy)) { i0 = 2; i1 = 0; }
+    else return false;
+    const float4 A = P[i0], Bv = P[i1];
+    const float dx = Bv.x - A.x, dy = Bv.y - A.y, dw = Bv.w - A.w;
+    const float ax = A.x - ix * A.w, ay = A.y - iy * A.w;
+    const float bx = dx - ix * dw, by = dy - iy * dw;
+    const float den = bx * bx + by * by;
+    const float t = den != 0.f ? -(ax * bx + ay * by) / den : 0.5f;
+    s0 = 1.f - t; s1 = t;
+    return true;
+}
+
+// Unit normal of the triangle in NDC (rasterize.cu:608-633).
+__device__ __forceinline__ bool tri_normal_ndc(const float4 P[3], float n[3]) {
+    if (fabsf(P[0].w) < 1e-30f || fabsf(P[1].w) < 1e-30f || fabsf(P[2].w) < 1e-30f) return false;
+    const float X0 = P[0].x / P[0].w, Y0 = P[0].y / P[0].w, Z0 = P[0].z / P[0].w;
+    const float X1 = P[1].x / P[1].w, Y1 = P[1].y / P[1].w, Z1 = P[1].z / P[1].w;
+    const float X2 = P[2].x / P[2].w, Y2 = P[2].y / P[2].w, Z2 = P[2].z / P[2].w;
+    const float e1x = X1 - X0, e1y = Y1 - Y0, e1z = Z1 - Z0;
+    const float e2x = X2 - X0, e2y = Y2 - Y0, e2z = Z2 - Z0;
+    const float nx = e1y * e2z - e1z * e2y, ny = e1z * e2x - e1x * e2z, nz = e1x * e2y - e1y * e2x;
+    const float l2 = nx * nx + ny * ny + nz * nz;
+    if (!(l2 > 0.f)) return false;
+    const float il = rsqrtf(l2);
+    n[0] = nx * il; n[1] = ny * il; n[2] = nz * il;
+    return true;
+}
+
+// 2D boundary displacement of an intersection line (rasterize.cu:636-651).
+__device__ __forceinline__ void db_dp_2d(float nvx, float nvy, float nfx, float nfy, float& dbx, float& dby) {
+    float il = rsqrtf(fmaxf(1e-30f, nvx * nvx + nvy * nvy)); nvx *= il; nvy *= il;
+    il = rsqrtf(fmaxf(1e-30f, nfx * nfx + nfy * nfy)); nfx *= il; nfy *= il;
+    const float bx = -nfy, by = nfx;
+    const float den = bx * nvx + by * nvy;
+    const float s = fabsf(den) > 1e-12f ? bx / den : 0.f;
+    dbx = s * nvx; dby = s * nvy;
+}
+
+struct EdgeAccum {
+    float g[12];
+    bool any;
+};
+
+// Interior / implicit-edge contribution at the pixel-pair midpoint
+// (rasterize.cu:727-746, :811-835, :843-863).
+__device__ __forceinline__ void add_mid_contrib(float mx, float my, const float4 P[3], float gx, float gy, float gz,
+                                                bool use_z, EdgeAccum& a) {
+    float b0, b1, cz, cw;
+    if (!intersect_triangle(my, mx, P[0], P[1], P[2], b0, b1, cz, cw)) return;
+    const float b2 = 1.f - b0 - b1;
+    const float cx = mx * cw, cy = my * cw;
+    const float iw = 1.f / cw, iw2 = iw * iw;
+    const float gsum = use_z ? gx * cx + gy * cy + gz * cz : gx * cx + gy * cy;
+    const float bb[3] = {b0, b1, b2};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        a.g[k * 4 + 0] += bb[k] * gx * iw;
+        a.g[k * 4 + 1] += bb[k] * gy * iw;
+        if (use_z) a.g[k * 4 + 2] += bb[k] * gz * iw;
+        a.g[k * 4 + 3] += -bb[k] * gsum * iw2;
+    }
+    a.any = true;
+}
+
+// Edge-gradient estimator of one pixel (rasterize.cu:663-892).  Pixel
+// buffers are addressed as base + y*W + x with `base` the view's first pixel;
+// P0 holds the view's clip positions.  Returns the pixel's triangle (or -1)
+// and its clip-space vertex gradients in acc.g[vertex*4 + xyzw].
+__device__ __forceinline__ int edge_grad_pixel(int b, int y0, int x0, int H, int W, int C,
+                                               const float* __restrict__ color, const float* __restrict__ grad_color,
+                                               const float* __restrict__ rast, const float* __restrict__ posb,
+                                               const int* __restrict__ tri, int64_t base, EdgeAccum& acc) {
+    (void)b;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) acc.g[k] = 0.f;
+    acc.any = false;
+    const int64_t pix0 = base + (int64_t)y0 * W + x0;
+    const float4 r0 = reinterpret_cast<const float4*>(rast)[pix0];
+    const int it0 = (int)r0.w - 1;
+    if (it0 < 0) return -1;
+    const float depth0 = r0.z;
+    const float nx0 = -1.f + 2.f * ((float)x0 + 0.5f) / (float)W;
+    const float ny0 = -1.f + 2.f * ((float)y0 + 0.5f) / (float)H;
+    float4 P0[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) P0[k] = load_vertex(posb, __ldg(tri + it0 * 3 + k));
+    const float* c0 = color + pix0 * C;
+    const float* g0 = grad_color + pix0 * C;
+    const int DY[4] = {0, 0, -1, 1}, DX[4] = {1, -1, 0, 0};
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const int y1 = y0 + DY[e], x1 = x0 + DX[e];
+        if (y1 < 0 || y1 >= H || x1 < 0 || x1 >= W) continue;
+        const int64_t pix1 = base + (int64_t)y1 * W + x1;
+        const float4 r1 = reinterpret_cast<const float4*>(rast)[pix1];
+        const float depth1 = r1.z;
+        const int it1 = (int)r1.w - 1;
+        const float* c1 = color + pix1 * C;
+        const float* g1 = grad_color + pix1 * C;
+        float adj = 0.f;
+        for (int i = 0; i < C; ++i) adj += 0.5f * (g0[i] + g1[i]) * (c0[i] - c1[i]);
+        if (adj == 0.f) continue;
+        const float gx = adj * (float)DX[e] * (float)W / 2.f;
+        const float gy = adj * (float)DY[e] * (float)H / 2.f;
+        const float nx1 = -1.f + 2.f * ((float)x1 + 0.5f) / (float)W;
+        const float ny1 = -1.f + 2.f * ((float)y1 + 0.5f) / (float)H;
+        const float mx = 0.5f * (nx0 + nx1), my = 0.5f * (ny0 + ny1);
+        if (it1 == it0) {  // not an edge
+            add_mid_contrib(mx, my, P0, gx, gy, 0.f, false, acc);
+            continue;
+        }
+        float tb0, tb1, cz1, cw1;
+        if (intersect_triangle(ny1, nx1, P0[0], P0[1], P0[2], tb0, tb1, cz1, cw1)) {
+            // implicit edge: triangle intersection or opacity edge
+            const float d1_it0 = cz1 / cw1;
+            if (it1 >= 0 && depth1 < d1_it0) {
+                float4 P1[3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) P1[k] = load_vertex(posb, __ldg(tri + it1 * 3 + k));
+                float cz0, cw0;
+                if (intersect_triangle(ny0, nx0, P1[0], P1[1], P1[2], tb0, tb1, cz0, cw0)) {
+                    const float d0_it1 = cz0 / cw0;
+                    if (depth0 < d0_it1) {  // triangle intersection
+                        float nv[3], nf[3];
+                        if (tri_normal_ndc(P0, nv) && tri_normal_ndc(P1, nf)) {
+                            float gxn = 0.f, gyn = 0.f, gzn = 0.f;
+                            if (DX[e] != 0) {
+                                float dbx, dbz;
+                                db_dp_2d(nv[0], nv[2], nf[0], nf[2], dbx, dbz);
+                                gxn = gx * dbx; gzn = gx * dbz;
+                            } else {
+                                float dby, dbz;
+                                db_dp_2d(nv[1], nv[2], nf[1], nf[2], dby, dbz);
+                                gyn = gy * dby; gzn = gy * dbz;
+                            }
+                            add_mid_contrib(mx, my, P0, gxn, gyn, gzn, true, acc);
+                        }
+                    }
+                }
+            } else if (it1 < 0 || depth0 < depth1) {  // active opacity edge
+                add_mid_contrib(mx, my, P0, gx, gy, 0.f, false, acc);
+            }
+        } else if (it1 < 0 || depth0 < depth1) {  // active geometric edge
+            int i0, i1;
+            float s0, s1;
+            if (find_edge_intersection(P0, nx0, ny0, nx1, ny1, i0, i1, s0, s1)) {
+                const float cx = s0 * P0[i0].x + s1 * P0[i1].x;
+                const float cy = s0 * P0[i0].y + s1 * P0[i1].y;
+                const float cw = s0 * P0[i0].w + s1 * P0[i1].w;
+                const float iw = 1.f / cw, iw2 = iw * iw;
+                const float gsum = gx * cx + gy * cy;
+                acc.g[i0 * 4 + 0] += s0 * gx * iw; acc.g[i1 * 4 + 0] += s1 * gx * iw;
+                acc.g[i0 * 4 + 1] += s0 * gy * iw; acc.g[i1 * 4 + 1] += s1 * gy * iw;
+                acc.g[i0 * 4 + 3] += -s0 * gsum * iw2; acc.g[i1 * 4 + 3] += -s1 * gsum * iw2;
+                acc.any = true;
+            }
+        }
+    }
+    return it0;
+}
+
+// Per-fragment gradient of the opacity auxiliary objective
+// (rasterize.cu:955-970): +L/alpha for the visible fragment, -L/(1-alpha)
+// for the others in front of the surface or on empty pixels.
+__device__ __forceinline__ float aux_alpha_grad(float loss, float alpha, bool visible) {
+    const float eps = 1e-5f;
+    return visible ? loss / fmaxf(alpha, eps) : -(loss / fmaxf(1.f - alpha, eps));
+}
+
+}  // namespace dsb

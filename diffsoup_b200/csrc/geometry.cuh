@@ -1,0 +1,196 @@
+// diffsoup_b200/csrc/geometry.cuh -- per-triangle and per-pixel device math
+// shared by the fragment, tiled and shading kernels.  Each function follows
+// the reference's arithmetic (kenji-tojo/diffsoup, cited file:line) so that
+// triangle IDs, barycentrics and depths match it bit for bit.
+#pragma once
+
+#include "common.cuh"
+
+namespace dsb {
+
+// Outcode against the six clip planes (rasterize.cu:10-16).
+__device__ __forceinline__ int outcode4(float x, float y, float z, float w) {
+    int c = 0;
+    c |= (x < -w) ? 1 : 0;  c |= (x > w) ? 2 : 0;
+    c |= (y < -w) ? 4 : 0;  c |= (y > w) ? 8 : 0;
+    c |= (z < -w) ? 16 : 0; c |= (z > w) ? 32 : 0;
+    return c;
+}
+
+// NDC bounds with non-finite guards and clamping (rasterize.cu:18-41).
+__device__ __forceinline__ void accum_ndc4(float x, float y, float z, float w, float& xmin, float& ymin,
+                                           float& zmin, float& xmax, float& ymax, float& zmax) {
+    const float invw = __fdiv_rn(1.f, w);
+    float nx = __fmul_rn(x, invw), ny = __fmul_rn(y, invw), nz = __fmul_rn(z, invw);
+    if (!isfinite(nx)) nx = nx > 0.f ? 1.f : -1.f;
+    if (!isfinite(ny)) ny = ny > 0.f ? 1.f : -1.f;
+    if (!isfinite(nz)) nz = nz > 0.f ? 1.f : -1.f;
+    nx = fminf(1.f, fmaxf(-1.f, nx));
+    ny = fminf(1.f, fmaxf(-1.f, ny));
+    nz = fminf(1.f, fmaxf(-1.f, nz));
+    xmin = fminf(xmin, nx); xmax = fmaxf(xmax, nx);
+    ymin = fminf(ymin, ny); ymax = fmaxf(ymax, ny);
+    zmin = fminf(zmin, nz); zmax = fmaxf(zmax, nz);
+}
+
+// Screen rectangle of a clip-space triangle (rasterize.cu:76-136):
+// returns false when culled; otherwise rows [h0, h0+hlen) and columns
+// [w0, w0+wlen) bound every pixel the triangle can cover.
+__device__ __forceinline__ bool triangle_rect(int H, int W, float4 p0, float4 p1, float4 p2, int& h0, int& hlen,
+                                              int& w0, int& wlen) {
+    h0 = hlen = w0 = wlen = 0;
+    if (!(p0.w > 0.f && p1.w > 0.f && p2.w > 0.f)) return false;
+    const int c0 = outcode4(p0.x, p0.y, p0.z, p0.w);
+    const int c1 = outcode4(p1.x, p1.y, p1.z, p1.w);
+    const int c2 = outcode4(p2.x, p2.y, p2.z, p2.w);
+    if ((c0 & c1 & c2) != 0) return false;
+    float xmin = 1.f, ymin = 1.f, zmin = 1.f, xmax = -1.f, ymax = -1.f, zmax = -1.f;
+    accum_ndc4(p0.x, p0.y, p0.z, p0.w, xmin, ymin, zmin, xmax, ymax, zmax);
+    accum_ndc4(p1.x, p1.y, p1.z, p1.w, xmin, ymin, zmin, xmax, ymax, zmax);
+    accum_ndc4(p2.x, p2.y, p2.z, p2.w, xmin, ymin, zmin, xmax, ymax, zmax);
+    if (zmax < -1.f || zmin > 1.f) return false;
+    const float fH = (float)H, fW = (float)W;
+    float x0f = __fmul_rn(__fmul_rn(0.5f, __fadd_rn(xmin, 1.f)), fW);
+    float x1f = __fmul_rn(__fmul_rn(0.5f, __fadd_rn(xmax, 1.f)), fW);
+    float y0f = __fmul_rn(__fmul_rn(0.5f, __fadd_rn(ymin, 1.f)), fH);
+    float y1f = __fmul_rn(__fmul_rn(0.5f, __fadd_rn(ymax, 1.f)), fH);
+    if (x0f > x1f) { const float t = x0f; x0f = x1f; x1f = t; }
+    if (y0f > y1f) { const float t = y0f; y0f = y1f; y1f = t; }
+    const int a0 = max((int)floorf(x0f), 0);
+    const int a1 = min((int)floorf(x1f), W - 1) + 1;
+    const int b0 = max((int)floorf(y0f), 0);
+    const int b1 = min((int)floorf(y1f), H - 1) + 1;
+    const int wl = max(a1 - a0, 0), hl = max(b1 - b0, 0);
+    if (wl == 0 || hl == 0) return false;
+    h0 = b0; hlen = hl; w0 = a0; wlen = wl;
+    return true;
+}
+
+// Homogeneous 2D edge-function coverage test (rasterize.cu:170-206).
+// Writes barycentrics (b0, b1) and the interpolated clip z and w.
+__device__ __forceinline__ bool intersect_triangle(float ndc_y, float ndc_x, float4 p0, float4 p1, float4 p2,
+                                                   float& b0, float& b1, float& z, float& w) {
+    const float q0x = sub_mul(p0.x, ndc_x, p0.w), q0y = sub_mul(p0.y, ndc_y, p0.w);
+    const float q1x = sub_mul(p1.x, ndc_x, p1.w), q1y = sub_mul(p1.y, ndc_y, p1.w);
+    const float q2x = sub_mul(p2.x, ndc_x, p2.w), q2y = sub_mul(p2.y, ndc_y, p2.w);
+    const float A0 = cross2(q1x, q2y, q1y, q2x);
+    const float A1 = cross2(q2x, q0y, q2y, q0x);
+    const float A2 = cross2(q0x, q1y, q0y, q1x);
+    const float A = __fadd_rn(__fadd_rn(A0, A1), A2);
+    if (A == 0.f) return false;
+    const float invA = __fdiv_rn(1.f, A);
+    b0 = __fmul_rn(A0, invA);
+    b1 = __fmul_rn(A1, invA);
+    const float b2 = __fsub_rn(__fsub_rn(1.f, b0), b1);
+    z = dot3_z(b0, p0.z, b1, p1.z, b2, p2.z);
+    w = dot3_w(b0, p0.w, b1, p1.w, b2, p2.w);
+    return b0 >= 0.f && b1 >= 0.f && __fadd_rn(b0, b1) <= 1.f;
+}
+
+// Fragment test of compute_fragments (rasterize.cu:257-268): covered and
+// depth = z / w within [-1, 1].
+__device__ __forceinline__ bool fragment_at(float ndc_y, float ndc_x, float4 p0, float4 p1, float4 p2, float& b0,
+                                            float& b1, float& depth) {
+    float z, w;
+    if (!intersect_triangle(ndc_y, ndc_x, p0, p1, p2, b0, b1, z, w)) return false;
+    depth = __fdiv_rn(z, w);
+    return depth >= -1.f && depth <= 1.f;
+}
+
+__device__ __forceinline__ float4 load_vertex(const float* pos, int v) {
+    return __ldg(reinterpret_cast<const float4*>(pos) + v);
+}
+
+// ---------------------------------------------------------------------------
+// Multi-resolution barycentric lattice (multires.cu:10-68, multires.cuh:8-20)
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ uint32_t feats_at_level(uint32_t level) {
+    return level == 0u ? 3u : (((1u << (level - 1u)) + 1u) * ((1u << level) + 1u));
+}
+
+__host__ __device__ __forceinline__ uint32_t total_feats(uint32_t lo, uint32_t hi) {
+    uint32_t s = 0;
+    for (uint32_t l = lo; l <= hi; ++l) s += feats_at_level(l);
+    return s;
+}
+
+// Sample indices and weights of the lattice cell containing (b0, b1).
+__device__ __forceinline__ void lattice_cell(float b0, float b1, uint32_t level, uint32_t idx[3], float w[3]) {
+    const uint32_t res = 1u << level;
+    const float res_f = (float)res;
+    float b0l = __fmul_rn(b0, res_f), b1l = __fmul_rn(b1, res_f);
+    const uint32_t x = min((uint32_t)floorf(b0l), res - 1);
+    const uint32_t y = min((uint32_t)floorf(b1l), res - 1 - x);
+    b0l = __fsub_rn(b0l, (float)x);
+    b1l = __fsub_rn(b1l, (float)y);
+    const bool flip = __fadd_rn(b0l, b1l) > 1.f;
+    const uint32_t fu = (uint32_t)flip;
+    const uint32_t x0 = x + 1, y0 = y, x1 = x, y1 = y + 1;
+    const uint32_t x2 = x + fu;
+    const uint32_t y2 = min(y + fu, res - x2);
+    idx[0] = (x0 + y0) * (x0 + y0 + 1) / 2 + y0;
+    idx[1] = (x1 + y1) * (x1 + y1 + 1) / 2 + y1;
+    idx[2] = (x2 + y2) * (x2 + y2 + 1) / 2 + y2;
+    // Weights of multires.cu:50-53; flip is 0 or 1, so these are exact selects.
+    w[0] = flip ? __fsub_rn(1.f, b1l) : b0l;
+    w[1] = flip ? __fsub_rn(1.f, b0l) : b1l;
+    w[2] = __fsub_rn(__fsub_rn(1.f, w[0]), w[1]);
+}
+
+// Scalar lattice interpolation over levels [lo, hi] of one triangle's samples.
+__device__ __forceinline__ float interp_scalar(float b0, float b1, uint32_t lo, uint32_t hi, const float* src) {
+    float acc = 0.f;
+    uint32_t off = 0;
+    for (uint32_t l = lo; l <= hi; ++l) {
+        uint32_t idx[3]; float w[3];
+        lattice_cell(b0, b1, l, idx, w);
+        acc = madd(acc, w[0], __ldg(src + off + idx[0]));
+        acc = madd(acc, w[1], __ldg(src + off + idx[1]));
+        acc = madd(acc, w[2], __ldg(src + off + idx[2]));
+        off += feats_at_level(l);
+    }
+    return acc;
+}
+
+// Triangular-number inverse of multires.cu:314-325.
+__device__ __forceinline__ void index_to_xy(uint32_t idx, uint32_t& x, uint32_t& y) {
+    const float fi = (float)idx;
+    const uint32_t n = (uint32_t)floorf(__fmul_rn(__fsub_rn(__fsqrt_rn(__fadd_rn(__fmul_rn(8.f, fi), 1.f)), 1.f), 0.5f));
+    const uint32_t Tn = (n * (n + 1u)) >> 1;
+    y = idx - Tn;
+    x = n - y;
+}
+
+// ---------------------------------------------------------------------------
+// View direction from the inverse MVP (encoding.cu:9-53), unit vector from the
+// far plane towards the camera.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void view_direction(float ndc_x, float ndc_y, const float* M, float d[3]) {
+    float wn[3], wf[3];
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+        const float nz = s == 0 ? -1.f : 1.f;
+        float c[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) c[r] = M[r * 4 + 0] * ndc_x + M[r * 4 + 1] * ndc_y + M[r * 4 + 2] * nz + M[r * 4 + 3];
+        const float iw = 1.f / c[3];
+        float* o = s == 0 ? wn : wf;
+        o[0] = c[0] * iw; o[1] = c[1] * iw; o[2] = c[2] * iw;
+    }
+    const float dx = wn[0] - wf[0], dy = wn[1] - wf[1], dz = wn[2] - wf[2];
+    const float il = rsqrtf(dx * dx + dy * dy + dz * dz);
+    d[0] = dx * il; d[1] = dy * il; d[2] = dz * il;
+}
+
+// Real spherical-harmonic basis up to degree 2 (encoding.cu:55-85).
+__device__ __forceinline__ void sh2_basis(float x, float y, float z, float* sh) {
+    const float C0 = 0.28209479177387814f, C1 = 0.4886025119029199f;
+    const float C2a = 1.0925484305920792f, C2b = 0.31539156525252005f, C2c = 0.5462742152960396f;
+    sh[0] = C0;
+    sh[1] = -C1 * y; sh[2] = C1 * z; sh[3] = -C1 * x;
+    const float xx = x * x, yy = y * y, zz = z * z;
+    sh[4] = C2a * (x * y); sh[5] = -C2a * (y * z); sh[6] = C2b * (2.f * zz - xx - yy);
+    sh[7] = -C2a * (x * z); sh[8] = C2c * (xx - yy);
+}
+
+}  // namespace dsb

@@ -1,0 +1,199 @@
+/*
+ * diffsoup_b200.h -- C ABI of libdiffsoup_b200.so, the B200 (sm_100a)
+ * implementation of DiffSoup's differentiable rasterize-and-shade path.
+ *
+ * Conventions
+ *  - Every entry point returns DS_OK (0) or an error status; ds_last_error()
+ *    returns the message of the last failure on the calling thread.  No entry
+ *    point exits the process.
+ *  - Pointers are device pointers unless the parameter name ends in _host.
+ *    Tensors are dense, C-contiguous, with the layouts of the reference
+ *    (kenji-tojo/diffsoup python/diffsoup): pos [B,V,4] f32 clip space,
+ *    tri [T,3] i32, rast [B,H,W,4] f32 = (b0, b1, z_ndc, tri_id+1), 0 = empty.
+ *  - Work is enqueued on `stream` (a cudaStream_t).  Entry points documented
+ *    as "host-synchronising" read a count back, like the reference's launcher
+ *    does; all others never block the host and can be captured in a CUDA graph.
+ *  - Outputs that accumulate must be zeroed by the caller, as in the reference
+ *    (python/diffsoup/rasterize.py:171,177,271, multires.py:238,305).
+ *  - Temporary device memory comes from the caller as (workspace, bytes);
+ *    the matching *_workspace_size() function gives the required size.
+ */
+#ifndef DIFFSOUP_B200_H
+#define DIFFSOUP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void* ds_stream_t; /* cudaStream_t */
+
+enum {
+    DS_OK = 0,
+    DS_ERR_ARG = 1,         /* shape / argument mismatch (reference: std::runtime_error) */
+    DS_ERR_CUDA = 2,        /* CUDA runtime error (reference: CUDA_CHECK -> exit(1)) */
+    DS_ERR_WORKSPACE = 3,   /* workspace smaller than *_workspace_size() */
+    DS_ERR_OVERFLOW = 4,    /* a count exceeds the 32-bit range of the reference's layout */
+};
+
+/* Bits of the device status word written by the tiled kernels. */
+enum {
+    DS_STATUS_LIST_OVERFLOW = 1, /* tile lists exceeded capacity; affected tiles ran the exhaustive path */
+};
+
+const char* ds_last_error(void);
+const char* ds_version(void);
+
+/* ===================================================================== */
+/*  Reference operator mirror: one entry point per `_core` function.      */
+/* ===================================================================== */
+
+/* replaces _core.compute_triangle_rects (src/main.cpp:30-48,
+ * src/cuda/rasterize.cu:43-168).  rects [B*T,4] = (h0, h_len, w0, w_len),
+ * prefix [B*T] inclusive sum of h_len*w_len.  Host-synchronising: writes the
+ * total (the reference's return value) to *num_frags_host. */
+size_t ds_compute_triangle_rects_workspace(int B, int T);
+int ds_compute_triangle_rects(int H, int W, int B, int V, const float* pos, int T, const int* tri, int* rects,
+                              int* prefix, int* num_frags_host, void* workspace, size_t workspace_bytes,
+                              ds_stream_t stream);
+
+/* replaces _core.compute_fragments (src/main.cpp:50-76, rasterize.cu:208-305).
+ * frag_pix [num_frags,3] must be pre-filled with -1 (rasterize.py:69). */
+int ds_compute_fragments(int H, int W, int B, int V, const float* pos, int T, const int* tri, const int* prefix,
+                         const int* rects, int num_frags, int* frag_pix, float* frag_attrs, ds_stream_t stream);
+
+/* replaces _core.filter_valid_fragments (src/main.cpp:96-108,
+ * rasterize.cu:402-487).  Order preserving (the reference's block order is
+ * not).  Host-synchronising: writes the valid count to *count_host. */
+size_t ds_filter_valid_fragments_workspace(int num_frags);
+int ds_filter_valid_fragments(int num_frags, const int* frag_pix, const float* frag_attrs, int* frag_pix_out,
+                              float* frag_attrs_out, int* count_host, void* workspace, size_t workspace_bytes,
+                              ds_stream_t stream);
+
+/* replaces _core.depth_test (src/main.cpp:78-94, rasterize.cu:307-400).
+ * Writes the winning fragment of every covered pixel into rast (others are
+ * left untouched; the caller zeroes rast). */
+size_t ds_depth_test_workspace(int B, int H, int W);
+int ds_depth_test(int B, int H, int W, int num_frags, const int* frag_pix, const float* frag_attrs,
+                  const float* frag_alpha, const float* alpha_thresh, float* rast, void* workspace,
+                  size_t workspace_bytes, ds_stream_t stream);
+
+/* replaces _core.backward_edge_grad (src/main.cpp:112-130, rasterize.cu:653-921).
+ * grad_pos [B,V,4] accumulates. */
+int ds_backward_edge_grad(int B, int H, int W, int C, const float* color, const float* grad_color,
+                          const float* rast, int V, const float* pos, float* grad_pos, const int* tri,
+                          ds_stream_t stream);
+
+/* replaces _core.backward_opacity_aux_loss (src/main.cpp:134-154,
+ * rasterize.cu:923-992).  grad_frag_alpha accumulates. */
+int ds_backward_opacity_aux_loss(int B, int H, int W, int C, const float* color, const float* target,
+                                 const float* rast, int num_frags, const int* frag_pix, const float* frag_attrs,
+                                 const float* frag_alpha, float* grad_frag_alpha, ds_stream_t stream);
+
+/* replaces _core.encode_view_dir_sh2 (src/main.cpp:158-170, encoding.cu:89-130). */
+int ds_encode_view_dir_sh2(int B, int H, int W, const float* rast, const float* inv_mvp, float* encoding,
+                           ds_stream_t stream);
+
+/* replaces _core.multires_triangle_alpha (src/main.cpp:174-191, multires.cu:130-176).
+ * S must equal the lattice size of levels [min_level, max_level]. */
+int ds_multires_triangle_alpha(int num_frags, const float* frag_attrs, int min_level, int max_level, int S,
+                               const float* alpha_src, float* frag_alpha, ds_stream_t stream);
+
+/* replaces _core.backward_multires_triangle_alpha (src/main.cpp:193-210,
+ * multires.cu:178-222).  grad_alpha_src [T,S] accumulates. */
+int ds_backward_multires_triangle_alpha(int num_frags, const float* frag_attrs, int min_level, int max_level,
+                                        int S, float* grad_alpha_src, const float* grad_frag_alpha,
+                                        ds_stream_t stream);
+
+/* replaces _core.multires_triangle_color (src/main.cpp:212-232, multires.cu:224-266).
+ * out [B,H,W,C] accumulates (the reference zero-initialises it). */
+int ds_multires_triangle_color(int B, int H, int W, const float* rast, int min_level, int max_level, int S, int C,
+                               const float* features, float* out, ds_stream_t stream);
+
+/* replaces _core.backward_multires_triangle_color (src/main.cpp:234-254,
+ * multires.cu:268-311).  grad_features [T,S,C] accumulates. */
+int ds_backward_multires_triangle_color(int B, int H, int W, const float* rast, int min_level, int max_level,
+                                        int S, int C, float* grad_features, const float* grad_out,
+                                        ds_stream_t stream);
+
+/* replaces _core.accumulate_to_level_forward (src/main.cpp:258-280,
+ * multires.cu:329-389).  out [T,S_target,C] is overwritten. */
+int ds_accumulate_to_level_forward(int T, int min_level, int max_level, int target_level, int S, int S_target,
+                                   int C, const float* features, float* out, ds_stream_t stream);
+
+/* replaces _core.accumulate_to_level_backward (src/main.cpp:282-304,
+ * multires.cu:393-450).  grad_features [T,S,C] accumulates. */
+int ds_accumulate_to_level_backward(int T, int min_level, int max_level, int target_level, int S, int S_target,
+                                    int C, float* grad_features, const float* grad_out, ds_stream_t stream);
+
+/* ===================================================================== */
+/*  B200 path: screen-tile binning, tiled rasterizer, tiled aux gradient  */
+/* ===================================================================== */
+
+/* One view of a batch.  Views may differ in resolution; their pixels are
+ * packed one after another in the rast/colour buffers (pix_offset), and their
+ * 16x16 screen tiles are numbered consecutively (tile_base). */
+typedef struct {
+    int32_t H, W;
+    int32_t tiles_x, tiles_y;
+    int64_t pix_offset; /* first pixel of this view in the packed buffers */
+    int32_t tile_base;  /* first tile of this view */
+    int32_t pad;
+} ds_view_desc;
+
+#define DS_TILE 16
+
+/* Fills desc_host[b] for views of the given heights and widths; returns the
+ * total tile count and writes the total pixel count to *num_pixels_host. */
+int ds_make_view_table(int B, const int* H_host, const int* W_host, ds_view_desc* desc_host,
+                       int64_t* num_pixels_host);
+
+/* Bytes of workspace for binning B*T triangles into num_tiles tiles with room
+ * for list_capacity (triangle, tile) entries. */
+size_t ds_tiles_workspace_size(int B, int T, int num_tiles, int64_t list_capacity);
+
+/* Screen-tile binning (replaces compute_triangle_rects + compute_fragments +
+ * filter_valid_fragments of rasterize.py:40-76): per (view, triangle) rect of
+ * rasterize.cu:43-137, then per-tile triangle lists.  Never host-synchronising;
+ * lists that would exceed list_capacity set DS_STATUS_LIST_OVERFLOW in
+ * *status (device int) and those tiles fall back to testing every triangle of
+ * their view, so results stay exact. */
+int ds_tiles_bin(int B, const ds_view_desc* views, int num_tiles, int V, const float* pos, int T, const int* tri,
+                 void* workspace, size_t workspace_bytes, int64_t list_capacity, int* status, ds_stream_t stream);
+
+/* Tiled forward rasterizer with stochastic opacity (replaces
+ * rasterize_multires_triangle_alpha, python/diffsoup/multires.py:52-102:
+ * multires_triangle_alpha + threshold + depth_test).  Uses the bins of the
+ * preceding ds_tiles_bin on the same workspace.  alpha_src [T,S] at `level`.
+ * Threshold: thr_mode 0 = constant thr_const (0.5 is stochastic=False);
+ * thr_mode 1 = Philox-4x32-10 uniform keyed by (seed, iteration, view,
+ * pixel, triangle) with rng = device uint64[2] {seed, iteration}.
+ * Writes every pixel of rast (zeros where empty). */
+int ds_tiles_rasterize(int B, const ds_view_desc* views, int num_tiles, int V, const float* pos, int T,
+                       const int* tri, int level, int S, const float* alpha_src, int thr_mode, float thr_const,
+                       const uint64_t* rng, float* rast, void* workspace, size_t workspace_bytes,
+                       int64_t list_capacity, ds_stream_t stream);
+
+/* Tiled opacity auxiliary gradient (replaces the forward of
+ * _OpacityAuxLossFn, python/diffsoup/rasterize.py:147-190: fragments +
+ * multires_triangle_alpha + backward_opacity_aux_loss +
+ * backward_multires_triangle_alpha).  Recomputes the fragments tile by tile
+ * from the bins.  color/target [pixels, C]; grad_alpha_src [T,S] accumulates
+ * scale * dL/dalpha_src. */
+int ds_tiles_opacity_aux(int B, const ds_view_desc* views, int num_tiles, int V, const float* pos, int T,
+                         const int* tri, int level, int S, const float* alpha_src, int C, const float* color,
+                         const float* target, const float* rast, float scale, float* grad_alpha_src,
+                         void* workspace, size_t workspace_bytes, int64_t list_capacity, ds_stream_t stream);
+
+/* 3-D view direction per covered pixel (compute_view_direction of
+ * src/cuda/encoding.cu:28-53, which the reference does not export): enc [B,H,W,3]. */
+int ds_encode_view_dir(int B, int H, int W, const float* rast, const float* inv_mvp, float* encoding,
+                       ds_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DIFFSOUP_B200_H */
