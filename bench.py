@@ -1,0 +1,500 @@
+#!/usr/bin/env python
+"""Benchmark of the DiffSoup training step on B200.
+
+Workload (BASELINE configuration "plain method, object scale"): 15,000
+triangles on a noisy unit sphere shell, 8 views of 800x800 on a ring of radius
+4, multires features at levels 0..2 x 8 channels, shading MLP 11 -> 16 -> 3,
+stochastic binary opacity, MSE against a U[0,1] target, full forward+backward
+(edge gradients, opacity auxiliary gradient, feature/opacity/MLP/vertex
+gradients).  Synthetic, seeded inputs stand in for the reference's datasets.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  `value` is views/s of the batched BF16 step
+(diffsoup_b200.step.TrainStep, one CUDA graph per step) with inputs resident
+in HBM; `e2e` is the same step through the public API with each step's
+camera matrices and target images copied from pinned host memory and the loss
+read back.  N > 1 runs one independent replica per GPU (views are
+independent; the reference has no multi-GPU exchange), timed as the max over
+ranks.  --impl reference times the CPU restatement of the reference's step
+(oracle/pipeline.py, FP32, all host threads) on a bounded sample.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+bwd views/s @15K tris 800²: batched BF16 vs plain FP32 on one B200"
+WORKLOAD = "config2: 15K-tri sphere-shell soup, 8 views 800x800, levels 0..2 x 8 ch, MLP 11-16-3, stochastic opacity"
+N_INPUT_SETS = 4  # rotating view batches: 4 x 61 MB of targets, larger than the 126 MB L2
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        if self.proc is None:
+            return out
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        try:
+            rows = [l.strip().split(",") for l in open(self.path) if l.strip()]
+            os.unlink(self.path)
+        except Exception:
+            return out
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except Exception:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if sm:
+            out.update(sm_mhz=statistics.median(sm), sm_max_mhz=max(mx), samples=len(sm))
+        out["reasons"] = sorted(reasons)
+        return out
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+def make_inputs(rank: int):
+    from diffsoup_b200 import scenes
+
+    sc = scenes.make_scene(2, seed=0, with_targets=False)
+    mlp = scenes.mlp_weights(sc.mlp_input_dim, 3, sc.hidden_dim, sc.n_layers, seed=0)
+    sets = []
+    rng = np.random.default_rng(1000 + rank)
+    for r in range(N_INPUT_SETS):
+        phase = 2 * math.pi * (rank * N_INPUT_SETS + r) / (8 * N_INPUT_SETS * 64)
+        views = []
+        for i in range(8):
+            th = 2 * math.pi * i / 8 + phase
+            eye = np.array([4 * math.cos(th), 4 * math.sin(th), 1.2])
+            views.append(scenes._make_view(eye, 800, 800))
+        mvp = np.stack([v.mvp for v in views]).astype(np.float32)
+        inv = np.stack([v.inv_mvp for v in views]).astype(np.float32)
+        tgt = rng.uniform(0, 1, size=(8 * 800 * 800, 3)).astype(np.float32)
+        sets.append((mvp, inv, tgt))
+    return sc, mlp, sets
+
+
+def mlp_flat(mlp):
+    return np.concatenate([np.concatenate([W.reshape(-1), b]) for W, b in mlp]).astype(np.float32)
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args):
+    """CPU restatement of the reference's step (the oracle port), rank 0 only."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    from oracle import cpu, pipeline as P
+    from diffsoup_b200 import scenes
+
+    sc, mlp, sets = make_inputs(0)
+    cores = cpu.omp_threads()
+    torch.set_num_threads(max(1, os.cpu_count() or 1))
+
+    def one_view(i):
+        mvp, inv, tgt = sets[i % N_INPUT_SETS]
+        b = i % 8
+        inp = P.StepInputs(verts=sc.verts, tri=sc.tri, mvps=mvp[b:b + 1], inv_mvps=inv[b:b + 1], hw=[(800, 800)],
+                           feat_src=sc.feat_src, alpha_src=sc.alpha_src[..., 0], mlp=mlp,
+                           targets=[tgt.reshape(8, 800, 800, 3)[b]], min_level=sc.min_level,
+                           max_level=sc.max_level, stochastic=True, seed=7, iteration=i)
+        P.train_step(inp, "f32")
+
+    for i in range(min(args.warmup, 2)):
+        one_view(i)
+    budget = 120.0
+    t0 = time.perf_counter()
+    n = 0
+    for i in range(args.steps):
+        one_view(i)
+        n += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    dt = time.perf_counter() - t0
+    v = n / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "views/s", "n_gpus": args.gpus,
+        "steps": n, "warmup": min(args.warmup, 2), "ms_per_step": 1000 * dt / n, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD, "step_unit": "one 800x800 view per step (bounded sample)"},
+        "cpu_baseline": {"value": v, "unit": "views/s", "cores": cores, "kind": "port",
+                         "sample": f"{n} views of config 2 (800x800, 15K tris), FP32 oracle port, {cores} threads"},
+        "e2e": {"value": v, "unit": "views/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def algorithmic_bytes(phase: str, P_: int, B: int, T: int, V: int, ST: int, C_: int) -> float:
+    """Minimal DRAM bytes of one launch of each step kernel."""
+    if phase == "shade":  # rast 16 R, target 12 R, colour 12 W, dL/dcolour 12 W, |c-t| 4 W; bf16 features + fp32 grads
+        return P_ * 56.0 + T * ST * C_ * (2 + 8)
+    if phase == "raster":  # rast 16 W per pixel; triangle records 64 B per (view, tri); opacity table
+        return P_ * 16.0 + B * T * 64.0 + T * ST * 4.0
+    if phase == "aux":  # rast 16 R + |c-t| 4 R per pixel; records; opacity table + grads
+        return P_ * 20.0 + B * T * 64.0 + T * ST * 12.0
+    if phase == "edge":  # rast 16 + colour 12 + dL/dcolour 12 per pixel; clip positions + fp64 grads
+        return P_ * 40.0 + B * V * (16.0 + 64.0)
+    if phase == "bin":
+        return B * T * (12.0 * 3 + 64.0 + 2 * 16.0)
+    if phase == "prep":
+        return T * ST * C_ * 10.0 + B * V * 28.0
+    return 0.0
+
+
+def run_ours(args):
+    import torch.distributed as dist
+    from diffsoup_b200 import scenes, _core
+    from diffsoup_b200.step import TrainStep
+    import diffsoup_b200 as ds
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    sc, mlp, sets = make_inputs(rank)
+    B, T, V = 8, sc.T, sc.verts.shape[0]
+    hw = [(800, 800)] * B
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    verts, tri = t(sc.verts), t(sc.tri)
+    feat_src, alpha_src = t(sc.feat_src), t(sc.alpha_src[..., 0])
+    params = t(mlp_flat(mlp))
+    dsets = [(t(m), t(i), t(g)) for m, i, g in sets]
+    step = TrainStep(T, V, hw, sc.feat_dim, sc.min_level, sc.max_level, sc.hidden_dim, sc.n_layers,
+                     stochastic=True, seed=1234 + rank, device=dev)
+
+    def kw(s):
+        return dict(verts=verts, tri=tri, mvp=s[0], inv_mvp=s[1], feat_src=feat_src, alpha_src=alpha_src,
+                    mlp_params=params, target=s[2])
+
+    step.fit_capacity(**kw(dsets[0]))
+    for s in dsets[1:]:
+        step.status.zero_()
+        step.run(**kw(s))
+        if step.overflowed():
+            step.capacity *= 2
+            step._alloc()
+    graphs = [step.capture(**kw(s)) for s in dsets]
+    torch.cuda.synchronize()
+
+    # ---------------- device-resident throughput ------------------------------
+    for i in range(args.warmup):
+        graphs[i % N_INPUT_SETS].replay()
+    step.status.zero_()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.25)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(args.steps):
+        graphs[i % N_INPUT_SETS].replay()
+    e1.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        tt = torch.tensor([ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    overflow = step.overflowed()
+    value = B * args.steps * world / (ms / 1000.0)
+
+    # ---------------- end to end through the public API -----------------------
+    # pinned host inputs; each step copies its cameras and targets H2D on a copy
+    # stream (double-buffered, overlapping the previous step) and reads the loss.
+    host = [(torch.from_numpy(m).pin_memory(), torch.from_numpy(i).pin_memory(), torch.from_numpy(g).pin_memory())
+            for m, i, g in sets]
+    bufs = [tuple(x.clone() for x in dsets[0]) for _ in range(2)]
+    egraphs = [step.capture(**kw(b)) for b in bufs]
+    loss_host = torch.empty(max(args.steps, 1), dtype=torch.float32, pin_memory=True)
+    comp = torch.cuda.current_stream()
+    cs = torch.cuda.Stream(dev)
+    copied = [torch.cuda.Event() for _ in range(2)]
+    done = [torch.cuda.Event() for _ in range(2)]
+    for d in done:
+        d.record(comp)
+    h2d = sum(x.numel() * x.element_size() for x in host[0])
+
+    def issue_copy(i):
+        j = i % 2
+        cs.wait_event(done[j])
+        with torch.cuda.stream(cs):
+            for dst, src in zip(bufs[j], host[i % N_INPUT_SETS]):
+                dst.copy_(src, non_blocking=True)
+        copied[j].record(cs)
+
+    def e2e_loop(n):
+        issue_copy(0)
+        for i in range(n):
+            j = i % 2
+            if i + 1 < n:
+                issue_copy(i + 1)
+            comp.wait_event(copied[j])
+            egraphs[j].replay()
+            loss_host[i].copy_(step.loss[0], non_blocking=True)
+            done[j].record(comp)
+
+    e2e_loop(min(args.warmup, 4) or 1)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record()
+    cs.wait_event(f0)
+    e2e_loop(args.steps)
+    f1.record()
+    torch.cuda.synchronize()
+    ems = f0.elapsed_time(f1)
+    if world > 1:
+        tt = torch.tensor([ems], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ems = float(tt.item())
+    e2e = B * args.steps * world / (ems / 1000.0)
+    assert np.isfinite(loss_host[: args.steps].numpy()).all()
+
+    # ---------------- per-phase kernel time (roofline) ------------------------
+    names = ["prep", "bin", "raster", "shade", "aux", "edge", "finish"]
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(8)]
+    for e in evs:  # torch creates the CUDA event on first record
+        e.record()
+    torch.cuda.synchronize()
+    handles = ctypes_void_p_array(evs)
+    _core.check(_core.lib.ds_train_step_set_events(handles, 8))
+    acc = {n: 0.0 for n in names}
+    M = 20
+    for i in range(M):
+        step.run(**kw(dsets[i % N_INPUT_SETS]))
+        torch.cuda.synchronize()
+        for k, n in enumerate(names):
+            acc[n] += evs[k].elapsed_time(evs[k + 1])
+    _core.check(_core.lib.ds_train_step_set_events(None, 0))
+    phase_ms = {n: acc[n] / M for n in names}
+    dom = max(["raster", "shade", "aux", "edge"], key=lambda n: phase_ms[n])
+    ST = _core.feats_at_level(sc.max_level)
+    P_ = step.num_pixels
+    alg = algorithmic_bytes(dom, P_, B, T, V, ST, sc.feat_dim)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    achieved = alg / (phase_ms[dom] / 1000.0) / 1e9
+    traffic = read_traffic(dom)
+
+    # ---------------- plain FP32 single-view path (denominator) ---------------
+    plain = None
+    if not args.no_plain and rank == 0:
+        plain = run_plain(sc, mlp, sets[0], dev, n_views=16)
+
+    # ---------------- CPU baseline --------------------------------------------
+    cpu_base = None
+    if not args.no_cpu_baseline and rank == 0:
+        cpu_base = run_cpu_baseline(sc, mlp, sets[0])
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "views/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16", "data": "synthetic (seeded; stands in for the reference datasets)",
+        "config": {"workload": WORKLOAD, "views_per_step": B, "triangles": T, "resolution": "800x800",
+                   "parallelism": f"replicas x{world}", "graph": "one CUDA graph per step",
+                   "l2": f"{N_INPUT_SETS} rotating input sets (4 x 61 MB targets) larger than L2",
+                   "list_overflow": overflow},
+        "e2e": {"value": e2e, "unit": "views/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 4},
+        "gpu_launches": 16 * args.steps,
+        "clocks": clocks,
+        "phase_ms": {k: round(v, 4) for k, v in phase_ms.items()},
+        "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
+                     "algorithmic_bytes": alg},
+    }
+    if plain is not None:
+        line["plain_fp32"] = plain
+        line["speedup_vs_plain_fp32"] = value / plain["value"]
+    if cpu_base is not None:
+        line["cpu_baseline"] = cpu_base
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    del graphs, egraphs
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def ctypes_void_p_array(events):
+    import ctypes as C
+
+    arr = (C.c_void_p * len(events))()
+    for i, e in enumerate(events):
+        arr[i] = C.c_void_p(e.cuda_event)
+    return arr
+
+
+def read_traffic(kernel: str):
+    """DRAM bytes per launch from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    try:
+        for l in open(path):
+            f = l.split()
+            if len(f) >= 2 and f[0] == kernel and not l.startswith("#"):
+                return float(f[1])
+    except Exception:
+        pass
+    return None
+
+
+def run_plain(sc, mlp, s, dev, n_views: int):
+    """The drop-in API, one view per call, FP32, eager (no graph): the
+    reference's own training-step structure (examples/02_synthetic.py:354-385)."""
+    import diffsoup_b200 as ds
+
+    mvp, inv, tgt = s
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    verts = t(sc.verts).requires_grad_(True)
+    tri = t(sc.tri)
+    feat_src = t(sc.feat_src).requires_grad_(True)
+    alpha_src = t(sc.alpha_src).requires_grad_(True)
+    net = ds.ColorMLP(sc.mlp_input_dim, 3, hidden_dim=sc.hidden_dim, n_layers=sc.n_layers).to(dev)
+    with torch.no_grad():
+        lins = [m for m in net.mlp if isinstance(m, torch.nn.Linear)]
+        for lin, (W, b) in zip(lins, mlp):
+            lin.weight.copy_(t(W))
+            lin.bias.copy_(t(b))
+    mvps, invs = t(mvp), t(inv)
+    tg = t(tgt.reshape(8, 800, 800, 3))
+    lo, hi = sc.min_level, sc.max_level
+
+    def one(b):
+        vh = torch.cat([verts, torch.ones_like(verts[:, :1])], dim=-1)
+        clip = torch.einsum("bij,nj->bni", mvps[b:b + 1], vh).contiguous()
+        alpha_acc = ds.accumulate_to_level(lo, hi, alpha_src).sigmoid()
+        feat_acc = ds.accumulate_to_level(lo, hi, feat_src).sigmoid()
+        rast = ds.rasterize_multires_triangle_alpha((800, 800), clip, tri, hi, alpha_acc)
+        feat = ds.multires_triangle_color(rast, hi, feat_acc)
+        x = torch.cat([feat, ds.encode_view_dir(rast, invs[b:b + 1])], dim=-1)
+        color = net(x, mask=rast[..., -1] > 0)
+        m = (rast.detach()[..., -1:] > 0).float()
+        color = m * color + (1.0 - m)
+        target = tg[b:b + 1]
+        aux = ds.opacity_aux_loss(color.detach(), target, rast, clip, tri, hi, alpha_acc)
+        color = ds.edge_grad(color, rast, clip, tri)
+        loss = aux + ((color - target) ** 2).mean()
+        for p in (verts, feat_src, alpha_src, *net.parameters()):
+            p.grad = None
+        loss.backward()
+        return loss
+
+    for i in range(4):
+        one(i % 8)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(n_views):
+        one(i % 8)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return {"value": n_views / (ms / 1000.0), "unit": "views/s", "views": n_views,
+            "path": "diffsoup_b200 drop-in API, one 800x800 view per call, FP32, eager autograd, torch ColorMLP"}
+
+
+def run_cpu_baseline(sc, mlp, s):
+    from oracle import cpu, pipeline as P
+
+    mvp, inv, tgt = s
+    cores = cpu.omp_threads()
+    torch.set_num_threads(max(1, os.cpu_count() or 1))
+    t0 = time.perf_counter()
+    n = 0
+    while n < 8 and (n < 2 or time.perf_counter() - t0 < 15.0):
+        b = n % 8
+        inp = P.StepInputs(verts=sc.verts, tri=sc.tri, mvps=mvp[b:b + 1], inv_mvps=inv[b:b + 1], hw=[(800, 800)],
+                           feat_src=sc.feat_src, alpha_src=sc.alpha_src[..., 0], mlp=mlp,
+                           targets=[tgt.reshape(8, 800, 800, 3)[b]], min_level=sc.min_level, max_level=sc.max_level,
+                           stochastic=True, seed=7, iteration=n)
+        P.train_step(inp, "f32")
+        n += 1
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "views/s", "cores": cores, "kind": "port",
+            "sample": f"{n} views of config 2 (800x800, 15K tris) through the FP32 oracle port, {cores} threads"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,467 @@
+// diffsoup_b200/csrc/shade.cuh -- fused per-pixel shading forward+backward
+// of the DiffSoup training step, with the shading MLP on BF16 tensor cores.
+//
+// For every pixel of the packed batch this kernel does, in one pass:
+//   feature gather     multires_triangle_color (multires.cu:224-247), bf16
+//                      features, fp32 interpolation
+//   view direction     compute_view_direction (encoding.cu:28-53)
+//   shading MLP        ColorMLP (multires.py:171-207): Linear/ReLU layers and
+//                      a sigmoid output on mma.sync m16n8k16 (bf16 x bf16 ->
+//                      fp32), biases added in fp32
+//   residual blend     (1 - x3) * x[0:3] + x3 * mlp(x), background 1 where the
+//                      pixel is empty (examples/02_synthetic.py:365-368)
+//   MSE loss           sum of (c - target)^2 and dL/dc = 2 (c - target) / N
+//   MLP backward       dX and dW/db on the tensor cores
+//   feature scatter    adjoint of the gather (multires.cu:268-292)
+// and writes colour, dL/dcolour and |c - target| summed over channels for the
+// edge-gradient and opacity passes.  A warp owns 32 consecutive pixels; its
+// activations live in shared memory as row-major bf16 tiles that ldmatrix
+// turns into fragments (plain or transposed as each product needs).
+#pragma once
+
+#include "geometry.cuh"
+#include "mma.cuh"
+
+namespace dsb {
+
+template <int C_, int IN_PAD_, int HID_, int NL_>
+struct ShadeCfg {
+    static constexpr int C = C_;             // feature channels
+    static constexpr int IN_REAL = C_ + 3;   // features + view direction
+    static constexpr int IN_PAD = IN_PAD_;   // multiple of 16
+    static constexpr int HID = HID_;         // multiple of 16
+    static constexpr int NL = NL_;           // hidden layers
+    static constexpr int OUT = 3;
+    static constexpr int LDX = IN_PAD + 8;   // padded row strides (bf16): conflict-free ldmatrix
+    static constexpr int LDH = HID + 8;
+    static constexpr int LDO = 16 + 8;
+    static constexpr int LDS = (IN_PAD > 16 ? IN_PAD : 16) + 1;  // fp32 scratch stride
+    static constexpr int WARPS = 4;
+    static constexpr int NH = NL > 1 ? NL - 1 : 1;  // hidden-to-hidden matrices (at least 1 slot)
+    // packed fp32 parameter offsets: W0[HID][IN_REAL] b0[HID] (Wl[HID][HID] bl[HID])* Wo[3][HID] bo[3]
+    static constexpr int P_W0 = 0;
+    static constexpr int P_B0 = HID * IN_REAL;
+    static constexpr int P_WH = P_B0 + HID;
+    static constexpr int P_WO = P_WH + (NL - 1) * (HID * HID + HID);
+    static constexpr int P_BO = P_WO + OUT * HID;
+    static constexpr int NPARAM = P_BO + OUT;
+    static_assert(IN_PAD % 16 == 0 && IN_PAD >= IN_REAL && HID % 16 == 0, "MLP dims");
+    static_assert((LDX * 2) % 16 == 0 && (LDH * 2) % 16 == 0 && (LDO * 2) % 16 == 0, "ldmatrix row alignment");
+};
+
+// Every ldmatrix row address must be 16-byte aligned: all tiles start on
+// 16-byte boundaries and their row strides are multiples of 8 bf16.
+template <class K>
+struct __align__(16) ShadeWarpSmem {
+    __align__(16) __nv_bfloat16 X[32 * K::LDX];
+    __align__(16) __nv_bfloat16 H[K::NL][32 * K::LDH];
+    __align__(16) __nv_bfloat16 DZO[32 * K::LDO];
+    __align__(16) __nv_bfloat16 DH[2][32 * K::LDH];
+    __align__(16) float scr[32 * K::LDS];
+};
+
+template <class K>
+struct __align__(16) ShadeSmem {
+    __align__(16) __nv_bfloat16 W0[K::HID * K::LDX];
+    __align__(16) __nv_bfloat16 WH[K::NH][K::HID * K::LDH];
+    __align__(16) __nv_bfloat16 WO[16 * K::LDH];
+    float b0[K::HID];
+    float bh[K::NH][K::HID];
+    float bo[4];
+    // fp32 gradient accumulators of this CTA (same packing as the parameters)
+    float g[K::NPARAM];
+    float loss[K::WARPS];
+    __align__(16) ShadeWarpSmem<K> w[K::WARPS];
+};
+
+struct ShadeArgs {
+    int B;
+    const ds_view_desc* views;
+    int64_t num_pixels;
+    const float* rast;            // [P,4]
+    const __nv_bfloat16* feat;    // [T,S,C] sigmoid features, bf16
+    int level, S;
+    const float* inv_mvp;         // [B,16]
+    const float* target;          // [P,3]
+    const float* params;          // packed fp32 MLP parameters
+    float inv_n;                  // 1 / (P * 3)
+    float* color;                 // [P,3]
+    float* grad_color;            // [P,3]
+    float* l1;                    // [P]
+    float* grad_feat;             // [T,S,C] fp32, accumulates
+    float* grad_params;           // packed, accumulates
+    double* loss_sum;             // [1], accumulates sum of squared errors
+};
+
+__device__ __forceinline__ int view_of_pixel(const ds_view_desc* __restrict__ views, int B, int64_t p) {
+    int lo = 0, hi = B - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&views[mid].pix_offset) <= p) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Relu mask of an activation element stored as bf16 in smem.
+__device__ __forceinline__ float2 relu_gate(const __nv_bfloat16* h, float2 v) {
+    const __nv_bfloat162 hv = *reinterpret_cast<const __nv_bfloat162*>(h);
+    return make_float2(__low2float(hv) > 0.f ? v.x : 0.f, __high2float(hv) > 0.f ? v.y : 0.f);
+}
+
+template <class K>
+__global__ void __launch_bounds__(K::WARPS * 32) shade_step_kernel(ShadeArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ShadeSmem<K>& sm = *reinterpret_cast<ShadeSmem<K>*>(smem_raw);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, q = lane & 3;
+    constexpr int HID = K::HID, IN_PAD = K::IN_PAD;
+
+    // ---- weights to shared memory (bf16, zero padded), biases fp32 --------
+    for (int i = threadIdx.x; i < HID * K::LDX; i += blockDim.x) {
+        const int r = i / K::LDX, c = i % K::LDX;
+        sm.W0[i] = __float2bfloat16_rn(c < K::IN_REAL ? a.params[K::P_W0 + r * K::IN_REAL + c] : 0.f);
+    }
+    for (int l = 0; l < K::NL - 1; ++l)
+        for (int i = threadIdx.x; i < HID * K::LDH; i += blockDim.x) {
+            const int r = i / K::LDH, c = i % K::LDH;
+            sm.WH[l][i] = __float2bfloat16_rn(c < HID ? a.params[K::P_WH + l * (HID * HID + HID) + r * HID + c] : 0.f);
+        }
+    for (int i = threadIdx.x; i < 16 * K::LDH; i += blockDim.x) {
+        const int r = i / K::LDH, c = i % K::LDH;
+        sm.WO[i] = __float2bfloat16_rn(r < K::OUT && c < HID ? a.params[K::P_WO + r * HID + c] : 0.f);
+    }
+    for (int i = threadIdx.x; i < HID; i += blockDim.x) {
+        sm.b0[i] = a.params[K::P_B0 + i];
+        for (int l = 0; l < K::NL - 1; ++l) sm.bh[l][i] = a.params[K::P_WH + l * (HID * HID + HID) + HID * HID + i];
+    }
+    if (threadIdx.x < 4) sm.bo[threadIdx.x] = threadIdx.x < 3 ? a.params[K::P_BO + threadIdx.x] : 0.f;
+    for (int i = threadIdx.x; i < K::NPARAM; i += blockDim.x) sm.g[i] = 0.f;
+    __syncthreads();
+
+    ShadeWarpSmem<K>& ws = sm.w[warp];
+    float loss_acc = 0.f;
+    const int64_t nchunks = (a.num_pixels + 31) / 32;
+    for (int64_t chunk = (int64_t)blockIdx.x * K::WARPS + warp; chunk < nchunks;
+         chunk += (int64_t)gridDim.x * K::WARPS) {
+        // ---------------- pixel front: gather features, view direction ----------
+        const int64_t p = chunk * 32 + lane;
+        const bool valid = p < a.num_pixels;
+        float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (valid) r = reinterpret_cast<const float4*>(a.rast)[p];
+        const int t = (int)r.w - 1;
+        const bool mask = valid && t >= 0;
+        float x[K::IN_REAL];
+#pragma unroll
+        for (int c = 0; c < K::IN_REAL; ++c) x[c] = 0.f;
+        uint32_t idx[3] = {0, 0, 0};
+        float wgt[3] = {0.f, 0.f, 0.f};
+        if (mask) {
+            lattice_cell(r.x, r.y, (uint32_t)a.level, idx, wgt);
+            const __nv_bfloat16* tf = a.feat + (size_t)t * a.S * K::C;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const __nv_bfloat16* fv = tf + (size_t)idx[k] * K::C;
+#pragma unroll
+                for (int c = 0; c < K::C; c += 8) {
+                    const uint4 u = __ldg(reinterpret_cast<const uint4*>(fv + c));
+                    const __nv_bfloat162* h2 = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const float2 f = __bfloat1622float2(h2[j]);
+                        x[c + 2 * j] = __fmaf_rn(wgt[k], f.x, x[c + 2 * j]);
+                        x[c + 2 * j + 1] = __fmaf_rn(wgt[k], f.y, x[c + 2 * j + 1]);
+                    }
+                }
+            }
+            const int b = view_of_pixel(a.views, a.B, p);
+            const ds_view_desc vd = a.views[b];
+            const int64_t local = p - vd.pix_offset;
+            const int py = (int)(local / vd.W), px = (int)(local % vd.W);
+            float M[16];
+#pragma unroll
+            for (int k = 0; k < 16; ++k) M[k] = __ldg(a.inv_mvp + (size_t)b * 16 + k);
+            float d[3];
+            view_direction(pix_ndc(px, vd.W), pix_ndc(py, vd.H), M, d);
+            x[K::C + 0] = d[0]; x[K::C + 1] = d[1]; x[K::C + 2] = d[2];
+        }
+        {
+            __nv_bfloat16* xr = ws.X + lane * K::LDX;
+#pragma unroll
+            for (int c = 0; c < IN_PAD; c += 2) {
+                const float v0 = c < K::IN_REAL ? x[c < K::IN_REAL ? c : 0] : 0.f;
+                const float v1 = c + 1 < K::IN_REAL ? x[c + 1 < K::IN_REAL ? c + 1 : 0] : 0.f;
+                *reinterpret_cast<uint32_t*>(xr + c) = pack_bf16(v0, v1);
+            }
+        }
+        __syncwarp();
+
+        // ---------------- MLP forward -------------------------------------------
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+#pragma unroll
+            for (int nt = 0; nt < HID / 8; ++nt) {
+                float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+                for (int kt = 0; kt < IN_PAD / 16; ++kt) {
+                    uint32_t af[4], bf[2];
+                    load_a(af, ws.X, K::LDX, mt * 16, kt * 16);
+                    load_b(bf, sm.W0, K::LDX, nt * 8, kt * 16);
+                    mma_16816(acc, af, bf);
+                }
+                const int col = nt * 8 + 2 * q;
+                const float b0v = sm.b0[col], b1v = sm.b0[col + 1];
+                __nv_bfloat16* h = ws.H[0];
+                *reinterpret_cast<uint32_t*>(h + (mt * 16 + g) * K::LDH + col) =
+                    pack_bf16(fmaxf(acc[0] + b0v, 0.f), fmaxf(acc[1] + b1v, 0.f));
+                *reinterpret_cast<uint32_t*>(h + (mt * 16 + g + 8) * K::LDH + col) =
+                    pack_bf16(fmaxf(acc[2] + b0v, 0.f), fmaxf(acc[3] + b1v, 0.f));
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int l = 1; l < K::NL; ++l) {
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt) {
+#pragma unroll
+                for (int nt = 0; nt < HID / 8; ++nt) {
+                    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+                    for (int kt = 0; kt < HID / 16; ++kt) {
+                        uint32_t af[4], bf[2];
+                        load_a(af, ws.H[l - 1], K::LDH, mt * 16, kt * 16);
+                        load_b(bf, sm.WH[l - 1], K::LDH, nt * 8, kt * 16);
+                        mma_16816(acc, af, bf);
+                    }
+                    const int col = nt * 8 + 2 * q;
+                    const float b0v = sm.bh[l - 1][col], b1v = sm.bh[l - 1][col + 1];
+                    __nv_bfloat16* h = ws.H[l];
+                    *reinterpret_cast<uint32_t*>(h + (mt * 16 + g) * K::LDH + col) =
+                        pack_bf16(fmaxf(acc[0] + b0v, 0.f), fmaxf(acc[1] + b1v, 0.f));
+                    *reinterpret_cast<uint32_t*>(h + (mt * 16 + g + 8) * K::LDH + col) =
+                        pack_bf16(fmaxf(acc[2] + b0v, 0.f), fmaxf(acc[3] + b1v, 0.f));
+                }
+            }
+            __syncwarp();
+        }
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+            float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int kt = 0; kt < HID / 16; ++kt) {
+                uint32_t af[4], bf[2];
+                load_a(af, ws.H[K::NL - 1], K::LDH, mt * 16, kt * 16);
+                load_b(bf, sm.WO, K::LDH, 0, kt * 16);
+                mma_16816(acc, af, bf);
+            }
+            if (q < 2) {
+                const int col = 2 * q;
+                ws.scr[(mt * 16 + g) * K::LDS + col] = acc[0];
+                ws.scr[(mt * 16 + g) * K::LDS + col + 1] = acc[1];
+                ws.scr[(mt * 16 + g + 8) * K::LDS + col] = acc[2];
+                ws.scr[(mt * 16 + g + 8) * K::LDS + col + 1] = acc[3];
+            }
+        }
+        __syncwarp();
+
+        // ---------------- blend, loss, dL/dcolour, output-layer gradient ---------
+        float dz[3] = {0.f, 0.f, 0.f};
+        float dxd[4] = {0.f, 0.f, 0.f, 0.f};  // direct gradient of x[0..3] through the blend
+        if (valid) {
+            const float res = x[3];
+            float s[3], col[3], tg[3];
+            float l1 = 0.f;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                s[c] = 1.f / (1.f + expf(-(ws.scr[lane * K::LDS + c] + sm.bo[c])));
+                col[c] = mask ? (1.f - res) * x[c] + res * s[c] : 1.f;
+                tg[c] = a.target[p * 3 + c];
+                const float diff = col[c] - tg[c];
+                loss_acc += diff * diff;
+                const float gc = 2.f * diff * a.inv_n;
+                a.color[p * 3 + c] = col[c];
+                a.grad_color[p * 3 + c] = gc;
+                l1 += fabsf(diff);
+                if (mask) {
+                    dxd[c] = (1.f - res) * gc;
+                    dxd[3] += (s[c] - x[c]) * gc;
+                    dz[c] = res * gc * s[c] * (1.f - s[c]);
+                }
+            }
+            a.l1[p] = l1;
+        }
+        {
+            __nv_bfloat16* dr = ws.DZO + lane * K::LDO;
+            *reinterpret_cast<uint32_t*>(dr + 0) = pack_bf16(dz[0], dz[1]);
+            *reinterpret_cast<uint32_t*>(dr + 2) = pack_bf16(dz[2], 0.f);
+#pragma unroll
+            for (int c = 4; c < 16; c += 2) *reinterpret_cast<uint32_t*>(dr + c) = 0u;
+        }
+        // output-layer bias gradient: column sums of dz over the warp
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            float v = dz[c];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) atomicAdd(&sm.g[K::P_BO + c], v);
+        }
+        __syncwarp();
+
+        // ---------------- MLP backward ------------------------------------------
+        // dWo[o][h] += sum_px dz[px][o] * H_last[px][h]
+#pragma unroll
+        for (int nt = 0; nt < HID / 8; ++nt) {
+            float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int kt = 0; kt < 2; ++kt) {
+                uint32_t af[4], bf[2];
+                load_a_t(af, ws.DZO, K::LDO, kt * 16, 0);
+                load_b_t(bf, ws.H[K::NL - 1], K::LDH, kt * 16, nt * 8);
+                mma_16816(acc, af, bf);
+            }
+            if (g < K::OUT) {
+                atomicAdd(&sm.g[K::P_WO + g * HID + nt * 8 + 2 * q], acc[0]);
+                atomicAdd(&sm.g[K::P_WO + g * HID + nt * 8 + 2 * q + 1], acc[1]);
+            }
+        }
+        // dZ_last = (dz . Wo) * relu'(H_last)
+        int cur = 0;
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+#pragma unroll
+            for (int nt = 0; nt < HID / 8; ++nt) {
+                float acc[4] = {0.f, 0.f, 0.f, 0.f};
+                uint32_t af[4], bf[2];
+                load_a(af, ws.DZO, K::LDO, mt * 16, 0);
+                load_b_t(bf, sm.WO, K::LDH, 0, nt * 8);
+                mma_16816(acc, af, bf);
+                const int col = nt * 8 + 2 * q;
+                const __nv_bfloat16* h = ws.H[K::NL - 1];
+                const float2 lo = relu_gate(h + (mt * 16 + g) * K::LDH + col, make_float2(acc[0], acc[1]));
+                const float2 hi = relu_gate(h + (mt * 16 + g + 8) * K::LDH + col, make_float2(acc[2], acc[3]));
+                *reinterpret_cast<uint32_t*>(ws.DH[cur] + (mt * 16 + g) * K::LDH + col) = pack_bf16(lo.x, lo.y);
+                *reinterpret_cast<uint32_t*>(ws.DH[cur] + (mt * 16 + g + 8) * K::LDH + col) = pack_bf16(hi.x, hi.y);
+                const int pb = K::NL == 1 ? K::P_B0 : K::P_WH + (K::NL - 2) * (HID * HID + HID) + HID * HID;
+                float s0 = lo.x + hi.x, s1 = lo.y + hi.y;
+#pragma unroll
+                for (int o = 4; o < 32; o <<= 1) {
+                    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+                    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+                }
+                if (g == 0) {
+                    atomicAdd(&sm.g[pb + col], s0);
+                    atomicAdd(&sm.g[pb + col + 1], s1);
+                }
+            }
+        }
+        __syncwarp();
+        // hidden layers, last to first
+#pragma unroll
+        for (int l = K::NL - 1; l >= 0; --l) {
+            const __nv_bfloat16* ain = l == 0 ? ws.X : ws.H[l > 0 ? l - 1 : 0];
+            const int ldin = l == 0 ? K::LDX : K::LDH;
+            const int nin = l == 0 ? IN_PAD : HID;
+            const __nv_bfloat16* wl = l == 0 ? sm.W0 : sm.WH[l > 0 ? l - 1 : 0];
+            const int ldw = l == 0 ? K::LDX : K::LDH;
+            const int pw = l == 0 ? K::P_W0 : K::P_WH + (l - 1) * (HID * HID + HID);
+            const int win = l == 0 ? K::IN_REAL : HID;  // row length of the packed W_l
+            // dW_l[h][i] += sum_px dZ_l[px][h] * A_in[px][i]
+#pragma unroll
+            for (int mh = 0; mh < HID / 16; ++mh) {
+#pragma unroll
+                for (int ni = 0; ni < nin / 8; ++ni) {
+                    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+                    for (int kt = 0; kt < 2; ++kt) {
+                        uint32_t af[4], bf[2];
+                        load_a_t(af, ws.DH[cur], K::LDH, kt * 16, mh * 16);
+                        load_b_t(bf, ain, ldin, kt * 16, ni * 8);
+                        mma_16816(acc, af, bf);
+                    }
+                    const int i0 = ni * 8 + 2 * q;
+                    const int h0 = mh * 16 + g;
+                    if (i0 < win) {
+                        atomicAdd(&sm.g[pw + h0 * win + i0], acc[0]);
+                        atomicAdd(&sm.g[pw + (h0 + 8) * win + i0], acc[2]);
+                    }
+                    if (i0 + 1 < win) {
+                        atomicAdd(&sm.g[pw + h0 * win + i0 + 1], acc[1]);
+                        atomicAdd(&sm.g[pw + (h0 + 8) * win + i0 + 1], acc[3]);
+                    }
+                }
+            }
+            // dA_in = dZ_l . W_l
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt) {
+#pragma unroll
+                for (int ni = 0; ni < nin / 8; ++ni) {
+                    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+                    for (int kt = 0; kt < HID / 16; ++kt) {
+                        uint32_t af[4], bf[2];
+                        load_a(af, ws.DH[cur], K::LDH, mt * 16, kt * 16);
+                        load_b_t(bf, wl, ldw, kt * 16, ni * 8);
+                        mma_16816(acc, af, bf);
+                    }
+                    const int col = ni * 8 + 2 * q;
+                    if (l == 0) {
+                        ws.scr[(mt * 16 + g) * K::LDS + col] = acc[0];
+                        ws.scr[(mt * 16 + g) * K::LDS + col + 1] = acc[1];
+                        ws.scr[(mt * 16 + g + 8) * K::LDS + col] = acc[2];
+                        ws.scr[(mt * 16 + g + 8) * K::LDS + col + 1] = acc[3];
+                    } else {
+                        const __nv_bfloat16* h = ws.H[l > 0 ? l - 1 : 0];
+                        const float2 lo = relu_gate(h + (mt * 16 + g) * K::LDH + col, make_float2(acc[0], acc[1]));
+                        const float2 hi = relu_gate(h + (mt * 16 + g + 8) * K::LDH + col, make_float2(acc[2], acc[3]));
+                        *reinterpret_cast<uint32_t*>(ws.DH[cur ^ 1] + (mt * 16 + g) * K::LDH + col) = pack_bf16(lo.x, lo.y);
+                        *reinterpret_cast<uint32_t*>(ws.DH[cur ^ 1] + (mt * 16 + g + 8) * K::LDH + col) = pack_bf16(hi.x, hi.y);
+                        const int pb = l - 1 == 0 ? K::P_B0 : K::P_WH + (l - 2) * (HID * HID + HID) + HID * HID;
+                        float s0 = lo.x + hi.x, s1 = lo.y + hi.y;
+#pragma unroll
+                        for (int o = 4; o < 32; o <<= 1) {
+                            s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+                            s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+                        }
+                        if (g == 0) {
+                            atomicAdd(&sm.g[pb + col], s0);
+                            atomicAdd(&sm.g[pb + col + 1], s1);
+                        }
+                    }
+                }
+            }
+            __syncwarp();
+            cur ^= 1;
+        }
+
+        // ---------------- feature-gradient scatter --------------------------------
+        if (mask) {
+            float dx[K::C];
+#pragma unroll
+            for (int c = 0; c < K::C; ++c) dx[c] = ws.scr[lane * K::LDS + c] + (c < 4 ? dxd[c] : 0.f);
+            float* tg = a.grad_feat + (size_t)t * a.S * K::C;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                float* dst = tg + (size_t)idx[k] * K::C;
+#pragma unroll
+                for (int c = 0; c < K::C; c += 4)
+                    atomicAdd(reinterpret_cast<float4*>(dst + c),
+                              make_float4(wgt[k] * dx[c], wgt[k] * dx[c + 1], wgt[k] * dx[c + 2], wgt[k] * dx[c + 3]));
+            }
+        }
+        __syncwarp();
+    }
+
+    // ---- CTA reduction of the loss and the parameter gradients ----------------
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) loss_acc += __shfl_xor_sync(0xffffffffu, loss_acc, o);
+    if (lane == 0) sm.loss[warp] = loss_acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < K::WARPS; ++w) s += sm.loss[w];
+        atomicAdd(a.loss_sum, s);
+    }
+    for (int i = threadIdx.x; i < K::NPARAM; i += blockDim.x)
+        if (sm.g[i] != 0.f) atomicAdd(a.grad_params + i, sm.g[i]);
+}
+
+}  // namespace dsb

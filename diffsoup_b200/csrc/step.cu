@@ -1,0 +1,399 @@
+// diffsoup_b200/csrc/step.cu -- the batched training step of DiffSoup
+// (examples/02_synthetic.py:354-388 with an MSE photometric loss) as one
+// graph-capturable sequence of sm_100a kernels:
+//
+//   accumulate_to_level(...).sigmoid() for opacity and features   (prep)
+//   project_vertices (examples/utils.py:412-426)                   (prep)
+//   screen-tile binning + tiled stochastic-opacity rasterizer      (tiled.cu)
+//   fused shading forward + backward, BF16 MLP on tensor cores     (shade.cuh)
+//   opacity auxiliary gradient, recomputed tile by tile            (tiled.cu)
+//   edge gradients to clip-space vertices                          (edge)
+//   adjoints of the sigmoid, the level accumulation and projection (finish)
+//
+// Views may differ in resolution; their pixels are packed back to back.
+#include <cstdio>
+
+#include "edge_math.cuh"
+#include "shade.cuh"
+
+namespace dsb {
+
+// ---------------------------------------------------------------------------
+// Level accumulation + sigmoid, one warp per triangle (multires.cu:329-369).
+// The triangle's source samples are staged in shared memory; outputs are
+// sigmoid(sum over levels of the lattice interpolation at each target vertex).
+// ---------------------------------------------------------------------------
+constexpr int kPrepWarps = 4;
+constexpr int kMaxSrc = 2048;  // floats of one triangle's samples per warp (S*C)
+
+template <bool BF16OUT>
+__global__ void __launch_bounds__(kPrepWarps * 32) accum_sigmoid_kernel(int T, int lo, int hi, int target, int S,
+                                                                       int ST, int C, const float* __restrict__ src,
+                                                                       float* __restrict__ out_f32,
+                                                                       __nv_bfloat16* __restrict__ out_bf16) {
+    __shared__ float s_src[kPrepWarps][kMaxSrc];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int t = blockIdx.x * kPrepWarps + warp;
+    if (t >= T) return;
+    const int n = S * C;
+    const float* ts = src + (size_t)t * n;
+    for (int i = lane; i < n; i += 32) s_src[warp][i] = ts[i];
+    __syncwarp();
+    const float R = (float)(1u << target);
+    for (int e = lane; e < ST * C; e += 32) {
+        const int k = e / C, c = e % C;
+        uint32_t x, y;
+        index_to_xy((uint32_t)k, x, y);
+        const float b0 = __fdiv_rn((float)x, R), b1 = __fdiv_rn((float)y, R);
+        float acc = 0.f;
+        uint32_t off = 0;
+        for (int l = lo; l <= hi; ++l) {
+            uint32_t idx[3]; float w[3];
+            lattice_cell(b0, b1, (uint32_t)l, idx, w);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) acc = madd(acc, w[j], s_src[warp][(off + idx[j]) * C + c]);
+            off += feats_at_level((uint32_t)l);
+        }
+        const float s = 1.f / (1.f + expf(-acc));
+        out_f32[(size_t)t * ST * C + e] = s;
+        if (BF16OUT) out_bf16[(size_t)t * ST * C + e] = __float2bfloat16_rn(s);
+    }
+}
+
+// Adjoint of accum_sigmoid: grad_src[t] = sum_k lattice^T (grad_out * s (1-s)).
+// Accumulated per warp in shared memory, written once (no global atomics).
+__global__ void __launch_bounds__(kPrepWarps * 32) accum_sigmoid_backward_kernel(
+    int T, int lo, int hi, int target, int S, int ST, int C, const float* __restrict__ sig,
+    const float* __restrict__ grad_out, float* __restrict__ grad_src) {
+    __shared__ float s_acc[kPrepWarps][kMaxSrc];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int t = blockIdx.x * kPrepWarps + warp;
+    if (t >= T) return;
+    const int n = S * C;
+    for (int i = lane; i < n; i += 32) s_acc[warp][i] = 0.f;
+    __syncwarp();
+    const float R = (float)(1u << target);
+    for (int e = lane; e < ST * C; e += 32) {
+        const int k = e / C, c = e % C;
+        const float s = sig[(size_t)t * ST * C + e];
+        const float gz = grad_out[(size_t)t * ST * C + e] * s * (1.f - s);
+        if (gz == 0.f) continue;
+        uint32_t x, y;
+        index_to_xy((uint32_t)k, x, y);
+        const float b0 = __fdiv_rn((float)x, R), b1 = __fdiv_rn((float)y, R);
+        uint32_t off = 0;
+        for (int l = lo; l <= hi; ++l) {
+            uint32_t idx[3]; float w[3];
+            lattice_cell(b0, b1, (uint32_t)l, idx, w);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) atomicAdd(&s_acc[warp][(off + idx[j]) * C + c], gz * w[j]);
+            off += feats_at_level((uint32_t)l);
+        }
+    }
+    __syncwarp();
+    for (int i = lane; i < n; i += 32) grad_src[(size_t)t * n + i] = s_acc[warp][i];
+}
+
+// clip[b][v] = mvp[b] . (verts[v], 1)  (examples/utils.py:412-426)
+__global__ void __launch_bounds__(kThreads) project_kernel(int B, int V, const float* __restrict__ verts,
+                                                           const float* __restrict__ mvp, float* __restrict__ pos) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)B * V) return;
+    const int b = (int)(i / V), v = (int)(i % V);
+    const float* M = mvp + (size_t)b * 16;
+    const float x = verts[(size_t)v * 3], y = verts[(size_t)v * 3 + 1], z = verts[(size_t)v * 3 + 2];
+    // fixed evaluation order: ((M[r][3] + M[r][0] x) + M[r][1] y) + M[r][2] z, fused
+    float4 o;
+    o.x = __fmaf_rn(M[2], z, __fmaf_rn(M[1], y, __fmaf_rn(M[0], x, M[3])));
+    o.y = __fmaf_rn(M[6], z, __fmaf_rn(M[5], y, __fmaf_rn(M[4], x, M[7])));
+    o.z = __fmaf_rn(M[10], z, __fmaf_rn(M[9], y, __fmaf_rn(M[8], x, M[11])));
+    o.w = __fmaf_rn(M[14], z, __fmaf_rn(M[13], y, __fmaf_rn(M[12], x, M[15])));
+    reinterpret_cast<float4*>(pos)[i] = o;
+}
+
+// grad_verts[v] = sum_b mvp[b][:, :3]^T grad_pos[b][v]
+__global__ void __launch_bounds__(kThreads) project_backward_kernel(int B, int V, const float* __restrict__ mvp,
+                                                                    const double* __restrict__ grad_pos,
+                                                                    float* __restrict__ grad_verts) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    double gx = 0.0, gy = 0.0, gz = 0.0;
+    for (int b = 0; b < B; ++b) {
+        const float* M = mvp + (size_t)b * 16;
+        const double* gp = grad_pos + ((size_t)b * V + v) * 4;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            gx += (double)M[r * 4 + 0] * gp[r];
+            gy += (double)M[r * 4 + 1] * gp[r];
+            gz += (double)M[r * 4 + 2] * gp[r];
+        }
+    }
+    grad_verts[(size_t)v * 3] = (float)gx;
+    grad_verts[(size_t)v * 3 + 1] = (float)gy;
+    grad_verts[(size_t)v * 3 + 2] = (float)gz;
+}
+
+// Edge gradients over packed views (rasterize.cu:653-903).  Consecutive
+// pixels of a row mostly share a triangle: a segmented warp reduction sums
+// runs of equal triangles before one FP64 atomic per vertex component.
+__global__ void __launch_bounds__(kThreads) edge_step_kernel(int B, const ds_view_desc* __restrict__ views,
+                                                             int64_t num_pixels, int V, const float* __restrict__ pos,
+                                                             const int* __restrict__ tri,
+                                                             const float* __restrict__ color,
+                                                             const float* __restrict__ grad_color,
+                                                             const float* __restrict__ rast,
+                                                             double* __restrict__ grad_pos) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    EdgeAccum acc;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) acc.g[k] = 0.f;
+    acc.any = false;
+    int b = 0, it0 = -1;
+    if (p < num_pixels) {
+        b = view_of_pixel(views, B, p);
+        const ds_view_desc vd = views[b];
+        const int64_t local = p - vd.pix_offset;
+        const int y = (int)(local / vd.W), x = (int)(local % vd.W);
+        it0 = edge_grad_pixel(b, y, x, vd.H, vd.W, 3, color, grad_color, rast, pos + (size_t)b * V * 4, tri,
+                              vd.pix_offset, acc);
+    }
+    const int key = (it0 >= 0 && acc.any) ? it0 : -1 - lane;
+    const int prev = __shfl_up_sync(0xffffffffu, key, 1);
+    const int prevb = __shfl_up_sync(0xffffffffu, b, 1);
+    const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || prev != key || prevb != b);
+    const int seg = __popc(heads & ((2u << lane) - 1u));
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+        float v = acc.g[k];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const float ov = __shfl_down_sync(0xffffffffu, v, o);
+            const int os = __shfl_down_sync(0xffffffffu, seg, o);
+            if (lane + o < 32 && os == seg) v += ov;
+        }
+        acc.g[k] = v;
+    }
+    const bool head = (heads >> lane) & 1u;
+    if (head && key >= 0) {
+        double* gp = grad_pos + (size_t)b * V * 4;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const int v = __ldg(tri + it0 * 3 + k);
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (acc.g[k * 4 + j] != 0.f) atomicAdd(gp + (size_t)v * 4 + j, (double)acc.g[k * 4 + j]);
+        }
+    }
+}
+
+__global__ void finish_kernel(const double* __restrict__ loss_sum, float inv_n, float* __restrict__ loss,
+                              uint64_t* __restrict__ rng) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        *loss = (float)(*loss_sum * (double)inv_n);
+        if (rng) rng[1] += 1;  // next iteration of the opacity-threshold RNG
+    }
+}
+
+template <class K>
+static int launch_shade(const ShadeArgs& a, cudaStream_t st) {
+    const size_t smem = sizeof(ShadeSmem<K>);
+    static int per_sm = 0;  // set on the first (eager) call, before any graph capture
+    if (per_sm == 0) {
+        DS_CUDA(cudaFuncSetAttribute(shade_step_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        DS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, shade_step_kernel<K>, K::WARPS * 32, smem));
+        if (per_sm <= 0) return set_error(DS_ERR_CUDA, "shade_step: kernel does not fit on an SM");
+    }
+    const int64_t chunks = (a.num_pixels + 31) / 32;
+    const int64_t want = (chunks + K::WARPS - 1) / K::WARPS;
+    const int64_t cap = (int64_t)kSMs * (per_sm > 0 ? per_sm : 1);
+    const unsigned grid = (unsigned)(want < 1 ? 1 : (want < cap ? want : cap));
+    shade_step_kernel<K><<<grid, K::WARPS * 32, smem, st>>>(a);
+    return check_launch("shade_step");
+}
+
+static inline size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Optional phase events (profiling): recorded on the step's stream at the
+// boundaries prep | bin | raster | shade | aux | edge | finish.
+constexpr int kStepEvents = 8;
+static cudaEvent_t g_step_events[kStepEvents];
+static int g_step_nevents = 0;
+
+static int mark(int i, cudaStream_t st) {
+    if (i < g_step_nevents) DS_CUDA(cudaEventRecord(g_step_events[i], st));
+    return DS_OK;
+}
+
+struct StepWs {
+    float* pos;
+    float* alpha_acc;
+    float* feat_acc;
+    __nv_bfloat16* feat_bf16;
+    float* rast;
+    float* color;
+    float* grad_color;
+    float* l1;
+    double* grad_pos;
+    float* grad_alpha_acc;
+    float* grad_feat_acc;
+    double* loss_sum;
+    void* tiles;
+    size_t tiles_bytes;
+};
+
+static StepWs carve_step(void* ws, const ds_step_config& c, int num_tiles, int64_t P, int64_t cap, size_t* total) {
+    char* base = reinterpret_cast<char*>(ws);
+    const int ST = (int)feats_at_level((uint32_t)c.max_level);
+    size_t o = 0;
+    StepWs w;
+    w.pos = reinterpret_cast<float*>(base + o); o += al((size_t)c.B * c.V * 16);
+    w.alpha_acc = reinterpret_cast<float*>(base + o); o += al((size_t)c.T * ST * 4);
+    w.feat_acc = reinterpret_cast<float*>(base + o); o += al((size_t)c.T * ST * c.C * 4);
+    w.feat_bf16 = reinterpret_cast<__nv_bfloat16*>(base + o); o += al((size_t)c.T * ST * c.C * 2);
+    w.rast = reinterpret_cast<float*>(base + o); o += al((size_t)P * 16);
+    w.color = reinterpret_cast<float*>(base + o); o += al((size_t)P * 12);
+    w.grad_color = reinterpret_cast<float*>(base + o); o += al((size_t)P * 12);
+    w.l1 = reinterpret_cast<float*>(base + o); o += al((size_t)P * 4);
+    // zeroed together each step: grad_pos .. loss_sum
+    w.grad_pos = reinterpret_cast<double*>(base + o); o += al((size_t)c.B * c.V * 32);
+    w.grad_alpha_acc = reinterpret_cast<float*>(base + o); o += al((size_t)c.T * ST * 4);
+    w.grad_feat_acc = reinterpret_cast<float*>(base + o); o += al((size_t)c.T * ST * c.C * 4);
+    w.loss_sum = reinterpret_cast<double*>(base + o); o += 256;
+    w.tiles = base + o;
+    w.tiles_bytes = ds_tiles_workspace_size(c.B, c.T, num_tiles, cap);
+    o += al(w.tiles_bytes);
+    if (total) *total = o;
+    return w;
+}
+
+template <class K>
+static int shade_dispatch_check(const ds_step_config& c) {
+    return (c.C == K::C && c.hidden == K::HID && c.n_layers == K::NL) ? 1 : 0;
+}
+
+}  // namespace dsb
+
+using namespace dsb;
+
+using ShadeC8H16 = ShadeCfg<8, 16, 16, 1>;    // configs 1-3: 8 features + 3 view dir -> 16 -> 3
+using ShadeC16H64 = ShadeCfg<16, 32, 64, 2>;  // configs 4-5: 16 + 3 -> 64 -> 64 -> 3
+
+extern "C" {
+
+size_t ds_train_step_workspace_size(const ds_step_config* cfg, int num_tiles, int64_t num_pixels,
+                                    int64_t list_capacity) {
+    size_t total = 0;
+    carve_step(nullptr, *cfg, num_tiles, num_pixels, list_capacity, &total);
+    return total;
+}
+
+int ds_train_step_set_events(void* const* events, int n) {
+    DS_CHECK_ARG(n >= 0 && n <= kStepEvents && (n == 0 || events != nullptr), "train_step_set_events: bad count");
+    for (int i = 0; i < n; ++i) g_step_events[i] = (cudaEvent_t)events[i];
+    g_step_nevents = n;
+    return DS_OK;
+}
+
+int ds_train_step_layout(const ds_step_config* cfg, int num_tiles, int64_t num_pixels, int64_t list_capacity,
+                         int64_t* offsets) {
+    DS_CHECK_ARG(cfg != nullptr && offsets != nullptr, "train_step_layout: null argument");
+    StepWs w = carve_step(nullptr, *cfg, num_tiles, num_pixels, list_capacity, nullptr);
+    const void* ptrs[11] = {w.pos, w.alpha_acc, w.feat_acc, w.feat_bf16, w.rast, w.color, w.grad_color, w.l1,
+                            w.grad_pos, w.grad_alpha_acc, w.grad_feat_acc};
+    for (int i = 0; i < 11; ++i) offsets[i] = (int64_t)(reinterpret_cast<const char*>(ptrs[i]) - (const char*)nullptr);
+    return DS_OK;
+}
+
+int ds_mlp_param_count(int C, int hidden, int n_layers) {
+    const int in = C + 3;
+    return hidden * in + hidden + (n_layers - 1) * (hidden * hidden + hidden) + 3 * hidden + 3;
+}
+
+int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_tiles, int64_t num_pixels,
+                  const float* verts, const int* tri, const float* mvp, const float* inv_mvp, const float* feat_src,
+                  const float* alpha_src, const float* mlp_params, const float* target, uint64_t* rng,
+                  float* loss, float* grad_verts, float* grad_feat_src, float* grad_alpha_src,
+                  float* grad_mlp_params, float* rast_out, float* color_out, void* workspace, size_t workspace_bytes,
+                  int64_t list_capacity, int* status, ds_stream_t stream) {
+    DS_CHECK_ARG(cfg != nullptr, "train_step: null config");
+    const ds_step_config c = *cfg;
+    DS_CHECK_ARG(c.B > 0 && c.T >= 0 && c.V >= 0 && num_tiles > 0 && num_pixels > 0, "train_step: bad sizes");
+    DS_CHECK_ARG(c.min_level >= 0 && c.max_level >= c.min_level && c.max_level <= 8, "train_step: bad levels");
+    DS_CHECK_ARG(c.stochastic == 0 || rng != nullptr, "train_step: stochastic opacity needs the rng state");
+    const bool k8 = shade_dispatch_check<ShadeC8H16>(c), k16 = shade_dispatch_check<ShadeC16H64>(c);
+    DS_CHECK_ARG(k8 || k16, "train_step: unsupported MLP (C=%d hidden=%d layers=%d); built: 8/16/1, 16/64/2", c.C,
+                 c.hidden, c.n_layers);
+    const int S = (int)total_feats((uint32_t)c.min_level, (uint32_t)c.max_level);
+    const int ST = (int)feats_at_level((uint32_t)c.max_level);
+    DS_CHECK_ARG(S * c.C <= kMaxSrc, "train_step: %d samples x %d channels exceed the per-triangle limit", S, c.C);
+    size_t need = 0;
+    StepWs w = carve_step(workspace, c, num_tiles, num_pixels, list_capacity, &need);
+    if (workspace_bytes < need) return set_error(DS_ERR_WORKSPACE, "train_step: workspace too small");
+    cudaStream_t st = (cudaStream_t)stream;
+
+    int rc = mark(0, st);
+    if (rc) return rc;
+    // zero the accumulators of this step
+    DS_CUDA(cudaMemsetAsync(w.grad_pos, 0, reinterpret_cast<char*>(w.loss_sum) + 8 - reinterpret_cast<char*>(w.grad_pos),
+                            st));
+    DS_CUDA(cudaMemsetAsync(grad_mlp_params, 0, sizeof(float) * ds_mlp_param_count(c.C, c.hidden, c.n_layers), st));
+
+    // prep: opacity and feature accumulation + sigmoid, projection
+    const unsigned tb = (unsigned)((c.T + kPrepWarps - 1) / kPrepWarps);
+    if (c.T > 0) {
+        accum_sigmoid_kernel<false><<<tb, kPrepWarps * 32, 0, st>>>(c.T, c.min_level, c.max_level, c.max_level, S, ST, 1,
+                                                                   alpha_src, w.alpha_acc, nullptr);
+        accum_sigmoid_kernel<true><<<tb, kPrepWarps * 32, 0, st>>>(c.T, c.min_level, c.max_level, c.max_level, S, ST,
+                                                                  c.C, feat_src, w.feat_acc, w.feat_bf16);
+    }
+    if ((int64_t)c.B * c.V > 0)
+        project_kernel<<<blocks_for((int64_t)c.B * c.V), kThreads, 0, st>>>(c.B, c.V, verts, mvp, w.pos);
+    rc = check_launch("train_step prep");
+    if (rc || (rc = mark(1, st))) return rc;
+
+    // forward rasterization
+    float* rast = rast_out ? rast_out : w.rast;
+    rc = ds_tiles_bin(c.B, views, num_tiles, c.V, w.pos, c.T, tri, w.tiles, w.tiles_bytes, list_capacity, status,
+                      stream);
+    if (rc || (rc = mark(2, st))) return rc;
+    rc = ds_tiles_rasterize(c.B, views, num_tiles, c.V, w.pos, c.T, tri, c.max_level, ST, w.alpha_acc,
+                            c.stochastic ? 1 : 0, c.thr_const, rng, rast, w.tiles, w.tiles_bytes, list_capacity,
+                            stream);
+    if (rc || (rc = mark(3, st))) return rc;
+
+    // fused shading forward + backward
+    ShadeArgs a;
+    a.B = c.B; a.views = views; a.num_pixels = num_pixels; a.rast = rast; a.feat = w.feat_bf16;
+    a.level = c.max_level; a.S = ST; a.inv_mvp = inv_mvp; a.target = target; a.params = mlp_params;
+    a.inv_n = (float)(1.0 / ((double)num_pixels * 3.0));
+    a.color = color_out ? color_out : w.color; a.grad_color = w.grad_color; a.l1 = w.l1;
+    a.grad_feat = w.grad_feat_acc; a.grad_params = grad_mlp_params; a.loss_sum = w.loss_sum;
+    rc = k8 ? launch_shade<ShadeC8H16>(a, st) : launch_shade<ShadeC16H64>(a, st);
+    if (rc || (rc = mark(4, st))) return rc;
+
+    // opacity auxiliary gradient (scaled by 1/numel(colour), rasterize.py:183-195)
+    rc = ds_tiles_opacity_aux(c.B, views, num_tiles, c.V, w.pos, c.T, tri, c.max_level, ST, w.alpha_acc, 1, w.l1,
+                              nullptr, rast, a.inv_n, w.grad_alpha_acc, w.tiles, w.tiles_bytes, list_capacity, stream);
+    if (rc || (rc = mark(5, st))) return rc;
+
+    // edge gradients to clip-space positions
+    edge_step_kernel<<<blocks_for(num_pixels), kThreads, 0, st>>>(c.B, views, num_pixels, c.V, w.pos, tri, a.color,
+                                                                  w.grad_color, rast, w.grad_pos);
+    if ((rc = mark(6, st))) return rc;
+    // adjoints of sigmoid + level accumulation, and of the projection
+    if (c.T > 0) {
+        accum_sigmoid_backward_kernel<<<tb, kPrepWarps * 32, 0, st>>>(c.T, c.min_level, c.max_level, c.max_level, S,
+                                                                      ST, 1, w.alpha_acc, w.grad_alpha_acc,
+                                                                      grad_alpha_src);
+        accum_sigmoid_backward_kernel<<<tb, kPrepWarps * 32, 0, st>>>(c.T, c.min_level, c.max_level, c.max_level, S,
+                                                                      ST, c.C, w.feat_acc, w.grad_feat_acc,
+                                                                      grad_feat_src);
+    }
+    if (c.V > 0) project_backward_kernel<<<blocks_for(c.V), kThreads, 0, st>>>(c.B, c.V, mvp, w.grad_pos, grad_verts);
+    finish_kernel<<<1, 32, 0, st>>>(w.loss_sum, a.inv_n, loss, c.stochastic ? rng : nullptr);
+    if ((rc = mark(7, st))) return rc;
+    return check_launch("train_step");
+}
+
+}  // extern "C"

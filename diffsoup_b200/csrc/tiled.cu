@@ -248,7 +248,11 @@ __global__ void __launch_bounds__(kTileThreads) aux_kernel(int B, const ds_view_
             const float4 rp = reinterpret_cast<const float4*>(rast)[g.pix];
             tp = (int)rp.w - 1;
             zp = rp.z;
-            for (int c = 0; c < C; ++c) loss += fabsf(color[g.pix * C + c] - target[g.pix * C + c]);
+            if (target != nullptr) {
+                for (int c = 0; c < C; ++c) loss += fabsf(color[g.pix * C + c] - target[g.pix * C + c]);
+            } else {
+                loss = color[g.pix];  // caller passes the per-pixel sum |c - target| directly
+            }
         }
         for (int64_t c0 = g.begin; c0 < g.end; c0 += kTileThreads) {
             const int n = (int)min((int64_t)kTileThreads, g.end - c0);
@@ -381,6 +385,7 @@ int ds_tiles_opacity_aux(int B, const ds_view_desc* views, int num_tiles, int V,
     if (rc) return rc;
     DS_CHECK_ARG(level >= 0 && level <= 12 && (uint32_t)S == feats_at_level(level), "Invalid feature size.");
     DS_CHECK_ARG(C > 0, "tiles_opacity_aux: C must be positive");
+    DS_CHECK_ARG(target != nullptr || C == 1, "tiles_opacity_aux: without a target, color holds one value per pixel");
     DS_CHECK_ARG(((uintptr_t)rast & 15) == 0, "tiles_opacity_aux: rast not 16-byte aligned");
     if (num_tiles == 0) return DS_OK;
     cudaStream_t st = (cudaStream_t)stream;

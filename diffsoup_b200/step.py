@@ -1,0 +1,173 @@
+"""Batched training step: the whole forward+backward of one DiffSoup
+optimisation step for many views in one graph-capturable call.
+
+`TrainStep` wraps ds_train_step (csrc/step.cu) of the C ABI.  It computes,
+for a batch of views that may differ in resolution, what
+examples/02_synthetic.py:354-385 computes with an MSE photometric loss:
+
+    alpha = sigmoid(accumulate_to_level(lo, hi, alpha_src))
+    feat  = sigmoid(accumulate_to_level(lo, hi, feat_src))
+    pos   = project_vertices(verts, mvp)
+    rast  = rasterize_multires_triangle_alpha((H, W), pos, tri, hi, alpha)
+    x     = cat(multires_triangle_color(rast, hi, feat), view_dir(rast))
+    color = mask * ColorMLP(x, mask) + (1 - mask)
+    loss  = opacity_aux_loss(...) + mse(edge_grad(color, ...), target)
+
+and the gradients of loss with respect to verts, feat_src, alpha_src and the
+MLP parameters.  The shading MLP runs in BF16 on the tensor cores with FP32
+accumulation, features are gathered in BF16; coverage, depth and the
+triangle-ID buffer are exact FP32 as in the reference.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import torch
+from torch import nn
+
+from . import _core
+from . import tiles as _tiles
+
+
+class StepConfig(C.Structure):
+    _fields_ = [("B", C.c_int32), ("T", C.c_int32), ("V", C.c_int32), ("C", C.c_int32), ("min_level", C.c_int32),
+                ("max_level", C.c_int32), ("hidden", C.c_int32), ("n_layers", C.c_int32),
+                ("stochastic", C.c_int32), ("thr_const", C.c_float)]
+
+
+_L = _core.lib
+_L.ds_mlp_param_count.restype = C.c_int
+_L.ds_mlp_param_count.argtypes = [C.c_int, C.c_int, C.c_int]
+_L.ds_train_step_workspace_size.restype = C.c_size_t
+_L.ds_train_step_workspace_size.argtypes = [C.POINTER(StepConfig), C.c_int, C.c_int64, C.c_int64]
+_L.ds_train_step_layout.restype = C.c_int
+_L.ds_train_step_layout.argtypes = [C.POINTER(StepConfig), C.c_int, C.c_int64, C.c_int64, C.POINTER(C.c_int64)]
+_vp = C.c_void_p
+_L.ds_train_step.restype = C.c_int
+# cfg, views, num_tiles, num_pixels, 17 device pointers (verts .. workspace), bytes, capacity, status, stream
+_L.ds_train_step.argtypes = ([C.POINTER(StepConfig), _vp, C.c_int, C.c_int64] + [_vp] * 17
+                             + [C.c_size_t, C.c_int64, _vp, _vp])
+
+_L.ds_train_step_set_events.restype = C.c_int
+_L.ds_train_step_set_events.argtypes = [C.c_void_p, C.c_int]
+
+LAYOUT = ["pos", "alpha_acc", "feat_acc", "feat_bf16", "rast", "color", "grad_color", "l1", "grad_pos",
+          "grad_alpha_acc", "grad_feat_acc"]
+
+
+def mlp_param_count(C_: int, hidden: int, n_layers: int) -> int:
+    return int(_L.ds_mlp_param_count(C_, hidden, n_layers))
+
+
+def pack_mlp(mlp: nn.Module) -> torch.Tensor:
+    """Flatten a ColorMLP's Linear layers as [W0, b0, ..., Wout, bout] (fp32)."""
+    lins = [m for m in mlp.modules() if isinstance(m, nn.Linear)]
+    return torch.cat([t.detach().reshape(-1).float() for lin in lins for t in (lin.weight, lin.bias)]).contiguous()
+
+
+def unpack_mlp_grads(flat: torch.Tensor, mlp: nn.Module) -> None:
+    """Write a packed gradient into the .grad of a ColorMLP's parameters."""
+    o = 0
+    for lin in [m for m in mlp.modules() if isinstance(m, nn.Linear)]:
+        for p in (lin.weight, lin.bias):
+            n = p.numel()
+            p.grad = flat[o:o + n].view_as(p).clone()
+            o += n
+
+
+class TrainStep:
+    """Workspace and launch state of the batched training step for a fixed
+    batch layout (triangle count, vertex count, view resolutions)."""
+
+    def __init__(self, T: int, V: int, hw: Sequence[Tuple[int, int]], C_: int, min_level: int, max_level: int,
+                 hidden: int, n_layers: int, stochastic: bool = True, seed: int = 0,
+                 device: Optional[torch.device] = None, list_capacity: Optional[int] = None):
+        self.device = torch.device(device or "cuda")
+        self.hw = [(int(h), int(w)) for h, w in hw]
+        self.B = len(self.hw)
+        self.cfg = StepConfig(self.B, T, V, C_, min_level, max_level, hidden, n_layers, int(stochastic), 0.5)
+        self.views, self.num_tiles, self.num_pixels, self.pix_offsets = _tiles.view_table(self.hw, self.device)
+        self.S = sum(_core.feats_at_level(l) for l in range(min_level, max_level + 1))
+        self.nparam = mlp_param_count(C_, hidden, n_layers)
+        self.rng = torch.tensor([seed, 0], dtype=torch.int64, device=self.device)
+        self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self.loss = torch.zeros(1, dtype=torch.float32, device=self.device)
+        self.grad_verts = torch.zeros(V, 3, device=self.device)
+        self.grad_feat_src = torch.zeros(T, self.S, C_, device=self.device)
+        self.grad_alpha_src = torch.zeros(T, self.S, device=self.device)
+        self.grad_mlp = torch.zeros(self.nparam, device=self.device)
+        self.capacity = int(list_capacity or max(1 << 16, 8 * self.B * T))
+        self._alloc()
+        self.graph: Optional[torch.cuda.CUDAGraph] = None
+
+    def _alloc(self) -> None:
+        nb = int(_L.ds_train_step_workspace_size(C.byref(self.cfg), self.num_tiles, self.num_pixels, self.capacity))
+        self.workspace = torch.empty(nb, dtype=torch.uint8, device=self.device)
+        offs = (C.c_int64 * 11)()
+        _core.check(_L.ds_train_step_layout(C.byref(self.cfg), self.num_tiles, self.num_pixels, self.capacity, offs))
+        self.offsets = {k: int(offs[i]) for i, k in enumerate(LAYOUT)}
+
+    def intermediate(self, name: str) -> torch.Tensor:
+        """A view of one workspace intermediate (valid after a step)."""
+        c = self.cfg
+        ST = _core.feats_at_level(c.max_level)
+        shapes: Dict[str, Tuple[torch.dtype, Tuple[int, ...]]] = {
+            "pos": (torch.float32, (c.B, c.V, 4)), "alpha_acc": (torch.float32, (c.T, ST)),
+            "feat_acc": (torch.float32, (c.T, ST, c.C)), "feat_bf16": (torch.bfloat16, (c.T, ST, c.C)),
+            "rast": (torch.float32, (self.num_pixels, 4)), "color": (torch.float32, (self.num_pixels, 3)),
+            "grad_color": (torch.float32, (self.num_pixels, 3)), "l1": (torch.float32, (self.num_pixels,)),
+            "grad_pos": (torch.float64, (c.B, c.V, 4)), "grad_alpha_acc": (torch.float32, (c.T, ST)),
+            "grad_feat_acc": (torch.float32, (c.T, ST, c.C)),
+        }
+        dt, shp = shapes[name]
+        n = 1
+        for s in shp:
+            n *= s
+        o = self.offsets[name]
+        nbytes = n * torch.tensor([], dtype=dt).element_size()
+        return self.workspace[o:o + nbytes].view(dt).view(shp)
+
+    def run(self, verts: torch.Tensor, tri: torch.Tensor, mvp: torch.Tensor, inv_mvp: torch.Tensor,
+            feat_src: torch.Tensor, alpha_src: torch.Tensor, mlp_params: torch.Tensor, target: torch.Tensor,
+            rast_out: Optional[torch.Tensor] = None, color_out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        """Enqueue one step on the current stream; returns the device loss."""
+        p = _core.ptr
+        _core.check(_L.ds_train_step(C.byref(self.cfg), p(self.views), self.num_tiles, self.num_pixels, p(verts),
+                                     p(tri), p(mvp), p(inv_mvp), p(feat_src), p(alpha_src), p(mlp_params), p(target),
+                                     p(self.rng), p(self.loss), p(self.grad_verts), p(self.grad_feat_src),
+                                     p(self.grad_alpha_src), p(self.grad_mlp), p(rast_out), p(color_out),
+                                     p(self.workspace), self.workspace.numel(), self.capacity, p(self.status),
+                                     _core.stream()))
+        return self.loss
+
+    def overflowed(self) -> bool:
+        """True when a tile list outgrew its capacity (results stay exact; the
+        affected tiles ran the exhaustive path).  Synchronises on the status."""
+        return bool(int(self.status.item()) & _tiles.DS_STATUS_LIST_OVERFLOW)
+
+    def fit_capacity(self, *args, **kwargs) -> None:
+        """Run eager steps, doubling the tile-list capacity until it fits."""
+        for _ in range(16):
+            self.status.zero_()
+            self.run(*args, **kwargs)
+            if not self.overflowed():
+                return
+            self.capacity *= 2
+            self._alloc()
+        raise RuntimeError("tile list capacity did not converge")
+
+    def capture(self, *args, **kwargs) -> torch.cuda.CUDAGraph:
+        """Capture one step over fixed buffers into a CUDA graph (replay with
+        self.graph.replay() after refreshing the input buffers in place)."""
+        s = torch.cuda.Stream(self.device)
+        s.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(s):
+            self.run(*args, **kwargs)  # warm-up outside capture (sets kernel attributes)
+        torch.cuda.current_stream(self.device).wait_stream(s)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.run(*args, **kwargs)
+        self.graph = g
+        return g

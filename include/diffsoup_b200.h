@@ -187,6 +187,66 @@ int ds_tiles_opacity_aux(int B, const ds_view_desc* views, int num_tiles, int V,
                          const float* target, const float* rast, float scale, float* grad_alpha_src,
                          void* workspace, size_t workspace_bytes, int64_t list_capacity, ds_stream_t stream);
 
+/* ===================================================================== */
+/*  Batched training step                                                 */
+/* ===================================================================== */
+
+/* One training step of examples/02_synthetic.py:354-388 with an MSE
+ * photometric loss, for B views at once:
+ *   alpha = sigmoid(accumulate_to_level(min..max -> max, alpha_src))
+ *   feat  = sigmoid(accumulate_to_level(min..max -> max, feat_src))
+ *   pos   = project(verts, mvp)                                (utils.py:412-426)
+ *   rast  = rasterize_multires_triangle_alpha(pos, tri, max, alpha, stochastic)
+ *   x     = [multires_triangle_color(rast, feat), view_dir(rast, inv_mvp)]
+ *   color = mask ? ColorMLP(x) : 1;  loss = mean((color - target)^2)
+ *           + opacity_aux_loss(...) + edge_grad(...)   (zero-valued hooks)
+ * and the gradients of loss with respect to verts, feat_src, alpha_src and
+ * the MLP parameters (overwritten, not accumulated).  The MLP runs in BF16 on
+ * the tensor cores with FP32 accumulation; features are gathered as BF16.
+ * Never host-synchronising; capturable in a CUDA graph.  With stochastic
+ * opacity, rng = device uint64[2] {seed, iteration} and the iteration is
+ * incremented on the device at the end of the step. */
+typedef struct {
+    int32_t B, T, V;         /* views, triangles, vertices */
+    int32_t C;               /* feature channels */
+    int32_t min_level, max_level;
+    int32_t hidden, n_layers;/* shading MLP: (C+3) -> hidden x n_layers -> 3 */
+    int32_t stochastic;      /* 1: Philox threshold per (view, pixel, triangle); 0: thr_const */
+    float thr_const;
+} ds_step_config;
+
+/* Packed MLP parameter layout (fp32): W0[hidden][C+3] b0[hidden]
+ * (Wl[hidden][hidden] bl[hidden]) x (n_layers-1) Wout[3][hidden] bout[3],
+ * i.e. torch.nn.Linear weights in ColorMLP order. */
+int ds_mlp_param_count(int C, int hidden, int n_layers);
+
+size_t ds_train_step_workspace_size(const ds_step_config* cfg, int num_tiles, int64_t num_pixels,
+                                    int64_t list_capacity);
+
+/* Profiling hook: while set, ds_train_step records events[i] (cudaEvent_t)
+ * on its stream at the phase boundaries start | prep | bin | raster | shade |
+ * aux | edge | end (n <= 8; n = 0 disables). */
+int ds_train_step_set_events(void* const* events, int n);
+
+/* Byte offsets inside the train-step workspace of its intermediates, for
+ * inspection after a step: [0] pos [B,V,4] f32, [1] opacity [T,S_max] f32,
+ * [2] features [T,S_max,C] f32, [3] features bf16, [4] rast [pixels,4],
+ * [5] colour [pixels,3], [6] dL/dcolour [pixels,3], [7] |c - target| summed
+ * [pixels], [8] dL/dpos [B,V,4] f64, [9] dL/dopacity, [10] dL/dfeatures. */
+int ds_train_step_layout(const ds_step_config* cfg, int num_tiles, int64_t num_pixels, int64_t list_capacity,
+                         int64_t* offsets);
+
+/* verts [V,3], tri [T,3], mvp/inv_mvp [B,4,4], feat_src [T,S,C],
+ * alpha_src [T,S], target [pixels,3] (views packed by ds_view_desc),
+ * loss [1]; grad_* match their parameters.  rast_out [pixels,4] and
+ * color_out [pixels,3] are optional (NULL: kept in the workspace). */
+int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_tiles, int64_t num_pixels,
+                  const float* verts, const int* tri, const float* mvp, const float* inv_mvp, const float* feat_src,
+                  const float* alpha_src, const float* mlp_params, const float* target, uint64_t* rng, float* loss,
+                  float* grad_verts, float* grad_feat_src, float* grad_alpha_src, float* grad_mlp_params,
+                  float* rast_out, float* color_out, void* workspace, size_t workspace_bytes, int64_t list_capacity,
+                  int* status, ds_stream_t stream);
+
 /* 3-D view direction per covered pixel (compute_view_direction of
  * src/cuda/encoding.cu:28-53, which the reference does not export): enc [B,H,W,3]. */
 int ds_encode_view_dir(int B, int H, int W, const float* rast, const float* inv_mvp, float* encoding,

@@ -64,7 +64,9 @@ def _declare(L: C.CDLL) -> None:
     L.orc_fragment_thresholds.argtypes = [i64, vp, vp, i32, i32, u64, u32, vp]
     L.orc_depth_test.argtypes = [i32, i32, i32, i64, vp, vp, vp, vp, vp]
     L.orc_rasterize_alpha.restype = i64
-    L.orc_rasterize_alpha.argtypes = [i32, i32, i32, i32, i32, vp, i32, vp, i32, vp, i32, u64, u32, vp]
+    L.orc_rasterize_alpha.argtypes = [i32, i32, i32, i32, i32, vp, i32, vp, i32, vp, i32, u64, u32, i32, vp]
+    L.orc_project_f32.argtypes = [i32, i32, vp, vp, vp]
+    L.orc_accumulate_sigmoid_f32.argtypes = [i32, i32, i32, i32, i32, vp, vp]
     L.orc_multires_color_f32.argtypes = [i32, i32, i32, i32, vp, i32, i32, i32, vp, vp]
     L.orc_multires_color_f64.argtypes = [i32, i32, i32, vp, i32, i32, i32, vp, vp]
     L.orc_multires_color_backward.argtypes = [i32, i32, i32, vp, i32, i32, i32, vp, vp]
@@ -187,8 +189,26 @@ def depth_test(B: int, H: int, W: int, frag_pix, frag_attrs, frag_alpha, alpha_t
     return rast
 
 
+def project(verts, mvp) -> np.ndarray:
+    """Clip positions [B,V,4] with the product step's fused evaluation order."""
+    v, m = f32(verts), f32(mvp)
+    B, V = m.shape[0], v.shape[0]
+    out = np.zeros((B, V, 4), np.float32)
+    lib().orc_project_f32(B, V, _p(v), _p(m), _p(out))
+    return out
+
+
+def accumulate_sigmoid_f32(lo: int, hi: int, target: int, feat) -> np.ndarray:
+    """sigmoid(accumulate_to_level(lo, hi, feat, target)) in FP32."""
+    ft = f32(feat)
+    T, _, Cd = ft.shape
+    out = np.zeros((T, int(lib().orc_feats_at_level(target)), Cd), np.float32)
+    lib().orc_accumulate_sigmoid_f32(T, lo, hi, target, Cd, _p(ft), _p(out))
+    return out
+
+
 def rasterize_alpha(H: int, W: int, pos, tri, level: int, alpha_src, stochastic: bool = False, seed: int = 0,
-                    iteration: int = 0, variant: int = REF_VARIANT) -> Tuple[np.ndarray, int]:
+                    iteration: int = 0, variant: int = REF_VARIANT, view0: int = 0) -> Tuple[np.ndarray, int]:
     """rasterize_multires_triangle_alpha (multires.py:52-102) with the opacity
     threshold of each fragment taken from `fragment_thresholds`.  Returns
     (rast [B,H,W,4], number of covered fragments)."""
@@ -196,7 +216,7 @@ def rasterize_alpha(H: int, W: int, pos, tri, level: int, alpha_src, stochastic:
     B, V, _ = pos.shape
     rast = np.zeros((B, H, W, 4), np.float32)
     nf = lib().orc_rasterize_alpha(variant, H, W, B, V, _p(pos), tri.shape[0], _p(tri), level, _p(asrc),
-                                   int(stochastic), seed, iteration, _p(rast))
+                                   int(stochastic), seed, iteration, view0, _p(rast))
     return rast, int(nf)
 
 

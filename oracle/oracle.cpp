@@ -448,7 +448,7 @@ void orc_depth_test(int B, int H, int W, int64_t nf, const int* frag_pix, const 
 // Returns the number of covered fragments (before the depth test).
 int64_t orc_rasterize_alpha(int variant, int H, int W, int B, int V, const float* pos, int T,
                             const int* tri, int level, const float* alpha_src, int stochastic,
-                            uint64_t seed, uint32_t iter, float* rast) {
+                            uint64_t seed, uint32_t iter, int view0, float* rast) {
     int64_t total_frags = 0;
     const int64_t npix = (int64_t)H * W;
     for (int b = 0; b < B; ++b) {
@@ -462,7 +462,7 @@ int64_t orc_rasterize_alpha(int variant, int H, int W, int B, int V, const float
         std::vector<int> cpix((size_t)nbb * 3);
         std::vector<float> cattr((size_t)nbb * 4);
         const int64_t nf = orc_filter_valid(nbb, fpix.data(), fattr.data(), cpix.data(), cattr.data());
-        for (int64_t i = 0; i < nf; ++i) cpix[i * 3] = b;
+        for (int64_t i = 0; i < nf; ++i) cpix[i * 3] = view0 + b;
         std::vector<float> alpha((size_t)nf, 0.f), thr((size_t)nf);
         orc_multires_alpha(variant, nf, cattr.data(), level, level, alpha_src, alpha.data());
         orc_fragment_thresholds(nf, cpix.data(), cattr.data(), W, stochastic, seed, iter, thr.data());
@@ -868,6 +868,29 @@ void orc_opacity_aux(int variant, int f64, int B, int H, int W, int C, const voi
         }
         orc_multires_alpha_backward(nf, cattr.data(), level, level, T, grad_alpha_src, gfa.data());
     }
+}
+
+// Projection of the batched training step (examples/utils.py:412-426) with the
+// fixed fused order of the product kernel: ((M[r][3] + M[r][0] x) + M[r][1] y)
+// + M[r][2] z, each step one fma.
+void orc_project_f32(int B, int V, const float* verts, const float* mvp, float* pos) {
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)B * V; ++i) {
+        const int b = (int)(i / V), v = (int)(i % V);
+        const float* M = mvp + (size_t)b * 16;
+        const float x = verts[(size_t)v * 3], y = verts[(size_t)v * 3 + 1], z = verts[(size_t)v * 3 + 2];
+        for (int r = 0; r < 4; ++r)
+            pos[i * 4 + r] = std::fma(M[r * 4 + 2], z, std::fma(M[r * 4 + 1], y, std::fma(M[r * 4 + 0], x, M[r * 4 + 3])));
+    }
+}
+
+// Level accumulation + sigmoid as the product's step computes it in FP32
+// (accumulate_to_level then torch.sigmoid, examples/02_synthetic.py:355-356).
+void orc_accumulate_sigmoid_f32(int T, int lo, int hi, int target, int C, const float* feat, float* out) {
+    orc_accumulate_forward_f32(64 | 0, T, lo, hi, target, C, feat, out);
+    const int64_t n = (int64_t)T * feats_at_level((uint32_t)target) * C;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) out[i] = 1.f / (1.f + std::exp(-out[i]));
 }
 
 // Exposes the coverage test for contraction-variant pinning.

@@ -62,3 +62,21 @@ def test_view_table_and_argument_errors():
     assert rc == 1 and lib.ds_last_error() == b"Invalid feature size."
     with pytest.raises(RuntimeError, match="Invalid feature size"):
         _core.check(rc)
+
+
+def test_train_step_binding_argument_errors():
+    """ds_train_step's ctypes signature matches the header: an invalid batch is
+    rejected on the host with DS_ERR_ARG before any device work."""
+    import ctypes as C
+    from diffsoup_b200 import step as S
+    from diffsoup_b200 import _core
+
+    cfg = S.StepConfig(0, 10, 30, 8, 0, 2, 16, 1, 1, 0.5)
+    null = C.c_void_p(0)
+    rc = S._L.ds_train_step(C.byref(cfg), null, 0, 0, *([null] * 17), 0, 0, null, null)
+    assert rc == 1 and b"bad sizes" in _core.lib.ds_last_error()
+    cfg = S.StepConfig(2, 10, 30, 7, 0, 2, 16, 1, 0, 0.5)
+    rc = S._L.ds_train_step(C.byref(cfg), null, 4, 100, *([null] * 17), 0, 0, null, null)
+    assert rc == 1 and b"unsupported MLP" in _core.lib.ds_last_error()
+    assert S.mlp_param_count(8, 16, 1) == 16 * 11 + 16 + 3 * 16 + 3
+    assert S.mlp_param_count(16, 64, 2) == 64 * 19 + 64 + 64 * 64 + 64 + 3 * 64 + 3

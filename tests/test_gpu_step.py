@@ -1,0 +1,122 @@
+"""The batched BF16 training step against the FP64 oracle of the same step.
+
+Discrete outputs (clip positions, ID buffer) must match the oracle bit for bit
+given the step's own FP32 opacities.  Continuous outputs are compared with the
+FP64 oracle: image RMS error <= 1e-3 (the precision target), loss to 1e-3
+relative, and each gradient group to the relative L2 error recorded in
+GRAD_TOL (BF16 features and MLP; the values are printed for the report).
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from diffsoup_b200 import scenes
+from diffsoup_b200.step import TrainStep, pack_mlp
+from oracle import cpu
+from oracle import pipeline as P
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda"
+GRAD_TOL = {"grad_verts": 3e-2, "grad_feat_src": 2e-2, "grad_alpha_src": 2e-2, "mlp": 2e-2}
+
+
+def rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+def _mlp_flat(mlp):
+    return torch.from_numpy(np.concatenate([np.concatenate([W.reshape(-1), b]) for W, b in mlp])).float()
+
+
+def _setup(config, seed, **kw):
+    sc = scenes.make_scene(config, seed=seed, **kw)
+    hw = [(v.height, v.width) for v in sc.views]
+    # per-view projection (views may have different aspect ratios)
+    mlp = scenes.mlp_weights(sc.mlp_input_dim, 3, sc.hidden_dim, sc.n_layers, seed=seed)
+    inp = P.StepInputs(verts=sc.verts, tri=sc.tri, mvps=sc.mvps(), inv_mvps=sc.inv_mvps(), hw=hw,
+                       feat_src=sc.feat_src, alpha_src=sc.alpha_src[..., 0], mlp=mlp, targets=sc.targets,
+                       min_level=sc.min_level, max_level=sc.max_level, stochastic=True, seed=4242, iteration=0)
+    step = TrainStep(sc.T, sc.verts.shape[0], hw, sc.feat_dim, sc.min_level, sc.max_level, sc.hidden_dim,
+                     sc.n_layers, stochastic=True, seed=4242)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(DEV)  # noqa: E731
+    dev_inputs = dict(verts=t(sc.verts), tri=t(sc.tri), mvp=t(sc.mvps()), inv_mvp=t(sc.inv_mvps()),
+                      feat_src=t(sc.feat_src), alpha_src=t(sc.alpha_src[..., 0]), mlp_params=_mlp_flat(mlp).to(DEV),
+                      target=t(np.concatenate([x.reshape(-1, 3) for x in sc.targets])))
+    return sc, hw, inp, step, dev_inputs
+
+
+@pytest.mark.parametrize("config,seed,kw", [
+    (1, 0, dict(num_tris=1500, num_views=2, resolution=(96, 128))),
+    (2, 1, dict(num_tris=3000, num_views=3, resolution=(160, 160))),
+    (3, 2, dict(num_tris=2000, num_views=3)),
+    (4, 3, dict(num_tris=800, num_views=2, resolution=(80, 96))),
+])
+def test_train_step_matches_fp64_oracle(config, seed, kw):
+    sc, hw, inp, step, d = _setup(config, seed, **kw)
+    rast = torch.empty(step.num_pixels, 4, device=DEV)
+    color = torch.empty(step.num_pixels, 3, device=DEV)
+    loss = step.run(**d, rast_out=rast, color_out=color)
+    torch.cuda.synchronize()
+    assert not step.overflowed()
+    # discrete path: positions and ID buffer bit-exact with the oracle
+    pos = step.intermediate("pos").cpu().numpy()
+    assert np.array_equal(pos.view(np.uint32), cpu.project(sc.verts, sc.mvps()).view(np.uint32))
+    alpha32 = step.intermediate("alpha_acc").cpu().numpy()
+    want_alpha = cpu.accumulate_sigmoid_f32(sc.min_level, sc.max_level, sc.max_level, sc.alpha_src)[..., 0]
+    np.testing.assert_allclose(alpha32, want_alpha, rtol=0, atol=3e-7)
+    r = rast.cpu().numpy()
+    rasts = []
+    for b, (H, W) in enumerate(hw):
+        o = step.pix_offsets[b]
+        got = r[o:o + H * W].reshape(1, H, W, 4)
+        want, _ = cpu.rasterize_alpha(H, W, pos[b:b + 1], sc.tri, sc.max_level, alpha32, True, 4242, 0, view0=b)
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), f"view {b} ID buffer differs"
+        rasts.append(got)
+    # continuous path against the FP64 oracle on the same ID buffer
+    ref = P.train_step(inp, "f64", rast_in=rasts, pos32=pos, alpha32=alpha32)
+    c = color.cpu().numpy()
+    sq = [(c[step.pix_offsets[b]:step.pix_offsets[b] + H * W] - ref.color[b].reshape(-1, 3)) ** 2
+          for b, (H, W) in enumerate(hw)]
+    rms = float(np.sqrt(np.concatenate(sq).mean()))
+    errs = {
+        "loss": abs(float(loss.item()) - ref.loss) / ref.loss,
+        "image_rms": rms,
+        "grad_verts": rel(step.grad_verts.cpu().numpy(), ref.grad_verts),
+        "grad_feat_src": rel(step.grad_feat_src.cpu().numpy(), ref.grad_feat_src),
+        "grad_alpha_src": rel(step.grad_alpha_src.cpu().numpy(), ref.grad_alpha_src),
+        "mlp": rel(step.grad_mlp.cpu().numpy(), np.concatenate([np.concatenate([W.reshape(-1), b]) for W, b in ref.grad_mlp])),
+    }
+    print(f"config{config} errors vs FP64 oracle: " + ", ".join(f"{k}={v:.2e}" for k, v in errs.items()))
+    assert errs["image_rms"] <= 1e-3
+    assert errs["loss"] <= 1e-3
+    for k, tol in GRAD_TOL.items():
+        assert errs[k] <= tol, (k, errs[k])
+
+
+def test_train_step_graph_replay():
+    sc, hw, inp, step, d = _setup(1, 5, num_tris=1000, num_views=2, resolution=(64, 64))
+    step.run(**d)
+    torch.cuda.synchronize()
+    l0 = float(step.loss.item())
+    it0 = int(step.rng[1].item())
+    g = step.capture(**d)
+    losses = []
+    for _ in range(3):
+        g.replay()
+        torch.cuda.synchronize()
+        losses.append(float(step.loss.item()))
+    # the warm-up inside capture() advances the iteration once; capture itself runs nothing
+    assert int(step.rng[1].item()) == it0 + 4
+    assert all(np.isfinite(losses)) and abs(losses[0] - l0) / l0 < 0.05
+    # a replay equals an eager step with the same RNG state
+    step.rng[1] = 77
+    g.replay()
+    torch.cuda.synchronize()
+    gv_graph = step.grad_verts.clone()
+    step.rng[1] = 77
+    step.run(**d)
+    torch.cuda.synchronize()
+    assert rel(step.grad_verts.cpu().numpy(), gv_graph.cpu().numpy()) < 1e-5
