@@ -80,6 +80,18 @@ int ds_depth_test(int B, int H, int W, int num_frags, const int* frag_pix, const
                   const float* frag_alpha, const float* alpha_thresh, float* rast, void* workspace,
                   size_t workspace_bytes, ds_stream_t stream);
 
+/* No counterpart in the reference: the depth test of ds_depth_test for
+ * callers that cannot allocate device memory (an embedding application that
+ * owns all device memory, a fixed memory budget, or a loop that cannot pay for
+ * cudaMalloc/cudaFree).  It allocates nothing: its 8-byte-per-pixel depth
+ * keys live in a fixed __device__ buffer of this library, so B*H*W is limited
+ * to 2^21 pixels (larger batches return DS_ERR_ARG).  All calls on a device
+ * share that buffer (each clears what it uses); calls whose GPU work overlaps
+ * race on it.  The first call on each device looks up the buffer's address
+ * (cudaGetSymbolAddress); make it before any stream capture. */
+int ds_depth_test_noalloc(int B, int H, int W, int num_frags, const int* frag_pix, const float* frag_attrs,
+                          const float* frag_alpha, const float* alpha_thresh, float* rast, ds_stream_t stream);
+
 /* replaces _core.backward_edge_grad (src/main.cpp:112-130, rasterize.cu:653-921).
  * grad_pos [B,V,4] accumulates. */
 int ds_backward_edge_grad(int B, int H, int W, int C, const float* color, const float* grad_color,
