@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--views", type=int, default=8, help="views per step (8 is the benchmark workload; "
+                    "fewer only for small profiling cases)")
     return ap.parse_args()
 
 
@@ -112,7 +114,7 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # workload
 # ---------------------------------------------------------------------------
-def make_inputs(rank: int):
+def make_inputs(rank: int, nviews: int = 8):
     from diffsoup_b200 import scenes
 
     sc = scenes.make_scene(2, seed=0, with_targets=False)
@@ -122,13 +124,13 @@ def make_inputs(rank: int):
     for r in range(N_INPUT_SETS):
         phase = 2 * math.pi * (rank * N_INPUT_SETS + r) / (8 * N_INPUT_SETS * 64)
         views = []
-        for i in range(8):
+        for i in range(nviews):
             th = 2 * math.pi * i / 8 + phase
             eye = np.array([4 * math.cos(th), 4 * math.sin(th), 1.2])
             views.append(scenes._make_view(eye, 800, 800))
         mvp = np.stack([v.mvp for v in views]).astype(np.float32)
         inv = np.stack([v.inv_mvp for v in views]).astype(np.float32)
-        tgt = rng.uniform(0, 1, size=(8 * 800 * 800, 3)).astype(np.float32)
+        tgt = rng.uniform(0, 1, size=(nviews * 800 * 800, 3)).astype(np.float32)
         sets.append((mvp, inv, tgt))
     return sc, mlp, sets
 
@@ -215,8 +217,8 @@ def run_ours(args):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
 
-    sc, mlp, sets = make_inputs(rank)
-    B, T, V = 8, sc.T, sc.verts.shape[0]
+    sc, mlp, sets = make_inputs(rank, args.views)
+    B, T, V = args.views, sc.T, sc.verts.shape[0]
     hw = [(800, 800)] * B
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
     verts, tri = t(sc.verts), t(sc.tri)
@@ -365,7 +367,7 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": "views/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "bf16", "data": "synthetic (seeded; stands in for the reference datasets)",
-        "config": {"workload": WORKLOAD, "views_per_step": B, "triangles": T, "resolution": "800x800",
+        "config": {"workload": WORKLOAD if B == 8 else WORKLOAD.replace("8 views", f"{B} views"), "views_per_step": B, "triangles": T, "resolution": "800x800",
                    "parallelism": f"replicas x{world}", "graph": "one CUDA graph per step",
                    "l2": f"{N_INPUT_SETS} rotating input sets (4 x 61 MB targets) larger than L2",
                    "list_overflow": overflow},
@@ -430,7 +432,7 @@ def run_plain(sc, mlp, s, dev, n_views: int):
             lin.weight.copy_(t(W))
             lin.bias.copy_(t(b))
     mvps, invs = t(mvp), t(inv)
-    tg = t(tgt.reshape(8, 800, 800, 3))
+    tg = t(tgt.reshape(-1, 800, 800, 3))
     lo, hi = sc.min_level, sc.max_level
 
     def one(b):
@@ -453,13 +455,14 @@ def run_plain(sc, mlp, s, dev, n_views: int):
         loss.backward()
         return loss
 
+    nb = mvps.shape[0]
     for i in range(4):
-        one(i % 8)
+        one(i % nb)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for i in range(n_views):
-        one(i % 8)
+        one(i % nb)
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
@@ -479,7 +482,7 @@ def run_cpu_baseline(sc, mlp, s):
         b = n % 8
         inp = P.StepInputs(verts=sc.verts, tri=sc.tri, mvps=mvp[b:b + 1], inv_mvps=inv[b:b + 1], hw=[(800, 800)],
                            feat_src=sc.feat_src, alpha_src=sc.alpha_src[..., 0], mlp=mlp,
-                           targets=[tgt.reshape(8, 800, 800, 3)[b]], min_level=sc.min_level, max_level=sc.max_level,
+                           targets=[tgt.reshape(-1, 800, 800, 3)[b]], min_level=sc.min_level, max_level=sc.max_level,
                            stochastic=True, seed=7, iteration=n)
         P.train_step(inp, "f32")
         n += 1
