@@ -47,7 +47,8 @@ __device__ __forceinline__ bool find_edge_intersection(const float4 P[3], float 
     else if (segment_intersect2d(x0, y0, x1, y1, rx[1], ry[1], rx[2], ry[2], ix, iy)) { i0 = 1; i1 = 2; }
     else if (segment_intersect2d(x0, y0, x1, y1, rx[2], ry[2], rx[0], ry[0], ix, iy)) { i0 = 2; i1 = 0; }
     else return false;
-    const float4 A = P[i0], Bv = P[i1];
+    const float4 A = i0 == 0 ? P[0] : (i0 == 1 ? P[1] : P[2]);
+    const float4 Bv = i1 == 0 ? P[0] : (i1 == 1 ? P[1] : P[2]);
     const float dx = Bv.x - A.x, dy = Bv.y - A.y, dw = Bv.w - A.w;
     const float ax = A.x - ix * A.w, ay = A.y - iy * A.w;
     const float bx = dx - ix * dw, by = dy - iy * dw;
@@ -111,12 +112,18 @@ __device__ __forceinline__ void add_mid_contrib(float mx, float my, const float4
 
 // Edge-gradient estimator of one pixel (rasterize.cu:663-892).  Pixel
 // buffers are addressed as base + y*W + x with `base` the view's first pixel;
-// P0 holds the view's clip positions.  Returns the pixel's triangle (or -1)
+// posb holds the view's clip positions.  Returns the pixel's triangle (or -1)
 // and its clip-space vertex gradients in acc.g[vertex*4 + xyzw].
+//
+// `pair_once`: an interior pair (both pixels on the same triangle) gives the
+// same contribution from either pixel (the adjoint and the pixel offset both
+// change sign), so with pair_once the pair is evaluated only from the pixel on
+// its left/bottom and counted twice; the caller then runs every pixel.
 __device__ __forceinline__ int edge_grad_pixel(int b, int y0, int x0, int H, int W, int C,
                                                const float* __restrict__ color, const float* __restrict__ grad_color,
                                                const float* __restrict__ rast, const float* __restrict__ posb,
-                                               const int* __restrict__ tri, int64_t base, EdgeAccum& acc) {
+                                               const int* __restrict__ tri, int64_t base, EdgeAccum& acc,
+                                               bool pair_once = false) {
     (void)b;
 #pragma unroll
     for (int k = 0; k < 12; ++k) acc.g[k] = 0.f;
@@ -133,27 +140,32 @@ __device__ __forceinline__ int edge_grad_pixel(int b, int y0, int x0, int H, int
     for (int k = 0; k < 3; ++k) P0[k] = load_vertex(posb, __ldg(tri + it0 * 3 + k));
     const float* c0 = color + pix0 * C;
     const float* g0 = grad_color + pix0 * C;
-    const int DY[4] = {0, 0, -1, 1}, DX[4] = {1, -1, 0, 0};
-#pragma unroll
+#pragma unroll 1
     for (int e = 0; e < 4; ++e) {
-        const int y1 = y0 + DY[e], x1 = x0 + DX[e];
+        // neighbour offsets (+x, -x, -y, +y) as in rasterize.cu:691-692
+        const int DX = (e == 0) - (e == 1);
+        const int DY = (e == 3) - (e == 2);
+        const int y1 = y0 + DY, x1 = x0 + DX;
         if (y1 < 0 || y1 >= H || x1 < 0 || x1 >= W) continue;
         const int64_t pix1 = base + (int64_t)y1 * W + x1;
         const float4 r1 = reinterpret_cast<const float4*>(rast)[pix1];
         const float depth1 = r1.z;
         const int it1 = (int)r1.w - 1;
+        const bool interior = it1 == it0;
+        if (pair_once && interior && (DX < 0 || DY < 0)) continue;  // counted by the neighbour
         const float* c1 = color + pix1 * C;
         const float* g1 = grad_color + pix1 * C;
         float adj = 0.f;
         for (int i = 0; i < C; ++i) adj += 0.5f * (g0[i] + g1[i]) * (c0[i] - c1[i]);
         if (adj == 0.f) continue;
-        const float gx = adj * (float)DX[e] * (float)W / 2.f;
-        const float gy = adj * (float)DY[e] * (float)H / 2.f;
+        const float gx = adj * (float)DX * (float)W / 2.f;
+        const float gy = adj * (float)DY * (float)H / 2.f;
         const float nx1 = -1.f + 2.f * ((float)x1 + 0.5f) / (float)W;
         const float ny1 = -1.f + 2.f * ((float)y1 + 0.5f) / (float)H;
         const float mx = 0.5f * (nx0 + nx1), my = 0.5f * (ny0 + ny1);
-        if (it1 == it0) {  // not an edge
-            add_mid_contrib(mx, my, P0, gx, gy, 0.f, false, acc);
+        if (interior) {  // not an edge
+            const float m = pair_once ? 2.f : 1.f;
+            add_mid_contrib(mx, my, P0, m * gx, m * gy, 0.f, false, acc);
             continue;
         }
         float tb0, tb1, cz1, cw1;
@@ -171,7 +183,7 @@ __device__ __forceinline__ int edge_grad_pixel(int b, int y0, int x0, int H, int
                         float nv[3], nf[3];
                         if (tri_normal_ndc(P0, nv) && tri_normal_ndc(P1, nf)) {
                             float gxn = 0.f, gyn = 0.f, gzn = 0.f;
-                            if (DX[e] != 0) {
+                            if (DX != 0) {
                                 float dbx, dbz;
                                 db_dp_2d(nv[0], nv[2], nf[0], nf[2], dbx, dbz);
                                 gxn = gx * dbx; gzn = gx * dbz;
@@ -191,14 +203,22 @@ __device__ __forceinline__ int edge_grad_pixel(int b, int y0, int x0, int H, int
             int i0, i1;
             float s0, s1;
             if (find_edge_intersection(P0, nx0, ny0, nx1, ny1, i0, i1, s0, s1)) {
-                const float cx = s0 * P0[i0].x + s1 * P0[i1].x;
-                const float cy = s0 * P0[i0].y + s1 * P0[i1].y;
-                const float cw = s0 * P0[i0].w + s1 * P0[i1].w;
+                const float4 A = i0 == 0 ? P0[0] : (i0 == 1 ? P0[1] : P0[2]);
+                const float4 Bv = i1 == 0 ? P0[0] : (i1 == 1 ? P0[1] : P0[2]);
+                const float cx = s0 * A.x + s1 * Bv.x;
+                const float cy = s0 * A.y + s1 * Bv.y;
+                const float cw = s0 * A.w + s1 * Bv.w;
                 const float iw = 1.f / cw, iw2 = iw * iw;
                 const float gsum = gx * cx + gy * cy;
-                acc.g[i0 * 4 + 0] += s0 * gx * iw; acc.g[i1 * 4 + 0] += s1 * gx * iw;
-                acc.g[i0 * 4 + 1] += s0 * gy * iw; acc.g[i1 * 4 + 1] += s1 * gy * iw;
-                acc.g[i0 * 4 + 3] += -s0 * gsum * iw2; acc.g[i1 * 4 + 3] += -s1 * gsum * iw2;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {  // static indices: no local-memory array
+                    const float s = k == i0 ? s0 : (k == i1 ? s1 : 0.f);
+                    if (k == i0 || k == i1) {
+                        acc.g[k * 4 + 0] += s * gx * iw;
+                        acc.g[k * 4 + 1] += s * gy * iw;
+                        acc.g[k * 4 + 3] += -s * gsum * iw2;
+                    }
+                }
                 acc.any = true;
             }
         }

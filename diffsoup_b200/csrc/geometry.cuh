@@ -66,25 +66,59 @@ __device__ __forceinline__ bool triangle_rect(int H, int W, float4 p0, float4 p1
     return true;
 }
 
-// Homogeneous 2D edge-function coverage test (rasterize.cu:170-206).
-// Writes barycentrics (b0, b1) and the interpolated clip z and w.
-__device__ __forceinline__ bool intersect_triangle(float ndc_y, float ndc_x, float4 p0, float4 p1, float4 p2,
-                                                   float& b0, float& b1, float& z, float& w) {
+// Homogeneous 2D edge-function coverage test (rasterize.cu:170-206), in two
+// stages so that a warp can skip the divisions when none of its lanes needs
+// them: edge_terms() gives the three edge functions and their sum,
+// surely_outside() rejects what the full test is certain to reject, and
+// finish_coverage() completes the reference's test bit for bit.
+__device__ __forceinline__ void edge_terms(float ndc_y, float ndc_x, float4 p0, float4 p1, float4 p2, float& A0,
+                                           float& A1, float& A2, float& A) {
     const float q0x = sub_mul(p0.x, ndc_x, p0.w), q0y = sub_mul(p0.y, ndc_y, p0.w);
     const float q1x = sub_mul(p1.x, ndc_x, p1.w), q1y = sub_mul(p1.y, ndc_y, p1.w);
     const float q2x = sub_mul(p2.x, ndc_x, p2.w), q2y = sub_mul(p2.y, ndc_y, p2.w);
-    const float A0 = cross2(q1x, q2y, q1y, q2x);
-    const float A1 = cross2(q2x, q0y, q2y, q0x);
-    const float A2 = cross2(q0x, q1y, q0y, q1x);
-    const float A = __fadd_rn(__fadd_rn(A0, A1), A2);
-    if (A == 0.f) return false;
-    const float invA = __fdiv_rn(1.f, A);
+    A0 = cross2(q1x, q2y, q1y, q2x);
+    A1 = cross2(q2x, q0y, q2y, q0x);
+    A2 = cross2(q0x, q1y, q0y, q1x);
+    A = __fadd_rn(__fadd_rn(A0, A1), A2);
+}
+
+// True only where the reference's test fails.  A == 0 is its own rejection.
+// Otherwise, with 2^-60 <= |A| <= 2^60 (so 1/A rounds to a normal float):
+//  * b0 = A0 * (1/A) is negative (and nonzero) when A0 has the sign opposite
+//    to A and |A0| > 2^-100 |A|; likewise b1;
+//  * b0 + b1 rounds above 1 when A2 has the sign opposite to A and
+//    |A2| > 2^-20 (|A| + |A0| + |A1|): from A = rn(rn(A0 + A1) + A2),
+//    (b0 + b1) >= (1 - 2u)(1 + k - 2u - uk - um) with u = 2^-24,
+//    k = -A2/A and m = (|A0| + |A1|)/|A|, which exceeds 1 once k > 16u(1 + m).
+__device__ __forceinline__ bool surely_outside(float A0, float A1, float A2, float A) {
+    if (A == 0.f) return true;
+    const float aA = fabsf(A);
+    if (!(aA >= 0x1p-60f && aA <= 0x1p60f)) return false;
+    const bool negA = A < 0.f;
+    if (A0 != 0.f && (A0 < 0.f) != negA && fabsf(A0) > aA * 0x1p-100f) return true;
+    if (A1 != 0.f && (A1 < 0.f) != negA && fabsf(A1) > aA * 0x1p-100f) return true;
+    if (A2 != 0.f && (A2 < 0.f) != negA && fabsf(A2) > 0x1p-20f * (aA + fabsf(A0) + fabsf(A1))) return true;
+    return false;
+}
+
+// Remainder of intersect_triangle given its edge terms (A != 0).
+__device__ __forceinline__ bool finish_coverage(float A0, float A1, float A, float4 p0, float4 p1, float4 p2,
+                                                float& b0, float& b1, float& z, float& w) {
+    const float invA = __frcp_rn(A);  // == 1.f / A, correctly rounded
     b0 = __fmul_rn(A0, invA);
     b1 = __fmul_rn(A1, invA);
     const float b2 = __fsub_rn(__fsub_rn(1.f, b0), b1);
     z = dot3_z(b0, p0.z, b1, p1.z, b2, p2.z);
     w = dot3_w(b0, p0.w, b1, p1.w, b2, p2.w);
     return b0 >= 0.f && b1 >= 0.f && __fadd_rn(b0, b1) <= 1.f;
+}
+
+__device__ __forceinline__ bool intersect_triangle(float ndc_y, float ndc_x, float4 p0, float4 p1, float4 p2,
+                                                   float& b0, float& b1, float& z, float& w) {
+    float A0, A1, A2, A;
+    edge_terms(ndc_y, ndc_x, p0, p1, p2, A0, A1, A2, A);
+    if (surely_outside(A0, A1, A2, A)) return false;
+    return finish_coverage(A0, A1, A, p0, p1, p2, b0, b1, z, w);
 }
 
 // Fragment test of compute_fragments (rasterize.cu:257-268): covered and

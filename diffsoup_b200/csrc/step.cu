@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(kThreads) project_backward_kernel(int B, int V
 // Edge gradients over packed views (rasterize.cu:653-903).  Consecutive
 // pixels of a row mostly share a triangle: a segmented warp reduction sums
 // runs of equal triangles before one FP64 atomic per vertex component.
-__global__ void __launch_bounds__(kThreads) edge_step_kernel(int B, const ds_view_desc* __restrict__ views,
+__global__ void __launch_bounds__(128) edge_step_kernel(int B, const ds_view_desc* __restrict__ views,
                                                              int64_t num_pixels, int V, const float* __restrict__ pos,
                                                              const int* __restrict__ tri,
                                                              const float* __restrict__ color,
@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(kThreads) edge_step_kernel(int B, const ds_vie
         const int64_t local = p - vd.pix_offset;
         const int y = (int)(local / vd.W), x = (int)(local % vd.W);
         it0 = edge_grad_pixel(b, y, x, vd.H, vd.W, 3, color, grad_color, rast, pos + (size_t)b * V * 4, tri,
-                              vd.pix_offset, acc);
+                              vd.pix_offset, acc, /*pair_once=*/true);
     }
     const int key = (it0 >= 0 && acc.any) ? it0 : -1 - lane;
     const int prev = __shfl_up_sync(0xffffffffu, key, 1);
@@ -378,7 +378,7 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     if (rc || (rc = mark(5, st))) return rc;
 
     // edge gradients to clip-space positions
-    edge_step_kernel<<<blocks_for(num_pixels), kThreads, 0, st>>>(c.B, views, num_pixels, c.V, w.pos, tri, a.color,
+    edge_step_kernel<<<blocks_for(num_pixels, 128), 128, 0, st>>>(c.B, views, num_pixels, c.V, w.pos, tri, a.color,
                                                                   w.grad_color, rast, w.grad_pos);
     if ((rc = mark(6, st))) return rc;
     // adjoints of sigmoid + level accumulation, and of the projection

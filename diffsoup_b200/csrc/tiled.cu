@@ -4,11 +4,14 @@
 // The reference enumerates one fragment per bbox pixel into global memory,
 // compacts it, and resolves depth with 64-bit atomics
 // (src/cuda/rasterize.cu:139-400).  Here each (view, triangle) is binned into
-// the 16x16 screen tiles its rect (rasterize.cu:43-137) overlaps; one CTA per
-// tile stages the tile's triangle records in shared memory, each warp skips
-// the triangles whose rect misses its 8x4 pixel block, and every thread
-// resolves its own pixel's depth test in registers.  No fragment list, no
-// global atomics, one coalesced 16-byte store per pixel.
+// the 16x16 screen tiles its rect (rasterize.cu:43-137) overlaps, and each
+// tile's list is sorted by the triangles' near-depth bound.  A work item is
+// one 8x4 pixel block of a tile, owned by one warp: the warp filters the
+// tile's triangle boxes 32 at a time (rect overlap, depth bound), stages the
+// survivors' vertices in its own shared memory, and every lane resolves its
+// pixel's depth test in registers.  Warps never wait for each other: no
+// fragment list, no CTA barrier, no global atomics, one 16-byte store per
+// pixel.
 //
 // Results equal the reference's: coverage, barycentrics and depth use its
 // FP32 arithmetic, the depth key is bits(z+2) with ties broken by the lower
@@ -19,24 +22,36 @@
 
 namespace dsb {
 
-// Per (view, triangle) record: clip vertices and the pixel rect
-// [y0, y1) x [x0, x1) (empty when y1 <= y0).
-struct __align__(16) TriRec {
-    float4 p0, p1, p2;
-    int4 rect;  // y0, y1, x0, x1
+// Per (view, triangle): the pixel rect [y0, y1) x [x0, x1) (empty when
+// y1 <= y0) and bounds [zlo, zhi] on the NDC depth of every fragment the
+// triangle can produce.  With every w > 0 (the rect test culls the rest), a
+// fragment's depth z/w is a convex combination of the vertices' z_i/w_i, so
+// [min, max] of those bound it; the bounds are widened by the rounding of the
+// fragment arithmetic.
+struct __align__(16) TriBox {
+    short y0, y1, x0, x1;
+    float zlo, zhi;
 };
-static_assert(sizeof(TriRec) == 64, "TriRec layout");
+static_assert(sizeof(TriBox) == 16, "TriBox layout");
 
-constexpr int kTileThreads = 256;  // one pixel per thread of a 16x16 tile
+struct __align__(16) TriVerts {
+    float4 p0, p1, p2;
+};
+
+constexpr int kWarpsPerCta = 8;
+constexpr int kBlocksPerTile = 8;  // 8x4 pixel blocks of a 16x16 tile
+constexpr int kSortMax = 512;      // longest tile list sorted by depth
 constexpr int kAuxSmemS = 160;     // per-warp shared accumulator for lattices up to level 4
 
 struct TileWs {
-    TriRec* recs;
+    TriBox* boxes;
+    TriVerts* verts;
     int* counts;
     int64_t* offsets;  // [num_tiles + 1] exclusive prefix of counts
     int* cursor;
+    int* sorted;       // per tile: 1 when its list is ordered by zlo
     int* list;
-    int* work;  // persistent-kernel tile queue counters [2]
+    int* work;         // persistent-kernel work counters [2]
     void* scan;
 };
 
@@ -46,10 +61,12 @@ static TileWs carve(void* ws, int B, int T, int num_tiles, int64_t capacity, siz
     char* p = reinterpret_cast<char*>(ws);
     TileWs w;
     size_t o = 0;
-    w.recs = reinterpret_cast<TriRec*>(p + o); o += al256((size_t)B * T * sizeof(TriRec));
+    w.boxes = reinterpret_cast<TriBox*>(p + o); o += al256((size_t)B * T * sizeof(TriBox));
+    w.verts = reinterpret_cast<TriVerts*>(p + o); o += al256((size_t)B * T * sizeof(TriVerts));
     w.counts = reinterpret_cast<int*>(p + o); o += al256((size_t)num_tiles * sizeof(int));
     w.offsets = reinterpret_cast<int64_t*>(p + o); o += al256((size_t)(num_tiles + 1) * sizeof(int64_t));
     w.cursor = reinterpret_cast<int*>(p + o); o += al256((size_t)num_tiles * sizeof(int));
+    w.sorted = reinterpret_cast<int*>(p + o); o += al256((size_t)num_tiles * sizeof(int));
     w.work = reinterpret_cast<int*>(p + o); o += 256;
     w.scan = p + o; o += al256(scan_workspace_bytes(num_tiles));
     w.list = reinterpret_cast<int*>(p + o); o += al256((size_t)capacity * sizeof(int));
@@ -66,41 +83,51 @@ __device__ __forceinline__ int find_view(const ds_view_desc* __restrict__ views,
     return lo;
 }
 
-// Tile range of a rect; false when the rect is empty.
-__device__ __forceinline__ bool rect_tiles(const int4 r, int& tx0, int& tx1, int& ty0, int& ty1) {
-    if (r.y <= r.x || r.w <= r.z) return false;
-    tx0 = r.z / DS_TILE; tx1 = (r.w - 1) / DS_TILE;
-    ty0 = r.x / DS_TILE; ty1 = (r.y - 1) / DS_TILE;
+// Tile range of a box; false when its rect is empty.
+__device__ __forceinline__ bool box_tiles(const TriBox& r, int& tx0, int& tx1, int& ty0, int& ty1) {
+    if (r.y1 <= r.y0 || r.x1 <= r.x0) return false;
+    tx0 = r.x0 / DS_TILE; tx1 = (r.x1 - 1) / DS_TILE;
+    ty0 = r.y0 / DS_TILE; ty1 = (r.y1 - 1) / DS_TILE;
     return true;
 }
 
-// Pass 1: records and per-tile counts.
+// Pass 1: boxes, vertices and per-tile counts.
 __global__ void __launch_bounds__(kThreads) bin_setup_kernel(int B, const ds_view_desc* __restrict__ views, int V,
                                                              const float* __restrict__ pos, int T,
-                                                             const int* __restrict__ tri, TriRec* __restrict__ recs,
-                                                             int* __restrict__ counts) {
+                                                             const int* __restrict__ tri, TriBox* __restrict__ boxes,
+                                                             TriVerts* __restrict__ verts, int* __restrict__ counts) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (int64_t)B * T) return;
     const int b = (int)(i / T), t = (int)(i % T);
     const ds_view_desc vd = views[b];
     const float* P = pos + (size_t)b * V * 4;
-    TriRec r;
-    r.p0 = load_vertex(P, __ldg(tri + t * 3 + 0));
-    r.p1 = load_vertex(P, __ldg(tri + t * 3 + 1));
-    r.p2 = load_vertex(P, __ldg(tri + t * 3 + 2));
+    TriVerts v;
+    v.p0 = load_vertex(P, __ldg(tri + t * 3 + 0));
+    v.p1 = load_vertex(P, __ldg(tri + t * 3 + 1));
+    v.p2 = load_vertex(P, __ldg(tri + t * 3 + 2));
     int h0, hl, w0, wl;
-    triangle_rect(vd.H, vd.W, r.p0, r.p1, r.p2, h0, hl, w0, wl);
-    r.rect = make_int4(h0, h0 + hl, w0, w0 + wl);
-    recs[i] = r;
+    triangle_rect(vd.H, vd.W, v.p0, v.p1, v.p2, h0, hl, w0, wl);
+    TriBox r;
+    r.y0 = (short)h0; r.y1 = (short)(h0 + hl); r.x0 = (short)w0; r.x1 = (short)(w0 + wl);
+    // depth bounds (only used when the rect is non-empty, i.e. every w > 0)
+    const float d0 = v.p0.z / v.p0.w, d1 = v.p1.z / v.p1.w, d2 = v.p2.z / v.p2.w;
+    const float mz = fmaxf(fmaxf(fabsf(v.p0.z), fabsf(v.p1.z)), fabsf(v.p2.z));
+    const float mw = fminf(fminf(v.p0.w, v.p1.w), v.p2.w);
+    const float margin = 1e-5f + 4e-6f * (mz / mw + fmaxf(fmaxf(fabsf(d0), fabsf(d1)), fabsf(d2)));
+    r.zlo = fminf(fminf(d0, d1), d2) - margin;
+    r.zhi = fmaxf(fmaxf(d0, d1), d2) + margin;
+    if (!(r.zlo == r.zlo && r.zhi == r.zhi)) { r.zlo = -INFINITY; r.zhi = INFINITY; }  // NaN: no bounds
+    boxes[i] = r;
+    verts[i] = v;
     int tx0, tx1, ty0, ty1;
-    if (!rect_tiles(r.rect, tx0, tx1, ty0, ty1)) return;
+    if (!box_tiles(r, tx0, tx1, ty0, ty1)) return;
     for (int ty = ty0; ty <= ty1; ++ty)
         for (int tx = tx0; tx <= tx1; ++tx) atomicAdd(counts + vd.tile_base + ty * vd.tiles_x + tx, 1);
 }
 
 // Pass 2: scatter record indices into the per-tile lists.
 __global__ void __launch_bounds__(kThreads) bin_fill_kernel(int B, const ds_view_desc* __restrict__ views, int T,
-                                                            const TriRec* __restrict__ recs,
+                                                            const TriBox* __restrict__ boxes,
                                                             const int64_t* __restrict__ offsets,
                                                             int* __restrict__ cursor, int* __restrict__ list,
                                                             int64_t capacity, int* __restrict__ status) {
@@ -108,9 +135,9 @@ __global__ void __launch_bounds__(kThreads) bin_fill_kernel(int B, const ds_view
     if (i >= (int64_t)B * T) return;
     const int b = (int)(i / T);
     const ds_view_desc vd = views[b];
-    const int4 rc = recs[i].rect;
+    const TriBox rc = boxes[i];
     int tx0, tx1, ty0, ty1;
-    if (!rect_tiles(rc, tx0, tx1, ty0, ty1)) return;
+    if (!box_tiles(rc, tx0, tx1, ty0, ty1)) return;
     bool over = false;
     for (int ty = ty0; ty <= ty1; ++ty)
         for (int tx = tx0; tx <= tx1; ++tx) {
@@ -121,25 +148,85 @@ __global__ void __launch_bounds__(kThreads) bin_fill_kernel(int B, const ds_view
     if (over) atomicOr(status, DS_STATUS_LIST_OVERFLOW);
 }
 
-struct TileGeom {
+// Pass 3: sort each tile's list by zlo (warp per tile, bitonic in shared
+// memory).  Lists longer than kSortMax, or cut by the capacity, stay as they
+// are and are marked unsorted.
+__global__ void __launch_bounds__(kWarpsPerCta * 32) sort_lists_kernel(int num_tiles, const TriBox* __restrict__ boxes,
+                                                                       const int64_t* __restrict__ offsets,
+                                                                       int* __restrict__ list, int64_t capacity,
+                                                                       int* __restrict__ sorted) {
+    __shared__ float s_key[kWarpsPerCta][kSortMax];
+    __shared__ int s_val[kWarpsPerCta][kSortMax];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tile = blockIdx.x * kWarpsPerCta + warp;
+    if (tile >= num_tiles) return;
+    const int64_t begin = offsets[tile], end = offsets[tile + 1];
+    const int n = (int)(end - begin);
+    if (end > capacity || n > kSortMax) {
+        if (lane == 0) sorted[tile] = 0;
+        return;
+    }
+    if (n <= 1) {
+        if (lane == 0) sorted[tile] = 1;
+        return;
+    }
+    int size = 32;
+    while (size < n) size <<= 1;
+    float* key = s_key[warp];
+    int* val = s_val[warp];
+    for (int i = lane; i < size; i += 32) {
+        if (i < n) {
+            const int ri = list[begin + i];
+            key[i] = fminf(boxes[ri].zlo, 3.0e38f);  // real keys stay below the +inf padding
+            val[i] = ri;
+        } else {
+            key[i] = INFINITY;
+            val[i] = -1;
+        }
+    }
+    __syncwarp();
+    for (int k = 2; k <= size; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = lane; i < size; i += 32) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const float a = key[i], c = key[l];
+                    const bool up = (i & k) == 0;
+                    if ((a > c) == up && a != c) {
+                        key[i] = c; key[l] = a;
+                        const int t = val[i]; val[i] = val[l]; val[l] = t;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+    for (int i = lane; i < n; i += 32) list[begin + i] = val[i];
+    if (lane == 0) sorted[tile] = 1;
+}
+
+// Geometry of one work item (tile, 8x4 block) for the calling lane.
+struct BlockGeom {
     int b, px, py, H, W;
-    int64_t pix;  // packed pixel index
+    int64_t pix;          // packed pixel index
     bool valid;
-    int wx0, wy0;  // this warp's 8x4 block origin
-    int64_t begin, end;  // entry range in the list, or [b*T, b*T+T) records when exhaustive
-    bool exhaustive;
+    int wx0, wy0;         // block origin
+    int64_t begin, end;   // list range, or [b*T, b*T+T) records when exhaustive
+    bool exhaustive, ordered;
 };
 
-__device__ __forceinline__ TileGeom tile_geometry(int tile, int B, const ds_view_desc* __restrict__ views, int T,
-                                                  const int64_t* __restrict__ offsets, int64_t capacity) {
-    TileGeom g;
+__device__ __forceinline__ BlockGeom block_geometry(int item, int B, const ds_view_desc* __restrict__ views, int T,
+                                                    const int64_t* __restrict__ offsets,
+                                                    const int* __restrict__ sorted, int64_t capacity) {
+    BlockGeom g;
+    const int tile = item / kBlocksPerTile, blk = item % kBlocksPerTile;
     g.b = find_view(views, B, tile);
     const ds_view_desc vd = views[g.b];
     const int tl = tile - vd.tile_base;
     const int tx = tl % vd.tiles_x, ty = tl / vd.tiles_x;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    g.wx0 = tx * DS_TILE + (warp & 1) * 8;
-    g.wy0 = ty * DS_TILE + (warp >> 1) * 4;
+    const int lane = threadIdx.x & 31;
+    g.wx0 = tx * DS_TILE + (blk & 1) * 8;
+    g.wy0 = ty * DS_TILE + (blk >> 1) * 4;
     g.px = g.wx0 + (lane & 7);
     g.py = g.wy0 + (lane >> 3);
     g.H = vd.H; g.W = vd.W;
@@ -148,67 +235,132 @@ __device__ __forceinline__ TileGeom tile_geometry(int tile, int B, const ds_view
     g.begin = offsets[tile];
     g.end = offsets[tile + 1];
     g.exhaustive = g.end > capacity;
+    g.ordered = !g.exhaustive && sorted[tile] != 0;
     if (g.exhaustive) { g.begin = (int64_t)g.b * T; g.end = g.begin + T; }
     return g;
 }
 
-__device__ __forceinline__ bool warp_overlaps(const int4 r, int wx0, int wy0) {
-    return r.x < wy0 + 4 && r.y > wy0 && r.z < wx0 + 8 && r.w > wx0;
+__device__ __forceinline__ bool box_overlaps(const TriBox& r, int wx0, int wy0) {
+    return r.y0 < wy0 + 4 && r.y1 > wy0 && r.x0 < wx0 + 8 && r.x1 > wx0;
 }
 
-__device__ __forceinline__ int next_tile(int* work, int* s_tile) {
-    __syncthreads();
-    if (threadIdx.x == 0) *s_tile = atomicAdd(work, 1);
-    __syncthreads();
-    return *s_tile;
+__device__ __forceinline__ int warp_next(int* work) {
+    int item = 0;
+    if ((threadIdx.x & 31) == 0) item = atomicAdd(work, 1);
+    return __shfl_sync(0xffffffffu, item, 0);
 }
 
-// Forward: depth test with stochastic opacity, one CTA per tile (persistent).
-__global__ void __launch_bounds__(kTileThreads) raster_kernel(int B, const ds_view_desc* __restrict__ views,
-                                                              int num_tiles, int T, const TriRec* __restrict__ recs,
-                                                              const int64_t* __restrict__ offsets,
-                                                              const int* __restrict__ list, int64_t capacity,
-                                                              int level, int S, const float* __restrict__ alpha_src,
-                                                              int thr_mode, float thr_const,
-                                                              const uint64_t* __restrict__ rng, int* work,
-                                                              float* __restrict__ rast) {
-    __shared__ TriRec s_rec[kTileThreads];
-    __shared__ int s_tri[kTileThreads];
-    __shared__ int s_tile;
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Candidates of one group of up to 32 list entries staged in warp-private
+// shared memory, in list order.
+struct WarpStage {
+    TriVerts v[32];
+    TriBox box[32];
+    int t[32];
+};
+
+// Loads entries [g0, g0+32) of the work item's range, keeps those whose box
+// meets the block and whose depth bound passes `zcut` (zlo <= zcut), stages
+// them, and returns how many were staged.  *head_zlo receives the zlo of the
+// group's first entry (the smallest, when the list is ordered).
+__device__ __forceinline__ int stage_group(const BlockGeom& g, int64_t g0, const TriBox* __restrict__ boxes,
+                                           const TriVerts* __restrict__ verts, const int* __restrict__ list, int T,
+                                           float zcut, WarpStage& st, float* head_zlo) {
+    const int lane = threadIdx.x & 31;
+    const int64_t e = g0 + lane;
+    const bool in = e < g.end;
+    int ri = 0;
+    TriBox bx;
+    bx.y0 = bx.y1 = bx.x0 = bx.x1 = 0;
+    bx.zlo = INFINITY; bx.zhi = INFINITY;
+    if (in) {
+        ri = g.exhaustive ? (int)e : __ldg(list + e);
+        bx = boxes[ri];
+    }
+    *head_zlo = __shfl_sync(0xffffffffu, bx.zlo, 0);
+    const bool c = in && box_overlaps(bx, g.wx0, g.wy0) && bx.zlo <= zcut;
+    const unsigned mask = __ballot_sync(0xffffffffu, c);
+    if (c) {
+        const int k = __popc(mask & ((1u << lane) - 1u));
+        st.v[k] = verts[ri];
+        st.box[k] = bx;
+        st.t[k] = ri - g.b * T;
+    }
+    __syncwarp();
+    return __popc(mask);
+}
+
+// Forward: depth test with stochastic opacity.  Each warp walks the
+// triangles of its block front to back (the tile list is sorted by zlo) and
+// stops once the next triangle's depth bound lies behind the winner of every
+// lane: no later triangle can improve a key (the bound's margin keeps
+// bits(z+2) strictly larger).  Within a triangle, the divisions run only when
+// some lane survives the cheap edge-sign test.
+__global__ void __launch_bounds__(kWarpsPerCta * 32) raster_kernel(
+    int B, const ds_view_desc* __restrict__ views, int num_tiles, int T, const TriBox* __restrict__ boxes,
+    const TriVerts* __restrict__ verts, const int64_t* __restrict__ offsets, const int* __restrict__ sorted,
+    const int* __restrict__ list, int64_t capacity, int level, int S, const float* __restrict__ alpha_src,
+    int thr_mode, float thr_const, const uint64_t* __restrict__ rng, int* work, float* __restrict__ rast) {
+    __shared__ WarpStage s_stage[kWarpsPerCta];
+    WarpStage& st = s_stage[threadIdx.x >> 5];
     uint64_t seed = 0;
     uint32_t iter = 0;
     if (thr_mode == 1) { seed = rng[0]; iter = (uint32_t)rng[1]; }
-    for (int tile = next_tile(work, &s_tile); tile < num_tiles; tile = next_tile(work, &s_tile)) {
-        const TileGeom g = tile_geometry(tile, B, views, T, offsets, capacity);
+    const int items = num_tiles * kBlocksPerTile;
+    for (int item = warp_next(work); item < items; item = warp_next(work)) {
+        const BlockGeom g = block_geometry(item, B, views, T, offsets, sorted, capacity);
         const float ndc_x = pix_ndc(g.px, g.W), ndc_y = pix_ndc(g.py, g.H);
         const uint32_t pixel_id = (uint32_t)(g.py * g.W + g.px);
         unsigned long long best = ~0ull;
         float bb0 = 0.f, bb1 = 0.f, bz = 0.f;
-        for (int64_t c0 = g.begin; c0 < g.end; c0 += kTileThreads) {
-            const int n = (int)min((int64_t)kTileThreads, g.end - c0);
-            __syncthreads();
-            if ((int)threadIdx.x < n) {
-                const int64_t e = c0 + threadIdx.x;
-                const int ri = g.exhaustive ? (int)e : __ldg(list + e);
-                s_rec[threadIdx.x] = recs[ri];
-                s_tri[threadIdx.x] = ri - g.b * T;
+        // max over the warp of the lanes' winning depth (+inf while a valid lane has none)
+        float warp_far = warp_max(g.valid ? INFINITY : -INFINITY);
+        for (int64_t g0 = g.begin; g0 < g.end; g0 += 32) {
+            float head;
+            const int nc = stage_group(g, g0, boxes, verts, list, T, warp_far, st, &head);
+            if (g.ordered && head > warp_far) break;  // this group and all later ones lie behind
+            for (int k = 0; k < nc; ++k) {
+                if (st.box[k].zlo > warp_far) {
+                    if (g.ordered) break;
+                    continue;
+                }
+                const float4 p0 = st.v[k].p0, p1 = st.v[k].p1, p2 = st.v[k].p2;
+                const TriBox r = st.box[k];
+                float A0, A1, A2, A;
+                edge_terms(ndc_y, ndc_x, p0, p1, p2, A0, A1, A2, A);
+                const bool cand = g.valid && g.px >= r.x0 && g.px < r.x1 && g.py >= r.y0 && g.py < r.y1 &&
+                                  !surely_outside(A0, A1, A2, A);
+                if (!__any_sync(0xffffffffu, cand)) continue;  // warp-uniform
+                bool improved = false;
+                if (cand) {
+                    float b0, b1, z, w;
+                    if (finish_coverage(A0, A1, A, p0, p1, p2, b0, b1, z, w)) {
+                        const float depth = __fdiv_rn(z, w);
+                        if (depth > -1.f && depth <= 1.f) {
+                            const uint32_t t = (uint32_t)st.t[k];
+                            const unsigned long long key = depth_key(depth, t);
+                            if (key < best) {
+                                const float alpha = interp_scalar(b0, b1, level, level, alpha_src + (size_t)t * S);
+                                const float thr = thr_mode == 1
+                                                      ? philox_uniform(seed, iter, (uint32_t)g.b, pixel_id, t)
+                                                      : thr_const;
+                                if (!(alpha < thr)) {
+                                    best = key; bb0 = b0; bb1 = b1; bz = depth;
+                                    improved = true;
+                                }
+                            }
+                        }
+                    }
+                }
+                if (__any_sync(0xffffffffu, improved))
+                    warp_far = warp_max(!g.valid ? -INFINITY : (best == ~0ull ? INFINITY : bz));
             }
-            __syncthreads();
-            for (int j = 0; j < n; ++j) {
-                const int4 r = s_rec[j].rect;
-                if (!warp_overlaps(r, g.wx0, g.wy0)) continue;  // warp-uniform
-                if (!g.valid || g.px < r.z || g.px >= r.w || g.py < r.x || g.py >= r.y) continue;
-                float b0, b1, depth;
-                if (!fragment_at(ndc_y, ndc_x, s_rec[j].p0, s_rec[j].p1, s_rec[j].p2, b0, b1, depth)) continue;
-                if (depth <= -1.f) continue;
-                const uint32_t t = (uint32_t)s_tri[j];
-                const unsigned long long key = depth_key(depth, t);
-                if (key >= best) continue;
-                const float alpha = interp_scalar(b0, b1, level, level, alpha_src + (size_t)t * S);
-                const float thr = thr_mode == 1 ? philox_uniform(seed, iter, (uint32_t)g.b, pixel_id, t) : thr_const;
-                if (alpha < thr) continue;
-                best = key; bb0 = b0; bb1 = b1; bz = depth;
-            }
+            __syncwarp();  // the stage is rewritten by the next group
         }
         if (g.valid) {
             float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -218,29 +370,30 @@ __global__ void __launch_bounds__(kTileThreads) raster_kernel(int B, const ds_vi
     }
 }
 
-// Opacity auxiliary gradient: re-enumerates each tile's fragments and
-// scatters dL/dalpha through the lattice adjoint.  All lanes of a warp work
-// on the same triangle at a time, so contributions are summed per warp in
-// shared memory and flushed with one global atomic per touched sample.
-__global__ void __launch_bounds__(kTileThreads) aux_kernel(int B, const ds_view_desc* __restrict__ views,
-                                                           int num_tiles, int T, const TriRec* __restrict__ recs,
-                                                           const int64_t* __restrict__ offsets,
-                                                           const int* __restrict__ list, int64_t capacity, int level,
-                                                           int S, const float* __restrict__ alpha_src, int C,
-                                                           const float* __restrict__ color,
-                                                           const float* __restrict__ target,
-                                                           const float* __restrict__ rast, float scale, int* work,
-                                                           float* __restrict__ grad_alpha_src) {
-    __shared__ TriRec s_rec[kTileThreads];
-    __shared__ int s_tri[kTileThreads];
-    __shared__ float s_acc[kTileThreads / 32][kAuxSmemS];
-    __shared__ int s_tile;
+// Opacity auxiliary gradient: re-enumerates each block's fragments and
+// scatters dL/dalpha through the lattice adjoint.  Fragments behind the
+// visible surface contribute nothing (rasterize.cu:950), so triangles whose
+// depth bound lies behind every lane's surface are never staged.  All lanes
+// of a warp work on the same triangle at a time, so contributions are summed
+// per warp in shared memory and flushed with one global atomic per touched
+// sample.
+__global__ void __launch_bounds__(kWarpsPerCta * 32) aux_kernel(
+    int B, const ds_view_desc* __restrict__ views, int num_tiles, int T, const TriBox* __restrict__ boxes,
+    const TriVerts* __restrict__ verts, const int64_t* __restrict__ offsets, const int* __restrict__ sorted,
+    const int* __restrict__ list, int64_t capacity, int level, int S, const float* __restrict__ alpha_src, int C,
+    const float* __restrict__ color, const float* __restrict__ target, const float* __restrict__ rast, float scale,
+    int* work, float* __restrict__ grad_alpha_src) {
+    __shared__ WarpStage s_stage[kWarpsPerCta];
+    __shared__ float s_acc[kWarpsPerCta][kAuxSmemS];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    WarpStage& st = s_stage[warp];
     const bool use_smem = S <= kAuxSmemS;
     if (use_smem)
         for (int k = lane; k < S; k += 32) s_acc[warp][k] = 0.f;
-    for (int tile = next_tile(work, &s_tile); tile < num_tiles; tile = next_tile(work, &s_tile)) {
-        const TileGeom g = tile_geometry(tile, B, views, T, offsets, capacity);
+    __syncwarp();
+    const int items = num_tiles * kBlocksPerTile;
+    for (int item = warp_next(work); item < items; item = warp_next(work)) {
+        const BlockGeom g = block_geometry(item, B, views, T, offsets, sorted, capacity);
         const float ndc_x = pix_ndc(g.px, g.W), ndc_y = pix_ndc(g.py, g.H);
         int tp = -1;
         float zp = 0.f, loss = 0.f;
@@ -254,29 +407,34 @@ __global__ void __launch_bounds__(kTileThreads) aux_kernel(int B, const ds_view_
                 loss = color[g.pix];  // caller passes the per-pixel sum |c - target| directly
             }
         }
-        for (int64_t c0 = g.begin; c0 < g.end; c0 += kTileThreads) {
-            const int n = (int)min((int64_t)kTileThreads, g.end - c0);
-            __syncthreads();
-            if ((int)threadIdx.x < n) {
-                const int64_t e = c0 + threadIdx.x;
-                const int ri = g.exhaustive ? (int)e : __ldg(list + e);
-                s_rec[threadIdx.x] = recs[ri];
-                s_tri[threadIdx.x] = ri - g.b * T;
-            }
-            __syncthreads();
-            for (int j = 0; j < n; ++j) {
-                const int4 r = s_rec[j].rect;
-                if (!warp_overlaps(r, g.wx0, g.wy0)) continue;  // warp-uniform
-                const int t = s_tri[j];
-                bool hit = g.valid && g.px >= r.z && g.px < r.w && g.py >= r.x && g.py < r.y;
-                float b0 = 0.f, b1 = 0.f, depth = 0.f;
-                if (hit) hit = fragment_at(ndc_y, ndc_x, s_rec[j].p0, s_rec[j].p1, s_rec[j].p2, b0, b1, depth);
-                if (hit && tp >= 0 && depth > zp) hit = false;
+        // farthest surface of the block (+inf where a valid pixel is empty)
+        const float warp_far = warp_max(!g.valid ? -INFINITY : (tp >= 0 ? zp : INFINITY));
+        for (int64_t g0 = g.begin; g0 < g.end; g0 += 32) {
+            float head;
+            const int nc = stage_group(g, g0, boxes, verts, list, T, warp_far, st, &head);
+            if (g.ordered && head > warp_far) break;
+            for (int k = 0; k < nc; ++k) {
+                const TriBox r = st.box[k];
+                const int t = st.t[k];
+                const float4 p0 = st.v[k].p0, p1 = st.v[k].p1, p2 = st.v[k].p2;
+                float A0, A1, A2, A;
+                edge_terms(ndc_y, ndc_x, p0, p1, p2, A0, A1, A2, A);
+                bool hit = g.valid && g.px >= r.x0 && g.px < r.x1 && g.py >= r.y0 && g.py < r.y1 &&
+                           !surely_outside(A0, A1, A2, A);
+                if (!__any_sync(0xffffffffu, hit)) continue;  // warp-uniform
+                float b0 = 0.f, b1 = 0.f;
+                if (hit) {
+                    float z, w;
+                    hit = finish_coverage(A0, A1, A, p0, p1, p2, b0, b1, z, w);
+                    if (hit) {
+                        const float depth = __fdiv_rn(z, w);
+                        hit = depth >= -1.f && depth <= 1.f && !(tp >= 0 && depth > zp);
+                    }
+                }
                 uint32_t idx[3] = {0, 0, 0};
                 float gw[3] = {0.f, 0.f, 0.f};
                 if (hit) {
-                    const float* as = alpha_src + (size_t)t * S;
-                    const float alpha = interp_scalar(b0, b1, level, level, as);
+                    const float alpha = interp_scalar(b0, b1, level, level, alpha_src + (size_t)t * S);
                     const float ga = aux_alpha_grad(loss, alpha, tp >= 0 && t == tp) * scale;
                     float w[3];
                     lattice_cell(b0, b1, level, idx, w);
@@ -286,21 +444,22 @@ __global__ void __launch_bounds__(kTileThreads) aux_kernel(int B, const ds_view_
                     if (!__any_sync(0xffffffffu, hit)) continue;
                     if (hit) {
 #pragma unroll
-                        for (int k = 0; k < 3; ++k) atomicAdd(&s_acc[warp][idx[k]], gw[k]);
+                        for (int q = 0; q < 3; ++q) atomicAdd(&s_acc[warp][idx[q]], gw[q]);
                     }
                     __syncwarp();
                     float* dst = grad_alpha_src + (size_t)t * S;
-                    for (int k = lane; k < S; k += 32) {
-                        const float v = s_acc[warp][k];
-                        if (v != 0.f) { atomicAdd(dst + k, v); s_acc[warp][k] = 0.f; }
+                    for (int q = lane; q < S; q += 32) {
+                        const float v = s_acc[warp][q];
+                        if (v != 0.f) { atomicAdd(dst + q, v); s_acc[warp][q] = 0.f; }
                     }
                     __syncwarp();
                 } else if (hit) {
                     float* dst = grad_alpha_src + (size_t)t * S;
 #pragma unroll
-                    for (int k = 0; k < 3; ++k) atomicAdd(dst + idx[k], gw[k]);
+                    for (int q = 0; q < 3; ++q) atomicAdd(dst + idx[q], gw[q]);
                 }
             }
+            __syncwarp();
         }
     }
 }
@@ -322,6 +481,7 @@ static int check_tiles_args(int B, const ds_view_desc* views, int num_tiles, int
     DS_CHECK_ARG(B >= 0 && num_tiles >= 0 && V >= 0 && T >= 0 && capacity >= 0, "tiles: bad sizes");
     DS_CHECK_ARG((int64_t)B * T <= 0x7fffffff, "tiles: B*T exceeds int32");
     DS_CHECK_ARG(capacity <= 0x7fffffff, "tiles: list capacity exceeds int32");
+    DS_CHECK_ARG((int64_t)num_tiles * kBlocksPerTile <= 0x7fffffff, "tiles: too many tiles");
     DS_CHECK_ARG(B == 0 || views != nullptr, "tiles: null view table");
     DS_CHECK_ARG(((uintptr_t)pos & 15) == 0, "tiles: pos not 16-byte aligned");
     if (ws_bytes < ds_tiles_workspace_size(B, T, num_tiles, capacity))
@@ -339,21 +499,28 @@ int ds_tiles_bin(int B, const ds_view_desc* views, int num_tiles, int V, const f
     DS_CUDA(cudaMemsetAsync(w.counts, 0, (size_t)num_tiles * sizeof(int), st));
     DS_CUDA(cudaMemsetAsync(w.cursor, 0, (size_t)num_tiles * sizeof(int), st));
     const int64_t n = (int64_t)B * T;
-    if (n > 0) bin_setup_kernel<<<blocks_for(n), kThreads, 0, st>>>(B, views, V, pos, T, tri, w.recs, w.counts);
+    if (n > 0)
+        bin_setup_kernel<<<blocks_for(n), kThreads, 0, st>>>(B, views, V, pos, T, tri, w.boxes, w.verts, w.counts);
     int64_t* total_dev = nullptr;
     rc = device_scan<int, int64_t>(w.counts, num_tiles, w.offsets, false, w.scan, st, &total_dev);
     if (rc) return rc;
     // offsets[num_tiles] = total number of entries
     DS_CUDA(cudaMemcpyAsync(w.offsets + num_tiles, total_dev, sizeof(int64_t), cudaMemcpyDeviceToDevice, st));
     if (n > 0)
-        bin_fill_kernel<<<blocks_for(n), kThreads, 0, st>>>(B, views, T, w.recs, w.offsets, w.cursor, w.list,
+        bin_fill_kernel<<<blocks_for(n), kThreads, 0, st>>>(B, views, T, w.boxes, w.offsets, w.cursor, w.list,
                                                             list_capacity, status);
+    if (num_tiles > 0)
+        sort_lists_kernel<<<(unsigned)((num_tiles + kWarpsPerCta - 1) / kWarpsPerCta), kWarpsPerCta * 32, 0, st>>>(
+            num_tiles, w.boxes, w.offsets, w.list, list_capacity, w.sorted);
     return check_launch("tiles_bin");
 }
 
-static unsigned tile_grid(int num_tiles) {
-    const int per_sm = 4;  // 256-thread CTAs, ~17 KB shared each
-    return (unsigned)max(1, min(num_tiles, kSMs * per_sm));
+static unsigned block_grid(int num_tiles) {
+    const int per_sm = 4;  // 8-warp CTAs, ~14 KB shared each
+    const int64_t warps = (int64_t)num_tiles * kBlocksPerTile;
+    const int64_t ctas = (warps + kWarpsPerCta - 1) / kWarpsPerCta;
+    const int64_t cap = (int64_t)kSMs * per_sm;
+    return (unsigned)(ctas < 1 ? 1 : (ctas < cap ? ctas : cap));
 }
 
 int ds_tiles_rasterize(int B, const ds_view_desc* views, int num_tiles, int V, const float* pos, int T,
@@ -370,9 +537,9 @@ int ds_tiles_rasterize(int B, const ds_view_desc* views, int num_tiles, int V, c
     cudaStream_t st = (cudaStream_t)stream;
     TileWs w = carve(workspace, B, T, num_tiles, list_capacity, nullptr);
     DS_CUDA(cudaMemsetAsync(w.work, 0, sizeof(int), st));
-    raster_kernel<<<tile_grid(num_tiles), kTileThreads, 0, st>>>(B, views, num_tiles, T, w.recs, w.offsets, w.list,
-                                                                 list_capacity, level, S, alpha_src, thr_mode,
-                                                                 thr_const, rng, w.work, rast);
+    raster_kernel<<<block_grid(num_tiles), kWarpsPerCta * 32, 0, st>>>(
+        B, views, num_tiles, T, w.boxes, w.verts, w.offsets, w.sorted, w.list, list_capacity, level, S, alpha_src,
+        thr_mode, thr_const, rng, w.work, rast);
     return check_launch("tiles_rasterize");
 }
 
@@ -391,9 +558,9 @@ int ds_tiles_opacity_aux(int B, const ds_view_desc* views, int num_tiles, int V,
     cudaStream_t st = (cudaStream_t)stream;
     TileWs w = carve(workspace, B, T, num_tiles, list_capacity, nullptr);
     DS_CUDA(cudaMemsetAsync(w.work + 1, 0, sizeof(int), st));
-    aux_kernel<<<tile_grid(num_tiles), kTileThreads, 0, st>>>(B, views, num_tiles, T, w.recs, w.offsets, w.list,
-                                                              list_capacity, level, S, alpha_src, C, color, target,
-                                                              rast, scale, w.work + 1, grad_alpha_src);
+    aux_kernel<<<block_grid(num_tiles), kWarpsPerCta * 32, 0, st>>>(
+        B, views, num_tiles, T, w.boxes, w.verts, w.offsets, w.sorted, w.list, list_capacity, level, S, alpha_src, C,
+        color, target, rast, scale, w.work + 1, grad_alpha_src);
     return check_launch("tiles_opacity_aux");
 }
 
