@@ -226,6 +226,142 @@ __device__ __forceinline__ int edge_grad_pixel(int b, int y0, int x0, int H, int
     return it0;
 }
 
+// The estimator of edge_grad_pixel for a colour of 3 channels, reorganised
+// for SIMT execution: each interior pair (both pixels on the same triangle)
+// is evaluated once, from its left/bottom pixel, and counted twice (the
+// adjoint and the pixel offset both change sign, so the two evaluations the
+// reference makes are equal); all interior pairs of a pixel run first as
+// uniform work, then the rarer silhouette / intersection pairs.
+__device__ __forceinline__ float pair_adjoint3(const float* c0, const float* g0, const float* c1, const float* g1) {
+    float adj = 0.f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) adj += 0.5f * (g0[i] + g1[i]) * (c0[i] - c1[i]);
+    return adj;
+}
+
+__device__ __forceinline__ int edge_grad_pixel_split(int y0, int x0, int H, int W, const float* __restrict__ color,
+                                                     const float* __restrict__ grad_color,
+                                                     const float* __restrict__ rast, const float* __restrict__ posb,
+                                                     const int* __restrict__ tri, int64_t base, EdgeAccum& acc) {
+#pragma unroll
+    for (int k = 0; k < 12; ++k) acc.g[k] = 0.f;
+    acc.any = false;
+    const int64_t pix0 = base + (int64_t)y0 * W + x0;
+    const float4 r0 = reinterpret_cast<const float4*>(rast)[pix0];
+    const int it0 = (int)r0.w - 1;
+    if (it0 < 0) return -1;
+    const float depth0 = r0.z;
+    // pixel-centre NDC with one reciprocal per axis (this path is compared to
+    // the oracle with a tolerance; the 1-ulp difference is far below it)
+    const float sx = 2.f / (float)W, sy = 2.f / (float)H;
+    const float nx0 = -1.f + ((float)x0 + 0.5f) * sx;
+    const float ny0 = -1.f + ((float)y0 + 0.5f) * sy;
+    float4 P0[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) P0[k] = load_vertex(posb, __ldg(tri + it0 * 3 + k));
+    float c0[3], g0[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) { c0[i] = color[pix0 * 3 + i]; g0[i] = grad_color[pix0 * 3 + i]; }
+    // neighbours (+x, -x, -y, +y) as in rasterize.cu:691-692
+    unsigned edge_mask = 0;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const int DX = (e == 0) - (e == 1);
+        const int DY = (e == 3) - (e == 2);
+        const int y1 = y0 + DY, x1 = x0 + DX;
+        if (y1 < 0 || y1 >= H || x1 < 0 || x1 >= W) continue;
+        const int64_t pix1 = base + (int64_t)y1 * W + x1;
+        const int it1 = (int)reinterpret_cast<const float4*>(rast)[pix1].w - 1;
+        if (it1 != it0) { edge_mask |= 1u << e; continue; }
+        if (DX < 0 || DY < 0) continue;  // interior pair counted by the neighbour
+        float c1[3], g1[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) { c1[i] = color[pix1 * 3 + i]; g1[i] = grad_color[pix1 * 3 + i]; }
+        const float adj = pair_adjoint3(c0, g0, c1, g1);
+        if (adj == 0.f) continue;
+        const float gx = adj * (float)DX * (float)W / 2.f;
+        const float gy = adj * (float)DY * (float)H / 2.f;
+        const float nx1 = -1.f + ((float)x1 + 0.5f) * sx;
+        const float ny1 = -1.f + ((float)y1 + 0.5f) * sy;
+        add_mid_contrib(0.5f * (nx0 + nx1), 0.5f * (ny0 + ny1), P0, 2.f * gx, 2.f * gy, 0.f, false, acc);
+    }
+#pragma unroll 1
+    for (int e = 0; e < 4; ++e) {
+        if (!((edge_mask >> e) & 1u)) continue;
+        const int DX = (e == 0) - (e == 1);
+        const int DY = (e == 3) - (e == 2);
+        const int y1 = y0 + DY, x1 = x0 + DX;
+        const int64_t pix1 = base + (int64_t)y1 * W + x1;
+        const float4 r1 = reinterpret_cast<const float4*>(rast)[pix1];
+        const float depth1 = r1.z;
+        const int it1 = (int)r1.w - 1;
+        float c1[3], g1[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) { c1[i] = color[pix1 * 3 + i]; g1[i] = grad_color[pix1 * 3 + i]; }
+        const float adj = pair_adjoint3(c0, g0, c1, g1);
+        if (adj == 0.f) continue;
+        const float gx = adj * (float)DX * (float)W / 2.f;
+        const float gy = adj * (float)DY * (float)H / 2.f;
+        const float nx1 = -1.f + ((float)x1 + 0.5f) * sx;
+        const float ny1 = -1.f + ((float)y1 + 0.5f) * sy;
+        const float mx = 0.5f * (nx0 + nx1), my = 0.5f * (ny0 + ny1);
+        float tb0, tb1, cz1, cw1;
+        if (intersect_triangle(ny1, nx1, P0[0], P0[1], P0[2], tb0, tb1, cz1, cw1)) {
+            const float d1_it0 = cz1 / cw1;
+            if (it1 >= 0 && depth1 < d1_it0) {
+                float4 P1[3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) P1[k] = load_vertex(posb, __ldg(tri + it1 * 3 + k));
+                float cz0, cw0;
+                if (intersect_triangle(ny0, nx0, P1[0], P1[1], P1[2], tb0, tb1, cz0, cw0)) {
+                    const float d0_it1 = cz0 / cw0;
+                    if (depth0 < d0_it1) {  // triangle intersection
+                        float nv[3], nf[3];
+                        if (tri_normal_ndc(P0, nv) && tri_normal_ndc(P1, nf)) {
+                            float gxn = 0.f, gyn = 0.f, gzn = 0.f;
+                            if (DX != 0) {
+                                float dbx, dbz;
+                                db_dp_2d(nv[0], nv[2], nf[0], nf[2], dbx, dbz);
+                                gxn = gx * dbx; gzn = gx * dbz;
+                            } else {
+                                float dby, dbz;
+                                db_dp_2d(nv[1], nv[2], nf[1], nf[2], dby, dbz);
+                                gyn = gy * dby; gzn = gy * dbz;
+                            }
+                            add_mid_contrib(mx, my, P0, gxn, gyn, gzn, true, acc);
+                        }
+                    }
+                }
+            } else if (it1 < 0 || depth0 < depth1) {  // active opacity edge
+                add_mid_contrib(mx, my, P0, gx, gy, 0.f, false, acc);
+            }
+        } else if (it1 < 0 || depth0 < depth1) {  // active geometric edge
+            int i0, i1;
+            float s0, s1;
+            if (find_edge_intersection(P0, nx0, ny0, nx1, ny1, i0, i1, s0, s1)) {
+                const float4 A = i0 == 0 ? P0[0] : (i0 == 1 ? P0[1] : P0[2]);
+                const float4 Bv = i1 == 0 ? P0[0] : (i1 == 1 ? P0[1] : P0[2]);
+                const float cx = s0 * A.x + s1 * Bv.x;
+                const float cy = s0 * A.y + s1 * Bv.y;
+                const float cw = s0 * A.w + s1 * Bv.w;
+                const float iw = 1.f / cw, iw2 = iw * iw;
+                const float gsum = gx * cx + gy * cy;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const float s = k == i0 ? s0 : (k == i1 ? s1 : 0.f);
+                    if (k == i0 || k == i1) {
+                        acc.g[k * 4 + 0] += s * gx * iw;
+                        acc.g[k * 4 + 1] += s * gy * iw;
+                        acc.g[k * 4 + 3] += -s * gsum * iw2;
+                    }
+                }
+                acc.any = true;
+            }
+        }
+    }
+    return it0;
+}
+
 // Per-fragment gradient of the opacity auxiliary objective
 // (rasterize.cu:955-970): +L/alpha for the visible fragment, -L/(1-alpha)
 // for the others in front of the surface or on empty pixels.

@@ -175,8 +175,8 @@ __global__ void __launch_bounds__(K::WARPS * 32) shade_step_kernel(ShadeArgs a) 
             }
             const int b = view_of_pixel(a.views, a.B, p);
             const ds_view_desc vd = a.views[b];
-            const int64_t local = p - vd.pix_offset;
-            const int py = (int)(local / vd.W), px = (int)(local % vd.W);
+            const int local = (int)(p - vd.pix_offset);  // < H*W < 2^31: 32-bit division
+            const int py = local / vd.W, px = local - py * vd.W;
             float M[16];
 #pragma unroll
             for (int k = 0; k < 16; ++k) M[k] = __ldg(a.inv_mvp + (size_t)b * 16 + k);

@@ -133,16 +133,21 @@ __global__ void __launch_bounds__(kThreads) project_backward_kernel(int B, int V
     grad_verts[(size_t)v * 3 + 2] = (float)gz;
 }
 
-// Edge gradients over packed views (rasterize.cu:653-903).  Consecutive
-// pixels of a row mostly share a triangle: a segmented warp reduction sums
-// runs of equal triangles before one FP64 atomic per vertex component.
-__global__ void __launch_bounds__(128) edge_step_kernel(int B, const ds_view_desc* __restrict__ views,
-                                                             int64_t num_pixels, int V, const float* __restrict__ pos,
-                                                             const int* __restrict__ tri,
-                                                             const float* __restrict__ color,
-                                                             const float* __restrict__ grad_color,
-                                                             const float* __restrict__ rast,
-                                                             double* __restrict__ grad_pos) {
+// Edge gradients over packed views (rasterize.cu:653-903), one pixel per
+// thread.  Consecutive pixels of a row mostly share a triangle: a segmented
+// warp reduction sums runs of equal (view, triangle) before one FP64 atomic
+// per vertex component.
+constexpr int kEdgeThreads = 128;
+
+__global__ void __launch_bounds__(kEdgeThreads) edge_step_kernel(int B, const ds_view_desc* __restrict__ views,
+                                                                 int64_t num_pixels, int V, int T,
+                                                                 const float* __restrict__ pos,
+                                                                 const int* __restrict__ tri,
+                                                                 const float* __restrict__ color,
+                                                                 const float* __restrict__ grad_color,
+                                                                 const float* __restrict__ rast,
+                                                                 double* __restrict__ grad_pos) {
+    (void)T;
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     EdgeAccum acc;
@@ -153,24 +158,26 @@ __global__ void __launch_bounds__(128) edge_step_kernel(int B, const ds_view_des
     if (p < num_pixels) {
         b = view_of_pixel(views, B, p);
         const ds_view_desc vd = views[b];
-        const int64_t local = p - vd.pix_offset;
-        const int y = (int)(local / vd.W), x = (int)(local % vd.W);
-        it0 = edge_grad_pixel(b, y, x, vd.H, vd.W, 3, color, grad_color, rast, pos + (size_t)b * V * 4, tri,
-                              vd.pix_offset, acc, /*pair_once=*/true);
+        const int local = (int)(p - vd.pix_offset);  // < H*W < 2^31: 32-bit division
+        const int y = local / vd.W, x = local - y * vd.W;
+        it0 = edge_grad_pixel_split(y, x, vd.H, vd.W, color, grad_color, rast, pos + (size_t)b * V * 4, tri,
+                                    vd.pix_offset, acc);
     }
     const int key = (it0 >= 0 && acc.any) ? it0 : -1 - lane;
     const int prev = __shfl_up_sync(0xffffffffu, key, 1);
     const int prevb = __shfl_up_sync(0xffffffffu, b, 1);
     const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || prev != key || prevb != b);
     const int seg = __popc(heads & ((2u << lane) - 1u));
+    int oseg[5];
+#pragma unroll
+    for (int s = 0; s < 5; ++s) oseg[s] = __shfl_down_sync(0xffffffffu, seg, 1 << s);
 #pragma unroll
     for (int k = 0; k < 12; ++k) {
         float v = acc.g[k];
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const float ov = __shfl_down_sync(0xffffffffu, v, o);
-            const int os = __shfl_down_sync(0xffffffffu, seg, o);
-            if (lane + o < 32 && os == seg) v += ov;
+        for (int s = 0; s < 5; ++s) {
+            const float ov = __shfl_down_sync(0xffffffffu, v, 1 << s);
+            if (lane + (1 << s) < 32 && oseg[s] == seg) v += ov;
         }
         acc.g[k] = v;
     }
@@ -378,8 +385,8 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     if (rc || (rc = mark(5, st))) return rc;
 
     // edge gradients to clip-space positions
-    edge_step_kernel<<<blocks_for(num_pixels, 128), 128, 0, st>>>(c.B, views, num_pixels, c.V, w.pos, tri, a.color,
-                                                                  w.grad_color, rast, w.grad_pos);
+    edge_step_kernel<<<blocks_for(num_pixels, kEdgeThreads), kEdgeThreads, 0, st>>>(
+        c.B, views, num_pixels, c.V, c.T, w.pos, tri, a.color, w.grad_color, rast, w.grad_pos);
     if ((rc = mark(6, st))) return rc;
     // adjoints of sigmoid + level accumulation, and of the projection
     if (c.T > 0) {
