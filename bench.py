@@ -39,6 +39,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "fwd+bwd views/s @15K tris 800²: batched BF16 vs plain FP32 on one B200"
+# kernels one training step launches: accumulate+sigmoid x2, project | bin_setup, 3 scan kernels,
+# bin_fill, sort_lists | raster | shade | aux from records, aux of re-enumerated blocks | edge |
+# accumulate+sigmoid backward x2, project backward, finish
+KERNELS_PER_STEP = 18
 WORKLOAD = "config2: 15K-tri sphere-shell soup, 8 views 800x800, levels 0..2 x 8 ch, MLP 11-16-3, stochastic opacity"
 N_INPUT_SETS = 4  # rotating view batches: 4 x 61 MB of targets, larger than the 126 MB L2
 
@@ -189,10 +193,11 @@ def algorithmic_bytes(phase: str, P_: int, B: int, T: int, V: int, ST: int, C_: 
     """Minimal DRAM bytes of one launch of each step kernel."""
     if phase == "shade":  # rast 16 R, target 12 R, colour 12 W, dL/dcolour 12 W, |c-t| 4 W; bf16 features + fp32 grads
         return P_ * 56.0 + T * ST * C_ * (2 + 8)
-    if phase == "raster":  # rast 16 W per pixel; triangle records 64 B per (view, tri); opacity table
-        return P_ * 16.0 + B * T * 64.0 + T * ST * 4.0
-    if phase == "aux":  # rast 16 R + |c-t| 4 R per pixel; records; opacity table + grads
-        return P_ * 20.0 + B * T * 64.0 + T * ST * 12.0
+    # fragment records: 16 B each, about one per pixel on this workload (fragments in front of the surface)
+    if phase == "raster":  # rast 16 W + records 16 W per pixel; triangle records 64 B per (view, tri); opacities
+        return P_ * 32.0 + B * T * 64.0 + T * ST * 4.0
+    if phase == "aux":  # records 16 R + |c-t| 4 R per record; opacity table + grads
+        return P_ * 20.0 + T * ST * 12.0
     if phase == "edge":  # rast 16 + colour 12 + dL/dcolour 12 per pixel; clip positions + fp64 grads
         return P_ * 40.0 + B * V * (16.0 + 64.0)
     if phase == "bin":
@@ -372,7 +377,7 @@ def run_ours(args):
                    "l2": f"{N_INPUT_SETS} rotating input sets (4 x 61 MB targets) larger than L2",
                    "list_overflow": overflow},
         "e2e": {"value": e2e, "unit": "views/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 4},
-        "gpu_launches": 16 * args.steps,
+        "gpu_launches": KERNELS_PER_STEP * args.steps,
         "clocks": clocks,
         "phase_ms": {k: round(v, 4) for k, v in phase_ms.items()},
         "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -5,6 +5,7 @@
 #pragma once
 
 #include "geometry.cuh"
+#include "tiled.cuh"
 
 namespace dsb {
 
@@ -37,11 +38,10 @@ __device__ __forceinline__ bool segment_intersect2d(float x0, float y0, float x1
 
 // Which triangle edge the pixel-pair segment crosses, and the perspective-
 // correct edge weights at the crossing (rasterize.cu:546-604).
-__device__ __forceinline__ bool find_edge_intersection(const float4 P[3], float x0, float y0, float x1, float y1,
-                                                       int& i0, int& i1, float& s0, float& s1) {
-    float rx[3], ry[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) { rx[k] = P[k].x / P[k].w; ry[k] = P[k].y / P[k].w; }
+// As find_edge_intersection, given the vertices' NDC rx, ry (x / w, y / w).
+__device__ __forceinline__ bool find_edge_intersection_ndc(const float4 P[3], const float rx[3], const float ry[3],
+                                                           float x0, float y0, float x1, float y1, int& i0, int& i1,
+                                                           float& s0, float& s1) {
     float ix = 0.f, iy = 0.f;
     if (segment_intersect2d(x0, y0, x1, y1, rx[0], ry[0], rx[1], ry[1], ix, iy)) { i0 = 0; i1 = 1; }
     else if (segment_intersect2d(x0, y0, x1, y1, rx[1], ry[1], rx[2], ry[2], ix, iy)) { i0 = 1; i1 = 2; }
@@ -56,6 +56,14 @@ __device__ __forceinline__ bool find_edge_intersection(const float4 P[3], float 
     const float t = den != 0.f ? -(ax * bx + ay * by) / den : 0.5f;
     s0 = 1.f - t; s1 = t;
     return true;
+}
+
+__device__ __forceinline__ bool find_edge_intersection(const float4 P[3], float x0, float y0, float x1, float y1,
+                                                       int& i0, int& i1, float& s0, float& s1) {
+    float rx[3], ry[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { rx[k] = P[k].x / P[k].w; ry[k] = P[k].y / P[k].w; }
+    return find_edge_intersection_ndc(P, rx, ry, x0, y0, x1, y1, i0, i1, s0, s1);
 }
 
 // Unit normal of the triangle in NDC (rasterize.cu:608-633).
@@ -241,8 +249,10 @@ __device__ __forceinline__ float pair_adjoint3(const float* c0, const float* g0,
 
 __device__ __forceinline__ int edge_grad_pixel_split(int y0, int x0, int H, int W, const float* __restrict__ color,
                                                      const float* __restrict__ grad_color,
-                                                     const float* __restrict__ rast, const float* __restrict__ posb,
-                                                     const int* __restrict__ tri, int64_t base, EdgeAccum& acc) {
+                                                     const float* __restrict__ rast,
+                                                     const TriVerts* __restrict__ tverts,
+                                                     const TriBox* __restrict__ tboxes,
+                                                     const TriNdc* __restrict__ tndc, int64_t base, EdgeAccum& acc) {
 #pragma unroll
     for (int k = 0; k < 12; ++k) acc.g[k] = 0.f;
     acc.any = false;
@@ -257,8 +267,10 @@ __device__ __forceinline__ int edge_grad_pixel_split(int y0, int x0, int H, int 
     const float nx0 = -1.f + ((float)x0 + 0.5f) * sx;
     const float ny0 = -1.f + ((float)y0 + 0.5f) * sy;
     float4 P0[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) P0[k] = load_vertex(posb, __ldg(tri + it0 * 3 + k));
+    {
+        const TriVerts v = tverts[it0];
+        P0[0] = v.p0; P0[1] = v.p1; P0[2] = v.p2;
+    }
     float c0[3], g0[3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) { c0[i] = color[pix0 * 3 + i]; g0[i] = grad_color[pix0 * 3 + i]; }
@@ -308,10 +320,16 @@ __device__ __forceinline__ int edge_grad_pixel_split(int y0, int x0, int H, int 
         float tb0, tb1, cz1, cw1;
         if (intersect_triangle(ny1, nx1, P0[0], P0[1], P0[2], tb0, tb1, cz1, cw1)) {
             const float d1_it0 = cz1 / cw1;
+            // it1 hides it0 at the neighbour.  Only a triangle intersection
+            // contributes, which needs it1 behind it0 at this pixel: never
+            // when it1's depth bound lies in front of depth0.
             if (it1 >= 0 && depth1 < d1_it0) {
+                if (tboxes[it1].zhi < depth0) continue;
                 float4 P1[3];
-#pragma unroll
-                for (int k = 0; k < 3; ++k) P1[k] = load_vertex(posb, __ldg(tri + it1 * 3 + k));
+                {
+                    const TriVerts v = tverts[it1];
+                    P1[0] = v.p0; P1[1] = v.p1; P1[2] = v.p2;
+                }
                 float cz0, cw0;
                 if (intersect_triangle(ny0, nx0, P1[0], P1[1], P1[2], tb0, tb1, cz0, cw0)) {
                     const float d0_it1 = cz0 / cw0;
@@ -338,7 +356,9 @@ __device__ __forceinline__ int edge_grad_pixel_split(int y0, int x0, int H, int 
         } else if (it1 < 0 || depth0 < depth1) {  // active geometric edge
             int i0, i1;
             float s0, s1;
-            if (find_edge_intersection(P0, nx0, ny0, nx1, ny1, i0, i1, s0, s1)) {
+            const TriNdc q = tndc[it0];
+            const float rx[3] = {q.a.x, q.a.z, q.b.x}, ry[3] = {q.a.y, q.a.w, q.b.y};
+            if (find_edge_intersection_ndc(P0, rx, ry, nx0, ny0, nx1, ny1, i0, i1, s0, s1)) {
                 const float4 A = i0 == 0 ? P0[0] : (i0 == 1 ? P0[1] : P0[2]);
                 const float4 Bv = i1 == 0 ? P0[0] : (i1 == 1 ? P0[1] : P0[2]);
                 const float cx = s0 * A.x + s1 * Bv.x;

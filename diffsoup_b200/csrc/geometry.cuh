@@ -101,6 +101,51 @@ __device__ __forceinline__ bool surely_outside(float A0, float A1, float A2, flo
     return false;
 }
 
+// True only when no pixel centre of a block, whose pixel-centre NDC
+// coordinates span [xa, xb] x [ya, yb], can pass the reference's coverage
+// test.  The edge terms are affine in the NDC point, so over the block their
+// extremes (and those of |A| + |A0| + |A1|, a convex function) lie at its
+// corners.  The reference's A_k at any pixel, and the value computed here at
+// a corner, differ from the exact affine value by at most
+// 4u (|q1x q2y| + |q1y q2x|) (u = 2^-24); the margins t_k = 2^-18 S_k, with
+// S_k a bound of those products over the block, cover both.  The block is
+// rejected when A keeps one sign with 2^-60 <= |A| <= 2^60 everywhere and
+// b0 or b1 is negative everywhere, or the b2 condition of surely_outside
+// holds everywhere.  NaN anywhere rejects nothing.
+__device__ __forceinline__ bool block_surely_outside(float4 p0, float4 p1, float4 p2, float xa, float xb, float ya,
+                                                     float yb) {
+    // bounds of |q| = |p.xy - ndc p.w| over the block, and the margins
+    float t0, t1, t2;
+    {
+        const float qx0 = fmaxf(fabsf(p0.x - xa * p0.w), fabsf(p0.x - xb * p0.w));
+        const float qx1 = fmaxf(fabsf(p1.x - xa * p1.w), fabsf(p1.x - xb * p1.w));
+        const float qx2 = fmaxf(fabsf(p2.x - xa * p2.w), fabsf(p2.x - xb * p2.w));
+        const float qy0 = fmaxf(fabsf(p0.y - ya * p0.w), fabsf(p0.y - yb * p0.w));
+        const float qy1 = fmaxf(fabsf(p1.y - ya * p1.w), fabsf(p1.y - yb * p1.w));
+        const float qy2 = fmaxf(fabsf(p2.y - ya * p2.w), fabsf(p2.y - yb * p2.w));
+        t0 = 0x1p-18f * (qx1 * qy2 + qy1 * qx2);
+        t1 = 0x1p-18f * (qx2 * qy0 + qy2 * qx0);
+        t2 = 0x1p-18f * (qx0 * qy1 + qy0 * qx1);
+    }
+    const float tA = t0 + t1 + t2;
+    bool pos = false, r0 = true, r1 = true;
+    float m = 0.f, a2 = -INFINITY;  // max of |A| + |A0| + |A1| and of the signed A2 over the corners
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        float A0, A1, A2, A;
+        edge_terms((c & 2) ? yb : ya, (c & 1) ? xb : xa, p0, p1, p2, A0, A1, A2, A);
+        const float aA = fabsf(A);
+        if (c == 0) pos = A > 0.f;
+        if (!(aA - tA >= 0x1p-60f && aA + tA <= 0x1p60f) || (A > 0.f) != pos) return false;
+        r0 = r0 && (pos ? A0 : -A0) < -t0;
+        r1 = r1 && (pos ? A1 : -A1) < -t1;
+        m = fmaxf(m, aA + fabsf(A0) + fabsf(A1));
+        a2 = fmaxf(a2, pos ? A2 : -A2);
+    }
+    if (r0 || r1) return true;
+    return a2 < -(t2 + 0x1p-19f * (m + tA));
+}
+
 // Remainder of intersect_triangle given its edge terms (A != 0).
 __device__ __forceinline__ bool finish_coverage(float A0, float A1, float A, float4 p0, float4 p1, float4 p2,
                                                 float& b0, float& b1, float& z, float& w) {

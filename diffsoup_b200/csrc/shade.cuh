@@ -45,6 +45,10 @@ struct ShadeCfg {
     static constexpr int P_WO = P_WH + (NL - 1) * (HID * HID + HID);
     static constexpr int P_BO = P_WO + OUT * HID;
     static constexpr int NPARAM = P_BO + OUT;
+    // Small MLPs keep their weight and bias gradients in registers for the
+    // whole kernel (mma accumulators that persist across pixel chunks)
+    // instead of adding every chunk's tiles into shared memory.
+    static constexpr bool REG_GRADS = NL == 1 && HID * IN_PAD <= 256;
     static_assert(IN_PAD % 16 == 0 && IN_PAD >= IN_REAL && HID % 16 == 0, "MLP dims");
     static_assert((LDX * 2) % 16 == 0 && (LDH * 2) % 16 == 0 && (LDO * 2) % 16 == 0, "ldmatrix row alignment");
 };
@@ -109,7 +113,7 @@ __device__ __forceinline__ float2 relu_gate(const __nv_bfloat16* h, float2 v) {
 }
 
 template <class K>
-__global__ void __launch_bounds__(K::WARPS * 32) shade_step_kernel(ShadeArgs a) {
+__global__ void __launch_bounds__(K::WARPS * 32, K::REG_GRADS ? 5 : 1) shade_step_kernel(ShadeArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ShadeSmem<K>& sm = *reinterpret_cast<ShadeSmem<K>*>(smem_raw);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -140,6 +144,22 @@ __global__ void __launch_bounds__(K::WARPS * 32) shade_step_kernel(ShadeArgs a) 
 
     ShadeWarpSmem<K>& ws = sm.w[warp];
     float loss_acc = 0.f;
+    // REG_GRADS: per-lane partial gradients (mma accumulator layout)
+    constexpr int GW0M = K::REG_GRADS ? HID / 16 : 1, GW0N = K::REG_GRADS ? IN_PAD / 8 : 1;
+    constexpr int GWO = K::REG_GRADS ? HID / 8 : 1;
+    float gw0[GW0M][GW0N][4], gwo[GWO][4], gbh[GWO][2], gbo[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int i = 0; i < GW0M; ++i)
+#pragma unroll
+        for (int j = 0; j < GW0N; ++j)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) gw0[i][j][k] = 0.f;
+#pragma unroll
+    for (int i = 0; i < GWO; ++i) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) gwo[i][k] = 0.f;
+        gbh[i][0] = gbh[i][1] = 0.f;
+    }
     const int64_t nchunks = (a.num_pixels + 31) / 32;
     for (int64_t chunk = (int64_t)blockIdx.x * K::WARPS + warp; chunk < nchunks;
          chunk += (int64_t)gridDim.x * K::WARPS) {
@@ -185,12 +205,20 @@ __global__ void __launch_bounds__(K::WARPS * 32) shade_step_kernel(ShadeArgs a) 
             x[K::C + 0] = d[0]; x[K::C + 1] = d[1]; x[K::C + 2] = d[2];
         }
         {
+            // 16-byte stores: rows are 16-byte aligned and, at these strides,
+            // the 8 lanes of each store phase hit distinct bank groups
             __nv_bfloat16* xr = ws.X + lane * K::LDX;
 #pragma unroll
-            for (int c = 0; c < IN_PAD; c += 2) {
-                const float v0 = c < K::IN_REAL ? x[c < K::IN_REAL ? c : 0] : 0.f;
-                const float v1 = c + 1 < K::IN_REAL ? x[c + 1 < K::IN_REAL ? c + 1 : 0] : 0.f;
-                *reinterpret_cast<uint32_t*>(xr + c) = pack_bf16(v0, v1);
+            for (int c = 0; c < IN_PAD; c += 8) {
+                uint32_t u[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int c0 = c + 2 * j, c1 = c + 2 * j + 1;
+                    const float v0 = c0 < K::IN_REAL ? x[c0 < K::IN_REAL ? c0 : 0] : 0.f;
+                    const float v1 = c1 < K::IN_REAL ? x[c1 < K::IN_REAL ? c1 : 0] : 0.f;
+                    u[j] = pack_bf16(v0, v1);
+                }
+                *reinterpret_cast<uint4*>(xr + c) = make_uint4(u[0], u[1], u[2], u[3]);
             }
         }
         __syncwarp();
@@ -291,18 +319,21 @@ __global__ void __launch_bounds__(K::WARPS * 32) shade_step_kernel(ShadeArgs a) 
         }
         {
             __nv_bfloat16* dr = ws.DZO + lane * K::LDO;
-            *reinterpret_cast<uint32_t*>(dr + 0) = pack_bf16(dz[0], dz[1]);
-            *reinterpret_cast<uint32_t*>(dr + 2) = pack_bf16(dz[2], 0.f);
-#pragma unroll
-            for (int c = 4; c < 16; c += 2) *reinterpret_cast<uint32_t*>(dr + c) = 0u;
+            *reinterpret_cast<uint4*>(dr) = make_uint4(pack_bf16(dz[0], dz[1]), pack_bf16(dz[2], 0.f), 0u, 0u);
+            *reinterpret_cast<uint4*>(dr + 8) = make_uint4(0u, 0u, 0u, 0u);
         }
         // output-layer bias gradient: column sums of dz over the warp
+        if (K::REG_GRADS) {
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            float v = dz[c];
+            for (int c = 0; c < 3; ++c) gbo[c] += dz[c];
+        } else {
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0) atomicAdd(&sm.g[K::P_BO + c], v);
+            for (int c = 0; c < 3; ++c) {
+                float v = dz[c];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane == 0) atomicAdd(&sm.g[K::P_BO + c], v);
+            }
         }
         __syncwarp();
 
@@ -311,14 +342,15 @@ __global__ void __launch_bounds__(K::WARPS * 32) shade_step_kernel(ShadeArgs a) 
 #pragma unroll
         for (int nt = 0; nt < HID / 8; ++nt) {
             float acc[4] = {0.f, 0.f, 0.f, 0.f};
+            float* d = K::REG_GRADS ? gwo[nt < GWO ? nt : 0] : acc;
 #pragma unroll
             for (int kt = 0; kt < 2; ++kt) {
                 uint32_t af[4], bf[2];
                 load_a_t(af, ws.DZO, K::LDO, kt * 16, 0);
                 load_b_t(bf, ws.H[K::NL - 1], K::LDH, kt * 16, nt * 8);
-                mma_16816(acc, af, bf);
+                mma_16816(d, af, bf);
             }
-            if (g < K::OUT) {
+            if (!K::REG_GRADS && g < K::OUT) {
                 atomicAdd(&sm.g[K::P_WO + g * HID + nt * 8 + 2 * q], acc[0]);
                 atomicAdd(&sm.g[K::P_WO + g * HID + nt * 8 + 2 * q + 1], acc[1]);
             }
@@ -342,14 +374,19 @@ __global__ void __launch_bounds__(K::WARPS * 32) shade_step_kernel(ShadeArgs a) 
                 *reinterpret_cast<uint32_t*>(ws.DH[cur] + (mt * 16 + g + 8) * K::LDH + col) = pack_bf16(hi.x, hi.y);
                 const int pb = K::NL == 1 ? K::P_B0 : K::P_WH + (K::NL - 2) * (HID * HID + HID) + HID * HID;
                 float s0 = lo.x + hi.x, s1 = lo.y + hi.y;
+                if (K::REG_GRADS) {
+                    gbh[nt < GWO ? nt : 0][0] += s0;
+                    gbh[nt < GWO ? nt : 0][1] += s1;
+                } else {
 #pragma unroll
-                for (int o = 4; o < 32; o <<= 1) {
-                    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-                    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-                }
-                if (g == 0) {
-                    atomicAdd(&sm.g[pb + col], s0);
-                    atomicAdd(&sm.g[pb + col + 1], s1);
+                    for (int o = 4; o < 32; o <<= 1) {
+                        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+                        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+                    }
+                    if (g == 0) {
+                        atomicAdd(&sm.g[pb + col], s0);
+                        atomicAdd(&sm.g[pb + col + 1], s1);
+                    }
                 }
             }
         }
@@ -370,13 +407,15 @@ __global__ void __launch_bounds__(K::WARPS * 32) shade_step_kernel(ShadeArgs a) 
 #pragma unroll
                 for (int ni = 0; ni < nin / 8; ++ni) {
                     float acc[4] = {0.f, 0.f, 0.f, 0.f};
+                    float* d = K::REG_GRADS ? gw0[mh < GW0M ? mh : 0][ni < GW0N ? ni : 0] : acc;
 #pragma unroll
                     for (int kt = 0; kt < 2; ++kt) {
                         uint32_t af[4], bf[2];
                         load_a_t(af, ws.DH[cur], K::LDH, kt * 16, mh * 16);
                         load_b_t(bf, ain, ldin, kt * 16, ni * 8);
-                        mma_16816(acc, af, bf);
+                        mma_16816(d, af, bf);
                     }
+                    if (K::REG_GRADS) continue;
                     const int i0 = ni * 8 + 2 * q;
                     const int h0 = mh * 16 + g;
                     if (i0 < win) {
@@ -448,6 +487,49 @@ __global__ void __launch_bounds__(K::WARPS * 32) shade_step_kernel(ShadeArgs a) 
             }
         }
         __syncwarp();
+    }
+
+    if (K::REG_GRADS) {
+        // W0[h][i]: tile (mh, ni) holds rows h0 = mh*16 + g (+8), columns i0 = ni*8 + 2q (+1)
+#pragma unroll
+        for (int mh = 0; mh < GW0M; ++mh)
+#pragma unroll
+            for (int ni = 0; ni < GW0N; ++ni) {
+                const int i0 = ni * 8 + 2 * q, h0 = mh * 16 + g;
+                if (i0 < K::IN_REAL) {
+                    atomicAdd(&sm.g[K::P_W0 + h0 * K::IN_REAL + i0], gw0[mh][ni][0]);
+                    atomicAdd(&sm.g[K::P_W0 + (h0 + 8) * K::IN_REAL + i0], gw0[mh][ni][2]);
+                }
+                if (i0 + 1 < K::IN_REAL) {
+                    atomicAdd(&sm.g[K::P_W0 + h0 * K::IN_REAL + i0 + 1], gw0[mh][ni][1]);
+                    atomicAdd(&sm.g[K::P_W0 + (h0 + 8) * K::IN_REAL + i0 + 1], gw0[mh][ni][3]);
+                }
+            }
+#pragma unroll
+        for (int nt = 0; nt < GWO; ++nt) {
+            if (g < K::OUT) {
+                atomicAdd(&sm.g[K::P_WO + g * HID + nt * 8 + 2 * q], gwo[nt][0]);
+                atomicAdd(&sm.g[K::P_WO + g * HID + nt * 8 + 2 * q + 1], gwo[nt][1]);
+            }
+            // hidden bias: sum over the rows g of the lane's columns
+            float s0 = gbh[nt][0], s1 = gbh[nt][1];
+#pragma unroll
+            for (int o = 4; o < 32; o <<= 1) {
+                s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+                s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+            }
+            if (g == 0) {
+                atomicAdd(&sm.g[K::P_B0 + nt * 8 + 2 * q], s0);
+                atomicAdd(&sm.g[K::P_B0 + nt * 8 + 2 * q + 1], s1);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            float v = gbo[c];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) atomicAdd(&sm.g[K::P_BO + c], v);
+        }
     }
 
     // ---- CTA reduction of the loss and the parameter gradients ----------------

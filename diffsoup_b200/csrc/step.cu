@@ -11,10 +11,12 @@
 //   adjoints of the sigmoid, the level accumulation and projection (finish)
 //
 // Views may differ in resolution; their pixels are packed back to back.
+#include <cmath>
 #include <cstdio>
 
 #include "edge_math.cuh"
 #include "shade.cuh"
+#include "tiled.cuh"
 
 namespace dsb {
 
@@ -141,13 +143,12 @@ constexpr int kEdgeThreads = 128;
 
 __global__ void __launch_bounds__(kEdgeThreads) edge_step_kernel(int B, const ds_view_desc* __restrict__ views,
                                                                  int64_t num_pixels, int V, int T,
-                                                                 const float* __restrict__ pos,
+                                                                 TileTables tab,
                                                                  const int* __restrict__ tri,
                                                                  const float* __restrict__ color,
                                                                  const float* __restrict__ grad_color,
                                                                  const float* __restrict__ rast,
                                                                  double* __restrict__ grad_pos) {
-    (void)T;
     const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     EdgeAccum acc;
@@ -160,8 +161,9 @@ __global__ void __launch_bounds__(kEdgeThreads) edge_step_kernel(int B, const ds
         const ds_view_desc vd = views[b];
         const int local = (int)(p - vd.pix_offset);  // < H*W < 2^31: 32-bit division
         const int y = local / vd.W, x = local - y * vd.W;
-        it0 = edge_grad_pixel_split(y, x, vd.H, vd.W, color, grad_color, rast, pos + (size_t)b * V * 4, tri,
-                                    vd.pix_offset, acc);
+        const size_t tb = (size_t)b * T;
+        it0 = edge_grad_pixel_split(y, x, vd.H, vd.W, color, grad_color, rast, tab.verts + tb, tab.boxes + tb,
+                                    tab.ndc + tb, vd.pix_offset, acc);
     }
     const int key = (it0 >= 0 && acc.any) ? it0 : -1 - lane;
     const int prev = __shfl_up_sync(0xffffffffu, key, 1);
@@ -195,10 +197,12 @@ __global__ void __launch_bounds__(kEdgeThreads) edge_step_kernel(int B, const ds
 }
 
 __global__ void finish_kernel(const double* __restrict__ loss_sum, float inv_n, float* __restrict__ loss,
-                              uint64_t* __restrict__ rng) {
+                              uint64_t* __restrict__ rng, const int* __restrict__ rec_counters,
+                              int* __restrict__ status) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         *loss = (float)(*loss_sum * (double)inv_n);
         if (rng) rng[1] += 1;  // next iteration of the opacity-threshold RNG
+        if (status && rec_counters[1] > 0) atomicOr(status, DS_STATUS_RECORD_FALLBACK);
     }
 }
 
@@ -245,9 +249,21 @@ struct StepWs {
     float* grad_alpha_acc;
     float* grad_feat_acc;
     double* loss_sum;
+    int* rec_counters;  // [2], zeroed with the accumulators
     void* tiles;
     size_t tiles_bytes;
+    RecordStore rec;    // rec.capacity == 0: no records
 };
+
+// Fragment records reserved for P pixels: frag_records per pixel plus one
+// chunk for every warp of the rasterizer's grid (each warp's last chunk is
+// partly filled), a multiple of the chunk size.
+static int64_t record_capacity(const ds_step_config& c, int num_tiles, int64_t P) {
+    if (!(c.frag_records > 0.f)) return 0;
+    const double n = std::ceil((double)P * (double)c.frag_records / kRecChunk);
+    const int64_t items = (int64_t)num_tiles * 8;
+    return ((int64_t)n + (items < kMaxTileWarps ? items : kMaxTileWarps)) * kRecChunk;
+}
 
 static StepWs carve_step(void* ws, const ds_step_config& c, int num_tiles, int64_t P, int64_t cap, size_t* total) {
     char* base = reinterpret_cast<char*>(ws);
@@ -266,10 +282,18 @@ static StepWs carve_step(void* ws, const ds_step_config& c, int num_tiles, int64
     w.grad_pos = reinterpret_cast<double*>(base + o); o += al((size_t)c.B * c.V * 32);
     w.grad_alpha_acc = reinterpret_cast<float*>(base + o); o += al((size_t)c.T * ST * 4);
     w.grad_feat_acc = reinterpret_cast<float*>(base + o); o += al((size_t)c.T * ST * c.C * 4);
-    w.loss_sum = reinterpret_cast<double*>(base + o); o += 256;
+    w.loss_sum = reinterpret_cast<double*>(base + o);
+    w.rec_counters = reinterpret_cast<int*>(base + o + 64);
+    o += 256;
     w.tiles = base + o;
     w.tiles_bytes = ds_tiles_workspace_size(c.B, c.T, num_tiles, cap);
     o += al(w.tiles_bytes);
+    const int64_t rcap = record_capacity(c, num_tiles, P);
+    w.rec.capacity = rcap;
+    w.rec.counters = w.rec_counters;
+    w.rec.rec = reinterpret_cast<int4*>(base + o); o += al((size_t)rcap * sizeof(int4));
+    w.rec.chunk_fill = reinterpret_cast<int*>(base + o); o += al((size_t)(rcap / kRecChunk) * sizeof(int));
+    w.rec.fallback = reinterpret_cast<int*>(base + o); o += al(rcap > 0 ? (size_t)num_tiles * 8 * sizeof(int) : 0);
     if (total) *total = o;
     return w;
 }
@@ -306,9 +330,11 @@ int ds_train_step_layout(const ds_step_config* cfg, int num_tiles, int64_t num_p
                          int64_t* offsets) {
     DS_CHECK_ARG(cfg != nullptr && offsets != nullptr, "train_step_layout: null argument");
     StepWs w = carve_step(nullptr, *cfg, num_tiles, num_pixels, list_capacity, nullptr);
-    const void* ptrs[11] = {w.pos, w.alpha_acc, w.feat_acc, w.feat_bf16, w.rast, w.color, w.grad_color, w.l1,
-                            w.grad_pos, w.grad_alpha_acc, w.grad_feat_acc};
-    for (int i = 0; i < 11; ++i) offsets[i] = (int64_t)(reinterpret_cast<const char*>(ptrs[i]) - (const char*)nullptr);
+    const void* ptrs[15] = {w.pos, w.alpha_acc, w.feat_acc, w.feat_bf16, w.rast, w.color, w.grad_color, w.l1,
+                            w.grad_pos, w.grad_alpha_acc, w.grad_feat_acc, w.rec.rec, w.rec.chunk_fill,
+                            w.rec_counters, w.rec.fallback};
+    for (int i = 0; i < 15; ++i) offsets[i] = (int64_t)(reinterpret_cast<const char*>(ptrs[i]) - (const char*)nullptr);
+    offsets[15] = w.rec.capacity;
     return DS_OK;
 }
 
@@ -334,16 +360,20 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     const int S = (int)total_feats((uint32_t)c.min_level, (uint32_t)c.max_level);
     const int ST = (int)feats_at_level((uint32_t)c.max_level);
     DS_CHECK_ARG(S * c.C <= kMaxSrc, "train_step: %d samples x %d channels exceed the per-triangle limit", S, c.C);
+    DS_CHECK_ARG(num_pixels <= 0xffffffffLL, "train_step: more than 2^32 pixels");
+    DS_CHECK_ARG(c.frag_records >= 0.f && record_capacity(c, num_tiles, num_pixels) <= 0x7fffffffLL - kMaxTileWarps * kRecChunk,
+                 "train_step: frag_records %g gives too many records", (double)c.frag_records);
     size_t need = 0;
     StepWs w = carve_step(workspace, c, num_tiles, num_pixels, list_capacity, &need);
+    const RecordStore* rs = w.rec.capacity > 0 ? &w.rec : nullptr;
     if (workspace_bytes < need) return set_error(DS_ERR_WORKSPACE, "train_step: workspace too small");
     cudaStream_t st = (cudaStream_t)stream;
 
     int rc = mark(0, st);
     if (rc) return rc;
     // zero the accumulators of this step
-    DS_CUDA(cudaMemsetAsync(w.grad_pos, 0, reinterpret_cast<char*>(w.loss_sum) + 8 - reinterpret_cast<char*>(w.grad_pos),
-                            st));
+    DS_CUDA(cudaMemsetAsync(w.grad_pos, 0,
+                            reinterpret_cast<char*>(w.rec_counters + 2) - reinterpret_cast<char*>(w.grad_pos), st));
     DS_CUDA(cudaMemsetAsync(grad_mlp_params, 0, sizeof(float) * ds_mlp_param_count(c.C, c.hidden, c.n_layers), st));
 
     // prep: opacity and feature accumulation + sigmoid, projection
@@ -364,9 +394,8 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     rc = ds_tiles_bin(c.B, views, num_tiles, c.V, w.pos, c.T, tri, w.tiles, w.tiles_bytes, list_capacity, status,
                       stream);
     if (rc || (rc = mark(2, st))) return rc;
-    rc = ds_tiles_rasterize(c.B, views, num_tiles, c.V, w.pos, c.T, tri, c.max_level, ST, w.alpha_acc,
-                            c.stochastic ? 1 : 0, c.thr_const, rng, rast, w.tiles, w.tiles_bytes, list_capacity,
-                            stream);
+    rc = tiles_rasterize_impl(c.B, views, num_tiles, c.T, c.max_level, ST, w.alpha_acc, c.stochastic ? 1 : 0,
+                              c.thr_const, rng, rast, w.tiles, list_capacity, rs, st);
     if (rc || (rc = mark(3, st))) return rc;
 
     // fused shading forward + backward
@@ -380,13 +409,14 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     if (rc || (rc = mark(4, st))) return rc;
 
     // opacity auxiliary gradient (scaled by 1/numel(colour), rasterize.py:183-195)
-    rc = ds_tiles_opacity_aux(c.B, views, num_tiles, c.V, w.pos, c.T, tri, c.max_level, ST, w.alpha_acc, 1, w.l1,
-                              nullptr, rast, a.inv_n, w.grad_alpha_acc, w.tiles, w.tiles_bytes, list_capacity, stream);
+    rc = tiles_aux_impl(c.B, views, num_tiles, c.T, c.max_level, ST, w.alpha_acc, w.l1, rast, a.inv_n,
+                        w.grad_alpha_acc, w.tiles, list_capacity, rs, st);
     if (rc || (rc = mark(5, st))) return rc;
 
     // edge gradients to clip-space positions
     edge_step_kernel<<<blocks_for(num_pixels, kEdgeThreads), kEdgeThreads, 0, st>>>(
-        c.B, views, num_pixels, c.V, c.T, w.pos, tri, a.color, w.grad_color, rast, w.grad_pos);
+        c.B, views, num_pixels, c.V, c.T, tiles_tables(w.tiles, c.B, c.T, num_tiles, list_capacity), tri, a.color,
+        w.grad_color, rast, w.grad_pos);
     if ((rc = mark(6, st))) return rc;
     // adjoints of sigmoid + level accumulation, and of the projection
     if (c.T > 0) {
@@ -398,7 +428,7 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
                                                                       grad_feat_src);
     }
     if (c.V > 0) project_backward_kernel<<<blocks_for(c.V), kThreads, 0, st>>>(c.B, c.V, mvp, w.grad_pos, grad_verts);
-    finish_kernel<<<1, 32, 0, st>>>(w.loss_sum, a.inv_n, loss, c.stochastic ? rng : nullptr);
+    finish_kernel<<<1, 32, 0, st>>>(w.loss_sum, a.inv_n, loss, c.stochastic ? rng : nullptr, w.rec_counters, status);
     if ((rc = mark(7, st))) return rc;
     return check_launch("train_step");
 }

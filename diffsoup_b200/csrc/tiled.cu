@@ -19,24 +19,9 @@
 // before the depth comparison exactly as depth_test_kernel does.
 #include "edge_math.cuh"
 #include "scan.cuh"
+#include "tiled.cuh"
 
 namespace dsb {
-
-// Per (view, triangle): the pixel rect [y0, y1) x [x0, x1) (empty when
-// y1 <= y0) and bounds [zlo, zhi] on the NDC depth of every fragment the
-// triangle can produce.  With every w > 0 (the rect test culls the rest), a
-// fragment's depth z/w is a convex combination of the vertices' z_i/w_i, so
-// [min, max] of those bound it; the bounds are widened by the rounding of the
-// fragment arithmetic.
-struct __align__(16) TriBox {
-    short y0, y1, x0, x1;
-    float zlo, zhi;
-};
-static_assert(sizeof(TriBox) == 16, "TriBox layout");
-
-struct __align__(16) TriVerts {
-    float4 p0, p1, p2;
-};
 
 constexpr int kWarpsPerCta = 8;
 constexpr int kBlocksPerTile = 8;  // 8x4 pixel blocks of a 16x16 tile
@@ -46,6 +31,7 @@ constexpr int kAuxSmemS = 160;     // per-warp shared accumulator for lattices u
 struct TileWs {
     TriBox* boxes;
     TriVerts* verts;
+    TriNdc* ndc;
     int* counts;
     int64_t* offsets;  // [num_tiles + 1] exclusive prefix of counts
     int* cursor;
@@ -63,6 +49,7 @@ static TileWs carve(void* ws, int B, int T, int num_tiles, int64_t capacity, siz
     size_t o = 0;
     w.boxes = reinterpret_cast<TriBox*>(p + o); o += al256((size_t)B * T * sizeof(TriBox));
     w.verts = reinterpret_cast<TriVerts*>(p + o); o += al256((size_t)B * T * sizeof(TriVerts));
+    w.ndc = reinterpret_cast<TriNdc*>(p + o); o += al256((size_t)B * T * sizeof(TriNdc));
     w.counts = reinterpret_cast<int*>(p + o); o += al256((size_t)num_tiles * sizeof(int));
     w.offsets = reinterpret_cast<int64_t*>(p + o); o += al256((size_t)(num_tiles + 1) * sizeof(int64_t));
     w.cursor = reinterpret_cast<int*>(p + o); o += al256((size_t)num_tiles * sizeof(int));
@@ -91,11 +78,21 @@ __device__ __forceinline__ bool box_tiles(const TriBox& r, int& tx0, int& tx1, i
     return true;
 }
 
+// False only when no pixel centre of the tile can be covered by the
+// triangle (the conservative test of block_surely_outside over the tile's
+// 16x16 pixel centres).
+__device__ __forceinline__ bool tile_may_cover(const TriVerts& v, const ds_view_desc& vd, int tx, int ty) {
+    const int x = tx * DS_TILE, y = ty * DS_TILE;
+    return !block_surely_outside(v.p0, v.p1, v.p2, pix_ndc(x, vd.W), pix_ndc(x + DS_TILE - 1, vd.W), pix_ndc(y, vd.H),
+                                 pix_ndc(y + DS_TILE - 1, vd.H));
+}
+
 // Pass 1: boxes, vertices and per-tile counts.
 __global__ void __launch_bounds__(kThreads) bin_setup_kernel(int B, const ds_view_desc* __restrict__ views, int V,
                                                              const float* __restrict__ pos, int T,
                                                              const int* __restrict__ tri, TriBox* __restrict__ boxes,
-                                                             TriVerts* __restrict__ verts, int* __restrict__ counts) {
+                                                             TriVerts* __restrict__ verts, TriNdc* __restrict__ ndc,
+                                                             int* __restrict__ counts) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (int64_t)B * T) return;
     const int b = (int)(i / T), t = (int)(i % T);
@@ -119,15 +116,21 @@ __global__ void __launch_bounds__(kThreads) bin_setup_kernel(int B, const ds_vie
     if (!(r.zlo == r.zlo && r.zhi == r.zhi)) { r.zlo = -INFINITY; r.zhi = INFINITY; }  // NaN: no bounds
     boxes[i] = r;
     verts[i] = v;
+    TriNdc q;
+    q.a = make_float4(v.p0.x / v.p0.w, v.p0.y / v.p0.w, v.p1.x / v.p1.w, v.p1.y / v.p1.w);
+    q.b = make_float4(v.p2.x / v.p2.w, v.p2.y / v.p2.w, 0.f, 0.f);
+    ndc[i] = q;
     int tx0, tx1, ty0, ty1;
     if (!box_tiles(r, tx0, tx1, ty0, ty1)) return;
     for (int ty = ty0; ty <= ty1; ++ty)
-        for (int tx = tx0; tx <= tx1; ++tx) atomicAdd(counts + vd.tile_base + ty * vd.tiles_x + tx, 1);
+        for (int tx = tx0; tx <= tx1; ++tx)
+            if (tile_may_cover(v, vd, tx, ty)) atomicAdd(counts + vd.tile_base + ty * vd.tiles_x + tx, 1);
 }
 
 // Pass 2: scatter record indices into the per-tile lists.
 __global__ void __launch_bounds__(kThreads) bin_fill_kernel(int B, const ds_view_desc* __restrict__ views, int T,
                                                             const TriBox* __restrict__ boxes,
+                                                            const TriVerts* __restrict__ verts,
                                                             const int64_t* __restrict__ offsets,
                                                             int* __restrict__ cursor, int* __restrict__ list,
                                                             int64_t capacity, int* __restrict__ status) {
@@ -138,9 +141,11 @@ __global__ void __launch_bounds__(kThreads) bin_fill_kernel(int B, const ds_view
     const TriBox rc = boxes[i];
     int tx0, tx1, ty0, ty1;
     if (!box_tiles(rc, tx0, tx1, ty0, ty1)) return;
+    const TriVerts v = verts[i];
     bool over = false;
     for (int ty = ty0; ty <= ty1; ++ty)
         for (int tx = tx0; tx <= tx1; ++tx) {
+            if (!tile_may_cover(v, vd, tx, ty)) continue;  // the same test as the count pass
             const int tile = vd.tile_base + ty * vd.tiles_x + tx;
             const int64_t at = offsets[tile] + atomicAdd(cursor + tile, 1);
             if (at < capacity) list[at] = (int)i; else over = true;
@@ -295,22 +300,110 @@ __device__ __forceinline__ int stage_group(const BlockGeom& g, int64_t g0, const
     return __popc(mask);
 }
 
+// Per-warp buffer of the fragment records of one 8x4 block (REC kernels).
+constexpr int kRecCap = 192;
+
+struct WarpRecs {
+    int t[kRecCap];
+    float b0[kRecCap], b1[kRecCap], z[kRecCap];
+    unsigned char lane[kRecCap];
+    float fin_z[32];  // per lane: depth of the visible surface (+inf when empty)
+    int fin_t[32];    // per lane: visible triangle (-1 when empty)
+};
+
+__device__ __forceinline__ void push_fallback(const RecordStore& rs, int item) {
+    if ((threadIdx.x & 31) == 0) rs.fallback[atomicAdd(rs.counters + 1, 1)] = item;
+}
+
+// Writes the records of the finished block that lie in front of (or level
+// with) each lane's final surface into the warp's chunk, reserving a new
+// chunk when the current one is full.  `cid` = current chunk (-1: none,
+// -2: the store is exhausted), `cfill` = records in it.
+__device__ __noinline__ void flush_records(const RecordStore& rs, WarpRecs& R, int nrec, int item, uint32_t pix,
+                                              unsigned long long best, float bz, int& cid, int& cfill) {
+    const int lane = threadIdx.x & 31;
+    if (nrec > kRecCap) {
+        push_fallback(rs, item);
+        return;
+    }
+    R.fin_z[lane] = best == ~0ull ? INFINITY : bz;
+    // the visible triangle as the backward pass reads it back from rast (id + 1 stored as a float)
+    R.fin_t[lane] = best == ~0ull ? -1 : (int)(float)((uint32_t)(best & 0xffffffffu) + 1u) - 1;
+    __syncwarp();
+    int n = 0;
+    for (int j0 = 0; j0 < nrec; j0 += 32) {
+        const int j = j0 + lane;
+        const bool keep = j < nrec && R.z[j] <= R.fin_z[R.lane[j]];
+        n += __popc(__ballot_sync(0xffffffffu, keep));
+    }
+    if (n == 0) return;
+    if (cid == -1 || (cid >= 0 && cfill + n > kRecChunk)) {
+        if (cid >= 0 && lane == 0) rs.chunk_fill[cid] = cfill;
+        int base = 0;
+        if (lane == 0) base = atomicAdd(rs.counters, kRecChunk);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if ((int64_t)base + kRecChunk <= rs.capacity) {
+            cid = base / kRecChunk;
+        } else {
+            cid = -2;
+        }
+        cfill = 0;
+    }
+    if (cid == -2) {
+        push_fallback(rs, item);
+        return;
+    }
+    int at = cfill;
+    for (int j0 = 0; j0 < nrec; j0 += 32) {
+        const int j = j0 + lane;
+        const int jj = j < nrec ? j : 0;
+        const int src = R.lane[jj];
+        const uint32_t p = __shfl_sync(0xffffffffu, pix, src);
+        const bool keep = j < nrec && R.z[jj] <= R.fin_z[src];
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (keep) {
+            const int t = R.t[jj];
+            const uint32_t tv = (uint32_t)t | (t == R.fin_t[src] ? 0x80000000u : 0u);
+            rs.rec[(int64_t)cid * kRecChunk + at + __popc(m & ((1u << lane) - 1u))] =
+                make_int4((int)p, (int)tv, __float_as_int(R.b0[jj]), __float_as_int(R.b1[jj]));
+        }
+        at += __popc(m);
+    }
+    cfill = at;
+}
+
 // Forward: depth test with stochastic opacity.  Each warp walks the
 // triangles of its block front to back (the tile list is sorted by zlo) and
 // stops once the next triangle's depth bound lies behind the winner of every
 // lane: no later triangle can improve a key (the bound's margin keeps
 // bits(z+2) strictly larger).  Within a triangle, the divisions run only when
 // some lane survives the cheap edge-sign test.
-__global__ void __launch_bounds__(kWarpsPerCta * 32) raster_kernel(
+//
+// REC: also keeps every fragment whose depth key does not lie behind the
+// lane's current winner.  Winner keys only decrease, and every fragment at
+// or in front of a lane's final surface has zlo <= that depth <= the warp's
+// bound at every point of the walk, so the walk meets and keeps all of them;
+// at the end of the block those behind the final surface are dropped.
+#ifndef DSB_RASTER_MIN_CTAS
+#define DSB_RASTER_MIN_CTAS 4  // resident 8-warp CTAs per SM the register budget is sized for
+#endif
+
+template <bool REC>
+__global__ void __launch_bounds__(kWarpsPerCta * 32, DSB_RASTER_MIN_CTAS) raster_kernel(
     int B, const ds_view_desc* __restrict__ views, int num_tiles, int T, const TriBox* __restrict__ boxes,
     const TriVerts* __restrict__ verts, const int64_t* __restrict__ offsets, const int* __restrict__ sorted,
     const int* __restrict__ list, int64_t capacity, int level, int S, const float* __restrict__ alpha_src,
-    int thr_mode, float thr_const, const uint64_t* __restrict__ rng, int* work, float* __restrict__ rast) {
+    int thr_mode, float thr_const, const uint64_t* __restrict__ rng, int* work, float* __restrict__ rast,
+    RecordStore rs) {
     __shared__ WarpStage s_stage[kWarpsPerCta];
-    WarpStage& st = s_stage[threadIdx.x >> 5];
+    __shared__ WarpRecs s_rec[REC ? kWarpsPerCta : 1];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    WarpStage& st = s_stage[warp];
+    WarpRecs& R = s_rec[REC ? warp : 0];
     uint64_t seed = 0;
     uint32_t iter = 0;
     if (thr_mode == 1) { seed = rng[0]; iter = (uint32_t)rng[1]; }
+    int cid = -1, cfill = 0;  // REC: the warp's current record chunk
     const int items = num_tiles * kBlocksPerTile;
     for (int item = warp_next(work); item < items; item = warp_next(work)) {
         const BlockGeom g = block_geometry(item, B, views, T, offsets, sorted, capacity);
@@ -318,6 +411,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) raster_kernel(
         const uint32_t pixel_id = (uint32_t)(g.py * g.W + g.px);
         unsigned long long best = ~0ull;
         float bb0 = 0.f, bb1 = 0.f, bz = 0.f;
+        int nrec = 0;
         // max over the warp of the lanes' winning depth (+inf while a valid lane has none)
         float warp_far = warp_max(g.valid ? INFINITY : -INFINITY);
         for (int64_t g0 = g.begin; g0 < g.end; g0 += 32) {
@@ -336,25 +430,44 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) raster_kernel(
                 const bool cand = g.valid && g.px >= r.x0 && g.px < r.x1 && g.py >= r.y0 && g.py < r.y1 &&
                                   !surely_outside(A0, A1, A2, A);
                 if (!__any_sync(0xffffffffu, cand)) continue;  // warp-uniform
-                bool improved = false;
+                bool improved = false, rec = false;
+                float b0 = 0.f, b1 = 0.f, depth = 0.f;
+                const uint32_t t = (uint32_t)st.t[k];
                 if (cand) {
-                    float b0, b1, z, w;
+                    float z, w;
                     if (finish_coverage(A0, A1, A, p0, p1, p2, b0, b1, z, w)) {
-                        const float depth = __fdiv_rn(z, w);
-                        if (depth > -1.f && depth <= 1.f) {
-                            const uint32_t t = (uint32_t)st.t[k];
+                        depth = __fdiv_rn(z, w);
+                        if (depth >= -1.f && depth <= 1.f) {
                             const unsigned long long key = depth_key(depth, t);
-                            if (key < best) {
-                                const float alpha = interp_scalar(b0, b1, level, level, alpha_src + (size_t)t * S);
-                                const float thr = thr_mode == 1
-                                                      ? philox_uniform(seed, iter, (uint32_t)g.b, pixel_id, t)
-                                                      : thr_const;
-                                if (!(alpha < thr)) {
-                                    best = key; bb0 = b0; bb1 = b1; bz = depth;
-                                    improved = true;
+                            // keep it unless its depth key lies behind the current winner's: the
+                            // winner's key only decreases, so nothing at or in front of the final
+                            // surface is dropped (the winner's depth itself can grow within one
+                            // bits(z+2) step when a lower triangle index takes a tie)
+                            if (REC) rec = (key >> 32) <= (best >> 32);
+                            if (depth > -1.f) {
+                                if (key < best) {
+                                    const float alpha = interp_scalar(b0, b1, level, level, alpha_src + (size_t)t * S);
+                                    const float thr = thr_mode == 1
+                                                          ? philox_uniform(seed, iter, (uint32_t)g.b, pixel_id, t)
+                                                          : thr_const;
+                                    if (!(alpha < thr)) {
+                                        best = key; bb0 = b0; bb1 = b1; bz = depth;
+                                        improved = true;
+                                    }
                                 }
                             }
                         }
+                    }
+                }
+                if (REC) {
+                    const unsigned m = __ballot_sync(0xffffffffu, rec);
+                    if (m) {
+                        const int at = nrec + __popc(m & ((1u << lane) - 1u));
+                        if (rec && at < kRecCap) {
+                            R.t[at] = (int)t; R.b0[at] = b0; R.b1[at] = b1; R.z[at] = depth;
+                            R.lane[at] = (unsigned char)lane;
+                        }
+                        nrec += __popc(m);
                     }
                 }
                 if (__any_sync(0xffffffffu, improved))
@@ -367,22 +480,62 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) raster_kernel(
             if (best != ~0ull) o = make_float4(bb0, bb1, bz, (float)((uint32_t)(best & 0xffffffffu) + 1u));
             reinterpret_cast<float4*>(rast)[g.pix] = o;
         }
+        if (REC && nrec > 0) {
+            __syncwarp();
+            flush_records(rs, R, nrec, item, (uint32_t)g.pix, best, bz, cid, cfill);
+            __syncwarp();  // the buffer is rewritten by the next block
+        }
+    }
+    if (REC && cid >= 0 && lane == 0) rs.chunk_fill[cid] = cfill;
+}
+
+// dL/dalpha of one fragment scattered through the lattice adjoint
+// (rasterize.cu:951-970 followed by multires.cu:130-222).
+__device__ __forceinline__ void aux_scatter(float b0, float b1, int level, int S, const float* __restrict__ alpha_src,
+                                            int t, float loss, bool visible, float scale,
+                                            float* __restrict__ grad_alpha_src) {
+    const float alpha = interp_scalar(b0, b1, level, level, alpha_src + (size_t)t * S);
+    const float ga = aux_alpha_grad(loss, alpha, visible) * scale;
+    uint32_t idx[3];
+    float w[3];
+    lattice_cell(b0, b1, level, idx, w);
+    float* dst = grad_alpha_src + (size_t)t * S;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) atomicAdd(dst + idx[q], ga * w[q]);
+}
+
+// Opacity auxiliary gradient from the fragment records: one thread per
+// record, blocks stride over the chunks.
+__global__ void __launch_bounds__(kRecChunk) aux_records_kernel(RecordStore rs, int level, int S,
+                                                               const float* __restrict__ alpha_src,
+                                                               const float* __restrict__ l1, float scale,
+                                                               float* __restrict__ grad_alpha_src) {
+    const int64_t reserved = rs.counters[0];
+    const int64_t nchunks = (reserved < rs.capacity ? reserved : rs.capacity) / kRecChunk;
+    for (int64_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
+        if ((int)threadIdx.x >= rs.chunk_fill[c]) continue;
+        const int4 r = rs.rec[c * kRecChunk + threadIdx.x];
+        const uint32_t tv = (uint32_t)r.y;
+        aux_scatter(__int_as_float(r.z), __int_as_float(r.w), level, S, alpha_src, (int)(tv & 0x7fffffffu),
+                    l1[(uint32_t)r.x], (tv >> 31) != 0, scale, grad_alpha_src);
     }
 }
 
-// Opacity auxiliary gradient: re-enumerates each block's fragments and
-// scatters dL/dalpha through the lattice adjoint.  Fragments behind the
-// visible surface contribute nothing (rasterize.cu:950), so triangles whose
-// depth bound lies behind every lane's surface are never staged.  All lanes
-// of a warp work on the same triangle at a time, so contributions are summed
-// per warp in shared memory and flushed with one global atomic per touched
-// sample.
+// Opacity auxiliary gradient by re-enumeration: each block's fragments are
+// recomputed and dL/dalpha is scattered through the lattice adjoint.
+// Fragments behind the visible surface contribute nothing
+// (rasterize.cu:950), so triangles whose depth bound lies behind every
+// lane's surface are never staged.  All lanes of a warp work on the same
+// triangle at a time, so contributions are summed per warp in shared memory
+// and flushed with one global atomic per touched sample.  With item_list,
+// only the blocks listed there (*item_count of them) are processed.
 __global__ void __launch_bounds__(kWarpsPerCta * 32) aux_kernel(
     int B, const ds_view_desc* __restrict__ views, int num_tiles, int T, const TriBox* __restrict__ boxes,
     const TriVerts* __restrict__ verts, const int64_t* __restrict__ offsets, const int* __restrict__ sorted,
     const int* __restrict__ list, int64_t capacity, int level, int S, const float* __restrict__ alpha_src, int C,
     const float* __restrict__ color, const float* __restrict__ target, const float* __restrict__ rast, float scale,
-    int* work, float* __restrict__ grad_alpha_src) {
+    const int* __restrict__ item_list, const int* __restrict__ item_count, int* work,
+    float* __restrict__ grad_alpha_src) {
     __shared__ WarpStage s_stage[kWarpsPerCta];
     __shared__ float s_acc[kWarpsPerCta][kAuxSmemS];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -391,8 +544,9 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) aux_kernel(
     if (use_smem)
         for (int k = lane; k < S; k += 32) s_acc[warp][k] = 0.f;
     __syncwarp();
-    const int items = num_tiles * kBlocksPerTile;
-    for (int item = warp_next(work); item < items; item = warp_next(work)) {
+    const int items = item_list ? *item_count : num_tiles * kBlocksPerTile;
+    for (int n = warp_next(work); n < items; n = warp_next(work)) {
+        const int item = item_list ? item_list[n] : n;
         const BlockGeom g = block_geometry(item, B, views, T, offsets, sorted, capacity);
         const float ndc_x = pix_ndc(g.px, g.W), ndc_y = pix_ndc(g.py, g.H);
         int tp = -1;
@@ -431,33 +585,28 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) aux_kernel(
                         hit = depth >= -1.f && depth <= 1.f && !(tp >= 0 && depth > zp);
                     }
                 }
-                uint32_t idx[3] = {0, 0, 0};
-                float gw[3] = {0.f, 0.f, 0.f};
+                if (!use_smem) {
+                    if (hit) aux_scatter(b0, b1, level, S, alpha_src, t, loss, tp >= 0 && t == tp, scale,
+                                         grad_alpha_src);
+                    continue;
+                }
+                if (!__any_sync(0xffffffffu, hit)) continue;
                 if (hit) {
                     const float alpha = interp_scalar(b0, b1, level, level, alpha_src + (size_t)t * S);
                     const float ga = aux_alpha_grad(loss, alpha, tp >= 0 && t == tp) * scale;
+                    uint32_t idx[3];
                     float w[3];
                     lattice_cell(b0, b1, level, idx, w);
-                    gw[0] = ga * w[0]; gw[1] = ga * w[1]; gw[2] = ga * w[2];
-                }
-                if (use_smem) {
-                    if (!__any_sync(0xffffffffu, hit)) continue;
-                    if (hit) {
 #pragma unroll
-                        for (int q = 0; q < 3; ++q) atomicAdd(&s_acc[warp][idx[q]], gw[q]);
-                    }
-                    __syncwarp();
-                    float* dst = grad_alpha_src + (size_t)t * S;
-                    for (int q = lane; q < S; q += 32) {
-                        const float v = s_acc[warp][q];
-                        if (v != 0.f) { atomicAdd(dst + q, v); s_acc[warp][q] = 0.f; }
-                    }
-                    __syncwarp();
-                } else if (hit) {
-                    float* dst = grad_alpha_src + (size_t)t * S;
-#pragma unroll
-                    for (int q = 0; q < 3; ++q) atomicAdd(dst + idx[q], gw[q]);
+                    for (int q = 0; q < 3; ++q) atomicAdd(&s_acc[warp][idx[q]], ga * w[q]);
                 }
+                __syncwarp();
+                float* dst = grad_alpha_src + (size_t)t * S;
+                for (int q = lane; q < S; q += 32) {
+                    const float v = s_acc[warp][q];
+                    if (v != 0.f) { atomicAdd(dst + q, v); s_acc[warp][q] = 0.f; }
+                }
+                __syncwarp();
             }
             __syncwarp();
         }
@@ -500,14 +649,15 @@ int ds_tiles_bin(int B, const ds_view_desc* views, int num_tiles, int V, const f
     DS_CUDA(cudaMemsetAsync(w.cursor, 0, (size_t)num_tiles * sizeof(int), st));
     const int64_t n = (int64_t)B * T;
     if (n > 0)
-        bin_setup_kernel<<<blocks_for(n), kThreads, 0, st>>>(B, views, V, pos, T, tri, w.boxes, w.verts, w.counts);
+        bin_setup_kernel<<<blocks_for(n), kThreads, 0, st>>>(B, views, V, pos, T, tri, w.boxes, w.verts, w.ndc,
+                                                              w.counts);
     int64_t* total_dev = nullptr;
     rc = device_scan<int, int64_t>(w.counts, num_tiles, w.offsets, false, w.scan, st, &total_dev);
     if (rc) return rc;
     // offsets[num_tiles] = total number of entries
     DS_CUDA(cudaMemcpyAsync(w.offsets + num_tiles, total_dev, sizeof(int64_t), cudaMemcpyDeviceToDevice, st));
     if (n > 0)
-        bin_fill_kernel<<<blocks_for(n), kThreads, 0, st>>>(B, views, T, w.boxes, w.offsets, w.cursor, w.list,
+        bin_fill_kernel<<<blocks_for(n), kThreads, 0, st>>>(B, views, T, w.boxes, w.verts, w.offsets, w.cursor, w.list,
                                                             list_capacity, status);
     if (num_tiles > 0)
         sort_lists_kernel<<<(unsigned)((num_tiles + kWarpsPerCta - 1) / kWarpsPerCta), kWarpsPerCta * 32, 0, st>>>(
@@ -515,13 +665,82 @@ int ds_tiles_bin(int B, const ds_view_desc* views, int num_tiles, int V, const f
     return check_launch("tiles_bin");
 }
 
-static unsigned block_grid(int num_tiles) {
-    const int per_sm = 4;  // 8-warp CTAs, ~14 KB shared each
+}  // extern "C"
+
+namespace dsb {
+
+// Persistent grid: as many 8-warp CTAs as fit on the SMs (queried once per
+// kernel), capped by the number of blocks.
+static unsigned block_grid(int num_tiles, const void* kernel, int& per_sm) {
+    if (per_sm == 0) {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, kWarpsPerCta * 32, 0) != cudaSuccess || n < 1)
+            n = 1;
+        per_sm = n;
+    }
     const int64_t warps = (int64_t)num_tiles * kBlocksPerTile;
     const int64_t ctas = (warps + kWarpsPerCta - 1) / kWarpsPerCta;
     const int64_t cap = (int64_t)kSMs * per_sm;
     return (unsigned)(ctas < 1 ? 1 : (ctas < cap ? ctas : cap));
 }
+
+static int g_occ_raster = 0, g_occ_raster_rec = 0, g_occ_aux = 0;
+
+int tiles_rasterize_impl(int B, const ds_view_desc* views, int num_tiles, int T, int level, int S,
+                         const float* alpha_src, int thr_mode, float thr_const, const uint64_t* rng, float* rast,
+                         void* workspace, int64_t list_capacity, const RecordStore* rs, cudaStream_t st) {
+    if (num_tiles == 0) return DS_OK;
+    TileWs w = carve(workspace, B, T, num_tiles, list_capacity, nullptr);
+    DS_CUDA(cudaMemsetAsync(w.work, 0, sizeof(int), st));
+    if (rs != nullptr) {
+        const void* k = reinterpret_cast<const void*>(&raster_kernel<true>);
+        raster_kernel<true><<<block_grid(num_tiles, k, g_occ_raster_rec), kWarpsPerCta * 32, 0, st>>>(
+            B, views, num_tiles, T, w.boxes, w.verts, w.offsets, w.sorted, w.list, list_capacity, level, S,
+            alpha_src, thr_mode, thr_const, rng, w.work, rast, *rs);
+    } else {
+        const void* k = reinterpret_cast<const void*>(&raster_kernel<false>);
+        raster_kernel<false><<<block_grid(num_tiles, k, g_occ_raster), kWarpsPerCta * 32, 0, st>>>(
+            B, views, num_tiles, T, w.boxes, w.verts, w.offsets, w.sorted, w.list, list_capacity, level, S,
+            alpha_src, thr_mode, thr_const, rng, w.work, rast, RecordStore{});
+    }
+    return check_launch("tiles_rasterize");
+}
+
+static int aux_launch(int B, const ds_view_desc* views, int num_tiles, int T, int level, int S,
+                      const float* alpha_src, int C, const float* color, const float* target, const float* rast,
+                      float scale, float* grad_alpha_src, void* workspace, int64_t list_capacity,
+                      const int* item_list, const int* item_count, cudaStream_t st) {
+    TileWs w = carve(workspace, B, T, num_tiles, list_capacity, nullptr);
+    DS_CUDA(cudaMemsetAsync(w.work + 1, 0, sizeof(int), st));
+    const void* k = reinterpret_cast<const void*>(&aux_kernel);
+    aux_kernel<<<block_grid(num_tiles, k, g_occ_aux), kWarpsPerCta * 32, 0, st>>>(
+        B, views, num_tiles, T, w.boxes, w.verts, w.offsets, w.sorted, w.list, list_capacity, level, S, alpha_src, C,
+        color, target, rast, scale, item_list, item_count, w.work + 1, grad_alpha_src);
+    return check_launch("tiles_opacity_aux");
+}
+
+TileTables tiles_tables(void* workspace, int B, int T, int num_tiles, int64_t list_capacity) {
+    const TileWs w = carve(workspace, B, T, num_tiles, list_capacity, nullptr);
+    return TileTables{w.boxes, w.verts, w.ndc};
+}
+
+int tiles_aux_impl(int B, const ds_view_desc* views, int num_tiles, int T, int level, int S, const float* alpha_src,
+                   const float* l1, const float* rast, float scale, float* grad_alpha_src, void* workspace,
+                   int64_t list_capacity, const RecordStore* rs, cudaStream_t st) {
+    if (num_tiles == 0) return DS_OK;
+    if (rs == nullptr)
+        return aux_launch(B, views, num_tiles, T, level, S, alpha_src, 1, l1, nullptr, rast, scale, grad_alpha_src,
+                          workspace, list_capacity, nullptr, nullptr, st);
+    aux_records_kernel<<<kSMs * 8, kRecChunk, 0, st>>>(*rs, level, S, alpha_src, l1, scale, grad_alpha_src);
+    const int rc = check_launch("tiles_opacity_aux records");
+    if (rc) return rc;
+    return aux_launch(B, views, num_tiles, T, level, S, alpha_src, 1, l1, nullptr, rast, scale, grad_alpha_src,
+                      workspace, list_capacity, rs->fallback, rs->counters + 1, st);
+}
+
+}  // namespace dsb
+
+extern "C" {
 
 int ds_tiles_rasterize(int B, const ds_view_desc* views, int num_tiles, int V, const float* pos, int T,
                        const int* tri, int level, int S, const float* alpha_src, int thr_mode, float thr_const,
@@ -533,14 +752,8 @@ int ds_tiles_rasterize(int B, const ds_view_desc* views, int num_tiles, int V, c
     DS_CHECK_ARG(level >= 0 && level <= 12 && (uint32_t)S == feats_at_level(level), "Invalid feature size.");
     DS_CHECK_ARG(thr_mode == 0 || (thr_mode == 1 && rng != nullptr), "tiles_rasterize: bad threshold mode");
     DS_CHECK_ARG(((uintptr_t)rast & 15) == 0, "tiles_rasterize: rast not 16-byte aligned");
-    if (num_tiles == 0) return DS_OK;
-    cudaStream_t st = (cudaStream_t)stream;
-    TileWs w = carve(workspace, B, T, num_tiles, list_capacity, nullptr);
-    DS_CUDA(cudaMemsetAsync(w.work, 0, sizeof(int), st));
-    raster_kernel<<<block_grid(num_tiles), kWarpsPerCta * 32, 0, st>>>(
-        B, views, num_tiles, T, w.boxes, w.verts, w.offsets, w.sorted, w.list, list_capacity, level, S, alpha_src,
-        thr_mode, thr_const, rng, w.work, rast);
-    return check_launch("tiles_rasterize");
+    return tiles_rasterize_impl(B, views, num_tiles, T, level, S, alpha_src, thr_mode, thr_const, rng, rast,
+                                workspace, list_capacity, nullptr, (cudaStream_t)stream);
 }
 
 int ds_tiles_opacity_aux(int B, const ds_view_desc* views, int num_tiles, int V, const float* pos, int T,
@@ -555,13 +768,8 @@ int ds_tiles_opacity_aux(int B, const ds_view_desc* views, int num_tiles, int V,
     DS_CHECK_ARG(target != nullptr || C == 1, "tiles_opacity_aux: without a target, color holds one value per pixel");
     DS_CHECK_ARG(((uintptr_t)rast & 15) == 0, "tiles_opacity_aux: rast not 16-byte aligned");
     if (num_tiles == 0) return DS_OK;
-    cudaStream_t st = (cudaStream_t)stream;
-    TileWs w = carve(workspace, B, T, num_tiles, list_capacity, nullptr);
-    DS_CUDA(cudaMemsetAsync(w.work + 1, 0, sizeof(int), st));
-    aux_kernel<<<block_grid(num_tiles), kWarpsPerCta * 32, 0, st>>>(
-        B, views, num_tiles, T, w.boxes, w.verts, w.offsets, w.sorted, w.list, list_capacity, level, S, alpha_src, C,
-        color, target, rast, scale, w.work + 1, grad_alpha_src);
-    return check_launch("tiles_opacity_aux");
+    return aux_launch(B, views, num_tiles, T, level, S, alpha_src, C, color, target, rast, scale, grad_alpha_src,
+                      workspace, list_capacity, nullptr, nullptr, (cudaStream_t)stream);
 }
 
 }  // extern "C"

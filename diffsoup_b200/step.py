@@ -34,7 +34,7 @@ from . import tiles as _tiles
 class StepConfig(C.Structure):
     _fields_ = [("B", C.c_int32), ("T", C.c_int32), ("V", C.c_int32), ("C", C.c_int32), ("min_level", C.c_int32),
                 ("max_level", C.c_int32), ("hidden", C.c_int32), ("n_layers", C.c_int32),
-                ("stochastic", C.c_int32), ("thr_const", C.c_float)]
+                ("stochastic", C.c_int32), ("thr_const", C.c_float), ("frag_records", C.c_float)]
 
 
 _L = _core.lib
@@ -54,7 +54,7 @@ _L.ds_train_step_set_events.restype = C.c_int
 _L.ds_train_step_set_events.argtypes = [C.c_void_p, C.c_int]
 
 LAYOUT = ["pos", "alpha_acc", "feat_acc", "feat_bf16", "rast", "color", "grad_color", "l1", "grad_pos",
-          "grad_alpha_acc", "grad_feat_acc"]
+          "grad_alpha_acc", "grad_feat_acc", "records", "chunk_fill", "record_counters", "fallback_blocks"]
 
 
 def mlp_param_count(C_: int, hidden: int, n_layers: int) -> int:
@@ -83,11 +83,15 @@ class TrainStep:
 
     def __init__(self, T: int, V: int, hw: Sequence[Tuple[int, int]], C_: int, min_level: int, max_level: int,
                  hidden: int, n_layers: int, stochastic: bool = True, seed: int = 0,
-                 device: Optional[torch.device] = None, list_capacity: Optional[int] = None):
+                 device: Optional[torch.device] = None, list_capacity: Optional[int] = None,
+                 frag_records: float = 2.0):
         self.device = torch.device(device or "cuda")
         self.hw = [(int(h), int(w)) for h, w in hw]
         self.B = len(self.hw)
-        self.cfg = StepConfig(self.B, T, V, C_, min_level, max_level, hidden, n_layers, int(stochastic), 0.5)
+        # frag_records: fragment records per pixel kept by the rasterizer for the
+        # opacity auxiliary gradient (0: that pass re-enumerates the tiles)
+        self.cfg = StepConfig(self.B, T, V, C_, min_level, max_level, hidden, n_layers, int(stochastic), 0.5,
+                              float(frag_records))
         self.views, self.num_tiles, self.num_pixels, self.pix_offsets = _tiles.view_table(self.hw, self.device)
         self.S = sum(_core.feats_at_level(l) for l in range(min_level, max_level + 1))
         self.nparam = mlp_param_count(C_, hidden, n_layers)
@@ -105,9 +109,10 @@ class TrainStep:
     def _alloc(self) -> None:
         nb = int(_L.ds_train_step_workspace_size(C.byref(self.cfg), self.num_tiles, self.num_pixels, self.capacity))
         self.workspace = torch.empty(nb, dtype=torch.uint8, device=self.device)
-        offs = (C.c_int64 * 11)()
+        offs = (C.c_int64 * 16)()
         _core.check(_L.ds_train_step_layout(C.byref(self.cfg), self.num_tiles, self.num_pixels, self.capacity, offs))
         self.offsets = {k: int(offs[i]) for i, k in enumerate(LAYOUT)}
+        self.record_capacity = int(offs[15])
 
     def intermediate(self, name: str) -> torch.Tensor:
         """A view of one workspace intermediate (valid after a step)."""
@@ -120,6 +125,9 @@ class TrainStep:
             "grad_color": (torch.float32, (self.num_pixels, 3)), "l1": (torch.float32, (self.num_pixels,)),
             "grad_pos": (torch.float64, (c.B, c.V, 4)), "grad_alpha_acc": (torch.float32, (c.T, ST)),
             "grad_feat_acc": (torch.float32, (c.T, ST, c.C)),
+            "records": (torch.int32, (self.record_capacity, 4)),
+            "chunk_fill": (torch.int32, (self.record_capacity // 256,)),
+            "record_counters": (torch.int32, (2,)), "fallback_blocks": (torch.int32, (self.num_tiles * 8 if self.record_capacity else 0,)),
         }
         dt, shp = shapes[name]
         n = 1
@@ -146,6 +154,12 @@ class TrainStep:
         """True when a tile list outgrew its capacity (results stay exact; the
         affected tiles ran the exhaustive path).  Synchronises on the status."""
         return bool(int(self.status.item()) & _tiles.DS_STATUS_LIST_OVERFLOW)
+
+    def record_fallback(self) -> bool:
+        """True when some blocks' fragment records did not fit and the opacity
+        auxiliary gradient re-enumerated them (results are the same).
+        Synchronises on the status."""
+        return bool(int(self.status.item()) & _tiles.DS_STATUS_RECORD_FALLBACK)
 
     def fit_capacity(self, *args, **kwargs) -> None:
         """Run eager steps, doubling the tile-list capacity until it fits."""

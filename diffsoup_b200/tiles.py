@@ -23,6 +23,7 @@ from . import _core
 
 DS_TILE = 16
 DS_STATUS_LIST_OVERFLOW = 1
+DS_STATUS_RECORD_FALLBACK = 2
 
 _capacity: Dict[int, int] = {}
 _pending_status: Dict[int, Tuple[torch.Tensor, torch.cuda.Event, int]] = {}

@@ -41,6 +41,7 @@ enum {
 /* Bits of the device status word written by the tiled kernels. */
 enum {
     DS_STATUS_LIST_OVERFLOW = 1, /* tile lists exceeded capacity; affected tiles ran the exhaustive path */
+    DS_STATUS_RECORD_FALLBACK = 2, /* some blocks' fragment records did not fit; they were re-enumerated */
 };
 
 const char* ds_last_error(void);
@@ -225,6 +226,13 @@ typedef struct {
     int32_t hidden, n_layers;/* shading MLP: (C+3) -> hidden x n_layers -> 3 */
     int32_t stochastic;      /* 1: Philox threshold per (view, pixel, triangle); 0: thr_const */
     float thr_const;
+    /* Fragment records per pixel reserved in the workspace (plus one chunk
+     * of 256 per rasterizer warp).  The rasterizer keeps every fragment in
+     * front of each pixel's surface there, and the opacity auxiliary gradient
+     * reads them back; blocks that do not fit are re-enumerated (same
+     * result, status bit DS_STATUS_RECORD_FALLBACK).  0 re-enumerates every
+     * block.  2 covers the benchmark scenes. */
+    float frag_records;
 } ds_step_config;
 
 /* Packed MLP parameter layout (fp32): W0[hidden][C+3] b0[hidden]
@@ -244,7 +252,12 @@ int ds_train_step_set_events(void* const* events, int n);
  * inspection after a step: [0] pos [B,V,4] f32, [1] opacity [T,S_max] f32,
  * [2] features [T,S_max,C] f32, [3] features bf16, [4] rast [pixels,4],
  * [5] colour [pixels,3], [6] dL/dcolour [pixels,3], [7] |c - target| summed
- * [pixels], [8] dL/dpos [B,V,4] f64, [9] dL/dopacity, [10] dL/dfeatures. */
+ * [pixels], [8] dL/dpos [B,V,4] f64, [9] dL/dopacity, [10] dL/dfeatures,
+ * [11] fragment records int32 [capacity,4] {pixel, triangle | visible << 31,
+ * b0 bits, b1 bits}, [12] record count of each 256-record chunk int32,
+ * [13] int32 {records reserved, blocks re-enumerated}, [14] ids of the
+ * re-enumerated 8x4 blocks (tile * 8 + block) int32; [15] holds the record
+ * capacity itself.  offsets has room for 16 entries. */
 int ds_train_step_layout(const ds_step_config* cfg, int num_tiles, int64_t num_pixels, int64_t list_capacity,
                          int64_t* offsets);
 

@@ -190,6 +190,46 @@ def test_tiled_rasterizer_uneven_views_and_overflow():
             assert (bits(got) == bits(ref)).all(), (cap_override, b)
 
 
+def test_tiled_rasterizer_adversarial_edges():
+    """Edges through pixel centres, shared edges, slivers, vertices at pixel
+    centres with varied w and huge triangles: the block-level rejection and
+    the per-pixel test must keep every fragment the reference keeps."""
+    H, W = 64, 96
+    rng = np.random.default_rng(17)
+    cx = lambda i: -1.0 + (2.0 * i + 1.0) / W  # noqa: E731
+    cy = lambda j: -1.0 + (2.0 * j + 1.0) / H  # noqa: E731
+    tris = []
+    for _ in range(300):  # vertices on pixel centres, random depth and w
+        ij = rng.integers(0, [W, H], size=(3, 2))
+        w = rng.uniform(0.3, 3.0, size=3)
+        z = rng.uniform(-0.9, 0.9, size=3)
+        tris.append([[cx(i) * wk, cy(j) * wk, zk * wk, wk] for (i, j), wk, zk in zip(ij, w, z)])
+    for _ in range(100):  # slivers along a line through pixel centres
+        i0, j0 = rng.integers(0, [W, H])
+        di, dj = rng.integers(-20, 21, size=2)
+        e = rng.uniform(-1e-6, 1e-6)
+        tris.append([[cx(i0), cy(j0), 0.1, 1.0], [cx(i0 + di), cy(j0 + dj), 0.2, 1.0],
+                     [cx(i0 + di) + e, cy(j0 + dj) - e, 0.3, 1.0]])
+    for _ in range(50):  # pairs sharing an edge through pixel centres
+        a, b, c, d = (rng.integers(0, [W, H], size=2) for _ in range(4))
+        z = float(rng.uniform(-0.5, 0.5))
+        pa, pb = [cx(a[0]), cy(a[1]), z, 1.0], [cx(b[0]), cy(b[1]), z, 1.0]
+        tris.append([pa, pb, [cx(c[0]), cy(c[1]), z, 1.0]])
+        tris.append([pb, pa, [cx(d[0]), cy(d[1]), z, 1.0]])
+    for _ in range(20):  # huge triangles, far vertices
+        v = rng.uniform(-50.0, 50.0, size=(3, 2))
+        w = rng.uniform(0.05, 2.0, size=3)
+        tris.append([[v[k, 0], v[k, 1], rng.uniform(-0.5, 0.5) * w[k], w[k]] for k in range(3)])
+    pos = np.asarray(tris, np.float32).reshape(1, -1, 4)
+    T = pos.shape[1] // 3
+    tri = np.arange(3 * T, dtype=np.int32).reshape(T, 3)
+    alpha = np.ones((T, 3), np.float32)
+    rast = ds.rasterize_multires_triangle_alpha((H, W), T_(pos), T_(tri), 0, T_(alpha[..., None]), stochastic=False)
+    ref, nf = cpu.rasterize_alpha(H, W, pos, tri, 0, alpha, stochastic=False)
+    assert nf > 0
+    assert (bits(rast) == bits(ref)).all()
+
+
 def test_tiled_empty_and_culled():
     H, W = 40, 56
     tri = torch.zeros((0, 3), dtype=torch.int32, device=DEV)
