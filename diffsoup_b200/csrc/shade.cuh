@@ -112,8 +112,12 @@ __device__ __forceinline__ float2 relu_gate(const __nv_bfloat16* h, float2 v) {
     return make_float2(__low2float(hv) > 0.f ? v.x : 0.f, __high2float(hv) > 0.f ? v.y : 0.f);
 }
 
+#ifndef DSB_SHADE_MIN_CTAS
+#define DSB_SHADE_MIN_CTAS 5  // resident CTAs per SM the small-MLP register budget is sized for
+#endif
+
 template <class K>
-__global__ void __launch_bounds__(K::WARPS * 32, K::REG_GRADS ? 5 : 1) shade_step_kernel(ShadeArgs a) {
+__global__ void __launch_bounds__(K::WARPS * 32, K::REG_GRADS ? DSB_SHADE_MIN_CTAS : 1) shade_step_kernel(ShadeArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ShadeSmem<K>& sm = *reinterpret_cast<ShadeSmem<K>*>(smem_raw);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;

@@ -96,6 +96,167 @@ __global__ void __launch_bounds__(kPrepWarps * 32) accum_sigmoid_backward_kernel
     for (int i = lane; i < n; i += 32) grad_src[(size_t)t * n + i] = s_acc[warp][i];
 }
 
+// ---------------------------------------------------------------------------
+// Table-driven level accumulation.  The interpolation from the levels'
+// lattices to the target lattice is the same sparse map for every triangle,
+// so each CTA builds it once in shared memory: the forward table lists, per
+// target sample, its (source sample, weight) pairs in level-then-corner
+// order (the summation order of accum_sigmoid_kernel, so results are
+// identical), and the backward table is the same map grouped by source
+// sample (CSR), which turns the adjoint into a gather without atomics.
+// Opacity (one channel) and features (C channels) go through one launch.
+// ---------------------------------------------------------------------------
+constexpr int kTabMax = 1024;   // (target sample, level, corner) entries
+constexpr int kTabRows = 256;   // source samples
+constexpr int kTabWarps = 4;
+
+struct LatticeTab {
+    int fidx[kTabMax];
+    float fw[kTabMax];
+    int row[kTabRows + 1];
+    short ck[kTabMax];
+    float cw[kTabMax];
+};
+
+__device__ void build_lattice_tab(LatticeTab& L, int lo, int hi, int ST, int S) {
+    const int NL = hi - lo + 1, NE = NL * 3, N = ST * NE;
+    const float inv_r = 1.f / (float)(1u << hi);  // a power of two: x * inv_r == x / 2^hi exactly
+    for (int u = threadIdx.x; u < ST * NL; u += blockDim.x) {
+        const int k = u / NL, li = u - (u / NL) * NL, l = lo + li;
+        uint32_t x, y;
+        index_to_xy((uint32_t)k, x, y);
+        uint32_t idx[3];
+        float w[3];
+        lattice_cell(__fmul_rn((float)x, inv_r), __fmul_rn((float)y, inv_r), (uint32_t)l, idx, w);
+        uint32_t off = 0;
+        for (int m = lo; m < l; ++m) off += feats_at_level((uint32_t)m);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            L.fidx[k * NE + li * 3 + j] = (int)(off + idx[j]);
+            L.fw[k * NE + li * 3 + j] = w[j];
+        }
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int d = warp; d < S; d += nw) {  // row lengths
+        int cnt = 0;
+        for (int e0 = 0; e0 < N; e0 += 32) cnt += __popc(__ballot_sync(0xffffffffu, e0 + lane < N && L.fidx[e0 + lane] == d));
+        if (lane == 0) L.row[d + 1] = cnt;
+    }
+    __syncthreads();
+    if (warp == 0) {  // exclusive prefix over the rows
+        int carry = 0;
+        if (lane == 0) L.row[0] = 0;
+        for (int d0 = 0; d0 < S; d0 += 32) {
+            const int d = d0 + lane;
+            int v = d < S ? L.row[d + 1] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int n = __shfl_up_sync(0xffffffffu, v, o);
+                if (lane >= o) v += n;
+            }
+            if (d < S) L.row[d + 1] = carry + v;
+            carry += __shfl_sync(0xffffffffu, v, 31);
+        }
+    }
+    __syncthreads();
+    for (int d = warp; d < S; d += nw) {  // entries of each row in (target, level, corner) order
+        int at = L.row[d];
+        for (int e0 = 0; e0 < N; e0 += 32) {
+            const int e = e0 + lane;
+            const bool hit = e < N && L.fidx[e] == d;
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
+            if (hit) {
+                const int pos = at + __popc(m & ((1u << lane) - 1u));
+                L.ck[pos] = (short)(e / NE);
+                L.cw[pos] = L.fw[e];
+            }
+            at += __popc(m);
+        }
+    }
+    __syncthreads();
+}
+
+// alpha_out[t] = sigmoid(accumulate(alpha_src[t])), feat_out[t] likewise
+// per channel (+ a bf16 copy); warp per triangle.
+template <int C>
+__global__ void __launch_bounds__(kTabWarps * 32) accum_tab_kernel(int T, int lo, int hi, int S, int ST,
+                                                                   const float* __restrict__ alpha_src,
+                                                                   const float* __restrict__ feat_src,
+                                                                   float* __restrict__ alpha_out,
+                                                                   float* __restrict__ feat_out,
+                                                                   __nv_bfloat16* __restrict__ feat_bf16) {
+    __shared__ LatticeTab L;
+    __shared__ float s_src[kTabWarps][kMaxSrc];
+    build_lattice_tab(L, lo, hi, ST, S);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int NE = (hi - lo + 1) * 3;
+    float* sa = s_src[warp];
+    float* sf = sa + S;
+    for (int t = blockIdx.x * kTabWarps + warp; t < T; t += gridDim.x * kTabWarps) {
+        for (int i = lane; i < S; i += 32) sa[i] = alpha_src[(size_t)t * S + i];
+        for (int i = lane; i < S * C; i += 32) sf[i] = feat_src[(size_t)t * S * C + i];
+        __syncwarp();
+        for (int k = lane; k < ST; k += 32) {
+            float acc = 0.f;
+            for (int n = 0; n < NE; ++n) acc = madd(acc, L.fw[k * NE + n], sa[L.fidx[k * NE + n]]);
+            alpha_out[(size_t)t * ST + k] = 1.f / (1.f + expf(-acc));
+        }
+        for (int e = lane; e < ST * C; e += 32) {
+            const int k = e / C, c = e % C;
+            float acc = 0.f;
+            for (int n = 0; n < NE; ++n) acc = madd(acc, L.fw[k * NE + n], sf[L.fidx[k * NE + n] * C + c]);
+            const float v = 1.f / (1.f + expf(-acc));
+            feat_out[(size_t)t * ST * C + e] = v;
+            feat_bf16[(size_t)t * ST * C + e] = __float2bfloat16_rn(v);
+        }
+        __syncwarp();
+    }
+}
+
+// Adjoint of accum_tab_kernel: grad_src[t][d] = sum over the targets k that
+// read d of w * grad_out[t][k] * s (1 - s); a gather, written once.
+template <int C>
+__global__ void __launch_bounds__(kTabWarps * 32) accum_tab_backward_kernel(
+    int T, int lo, int hi, int S, int ST, const float* __restrict__ alpha_sig, const float* __restrict__ alpha_grad,
+    const float* __restrict__ feat_sig, const float* __restrict__ feat_grad, float* __restrict__ alpha_src_grad,
+    float* __restrict__ feat_src_grad) {
+    __shared__ LatticeTab L;
+    __shared__ float s_gz[kTabWarps][kMaxSrc];
+    build_lattice_tab(L, lo, hi, ST, S);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float* ga = s_gz[warp];
+    float* gf = ga + ST;
+    for (int t = blockIdx.x * kTabWarps + warp; t < T; t += gridDim.x * kTabWarps) {
+        for (int i = lane; i < ST; i += 32) {
+            const float s = alpha_sig[(size_t)t * ST + i];
+            ga[i] = alpha_grad[(size_t)t * ST + i] * s * (1.f - s);
+        }
+        for (int i = lane; i < ST * C; i += 32) {
+            const float s = feat_sig[(size_t)t * ST * C + i];
+            gf[i] = feat_grad[(size_t)t * ST * C + i] * s * (1.f - s);
+        }
+        __syncwarp();
+        for (int d = lane; d < S; d += 32) {
+            float v = 0.f;
+            for (int n = L.row[d]; n < L.row[d + 1]; ++n) v = fmaf(L.cw[n], ga[L.ck[n]], v);
+            alpha_src_grad[(size_t)t * S + d] = v;
+        }
+        for (int o = lane; o < S * C; o += 32) {
+            const int d = o / C, c = o % C;
+            float v = 0.f;
+            for (int n = L.row[d]; n < L.row[d + 1]; ++n) v = fmaf(L.cw[n], gf[L.ck[n] * C + c], v);
+            feat_src_grad[(size_t)t * S * C + o] = v;
+        }
+        __syncwarp();
+    }
+}
+
+// Whether the table kernels cover this configuration.
+static bool lattice_tab_fits(int lo, int hi, int S, int ST, int C) {
+    return ST * (hi - lo + 1) * 3 <= kTabMax && S <= kTabRows && S * (C + 1) <= kMaxSrc && ST * (C + 1) <= kMaxSrc;
+}
+
 // clip[b][v] = mvp[b] . (verts[v], 1)  (examples/utils.py:412-426)
 __global__ void __launch_bounds__(kThreads) project_kernel(int B, int V, const float* __restrict__ verts,
                                                            const float* __restrict__ mvp, float* __restrict__ pos) {
@@ -140,8 +301,11 @@ __global__ void __launch_bounds__(kThreads) project_backward_kernel(int B, int V
 // warp reduction sums runs of equal (view, triangle) before one FP64 atomic
 // per vertex component.
 constexpr int kEdgeThreads = 128;
+#ifndef DSB_EDGE_MIN_CTAS
+#define DSB_EDGE_MIN_CTAS 6  // resident 4-warp CTAs per SM the register budget is sized for
+#endif
 
-__global__ void __launch_bounds__(kEdgeThreads) edge_step_kernel(int B, const ds_view_desc* __restrict__ views,
+__global__ void __launch_bounds__(kEdgeThreads, DSB_EDGE_MIN_CTAS) edge_step_kernel(int B, const ds_view_desc* __restrict__ views,
                                                                  int64_t num_pixels, int V, int T,
                                                                  TileTables tab,
                                                                  const int* __restrict__ tri,
@@ -378,7 +542,17 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
 
     // prep: opacity and feature accumulation + sigmoid, projection
     const unsigned tb = (unsigned)((c.T + kPrepWarps - 1) / kPrepWarps);
-    if (c.T > 0) {
+    const bool tab = lattice_tab_fits(c.min_level, c.max_level, S, ST, c.C);
+    const int64_t tw = ((int64_t)c.T + kTabWarps - 1) / kTabWarps;
+    const unsigned tgrid = (unsigned)(tw < kSMs * 4 ? tw : kSMs * 4);  // persistent: tables built once per CTA
+    if (c.T > 0 && tab) {
+        if (k8)
+            accum_tab_kernel<8><<<tgrid, kTabWarps * 32, 0, st>>>(c.T, c.min_level, c.max_level, S, ST, alpha_src,
+                                                                  feat_src, w.alpha_acc, w.feat_acc, w.feat_bf16);
+        else
+            accum_tab_kernel<16><<<tgrid, kTabWarps * 32, 0, st>>>(c.T, c.min_level, c.max_level, S, ST, alpha_src,
+                                                                   feat_src, w.alpha_acc, w.feat_acc, w.feat_bf16);
+    } else if (c.T > 0) {
         accum_sigmoid_kernel<false><<<tb, kPrepWarps * 32, 0, st>>>(c.T, c.min_level, c.max_level, c.max_level, S, ST, 1,
                                                                    alpha_src, w.alpha_acc, nullptr);
         accum_sigmoid_kernel<true><<<tb, kPrepWarps * 32, 0, st>>>(c.T, c.min_level, c.max_level, c.max_level, S, ST,
@@ -419,7 +593,16 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
         w.grad_color, rast, w.grad_pos);
     if ((rc = mark(6, st))) return rc;
     // adjoints of sigmoid + level accumulation, and of the projection
-    if (c.T > 0) {
+    if (c.T > 0 && tab) {
+        if (k8)
+            accum_tab_backward_kernel<8><<<tgrid, kTabWarps * 32, 0, st>>>(
+                c.T, c.min_level, c.max_level, S, ST, w.alpha_acc, w.grad_alpha_acc, w.feat_acc, w.grad_feat_acc,
+                grad_alpha_src, grad_feat_src);
+        else
+            accum_tab_backward_kernel<16><<<tgrid, kTabWarps * 32, 0, st>>>(
+                c.T, c.min_level, c.max_level, S, ST, w.alpha_acc, w.grad_alpha_acc, w.feat_acc, w.grad_feat_acc,
+                grad_alpha_src, grad_feat_src);
+    } else if (c.T > 0) {
         accum_sigmoid_backward_kernel<<<tb, kPrepWarps * 32, 0, st>>>(c.T, c.min_level, c.max_level, c.max_level, S,
                                                                       ST, 1, w.alpha_acc, w.grad_alpha_acc,
                                                                       grad_alpha_src);

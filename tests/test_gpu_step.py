@@ -120,3 +120,32 @@ def test_train_step_graph_replay():
     step.run(**d)
     torch.cuda.synchronize()
     assert rel(step.grad_verts.cpu().numpy(), gv_graph.cpu().numpy()) < 1e-5
+
+
+@pytest.mark.parametrize("config,kw", [
+    (2, dict(num_tris=3000, num_views=2, resolution=(128, 128))),
+    (4, dict(num_tris=800, num_views=2, resolution=(80, 96))),
+])
+def test_level_accumulation_matches_oracle(config, kw):
+    """Opacity and feature accumulation + sigmoid (forward; the sums bit for
+    bit, so only CUDA's and the host's expf may differ) and its adjoint
+    (given the step's own gradients of the accumulated values) against the
+    oracle's accumulate_to_level."""
+    sc, hw, inp, step, d = _setup(config, 7, **kw)
+    step.run(**d)
+    torch.cuda.synchronize()
+    lo, hi = sc.min_level, sc.max_level
+    a = step.intermediate("alpha_acc").cpu().numpy()
+    f = step.intermediate("feat_acc").cpu().numpy()
+    want_a = cpu.accumulate_sigmoid_f32(lo, hi, hi, sc.alpha_src)[..., 0]
+    want_f = cpu.accumulate_sigmoid_f32(lo, hi, hi, sc.feat_src)
+    np.testing.assert_allclose(a, want_a, rtol=0, atol=3e-7)
+    np.testing.assert_allclose(f, want_f, rtol=0, atol=3e-7)
+    bf = step.intermediate("feat_bf16").float().cpu().numpy()
+    assert np.array_equal(bf, torch.from_numpy(f).bfloat16().float().numpy())
+    ga = step.intermediate("grad_alpha_acc").cpu().numpy().astype(np.float64)
+    gf = step.intermediate("grad_feat_acc").cpu().numpy().astype(np.float64)
+    want_ga = cpu.accumulate_backward(lo, hi, hi, sc.T, (ga * a * (1 - a))[..., None])[..., 0]
+    want_gf = cpu.accumulate_backward(lo, hi, hi, sc.T, gf * f * (1 - f))
+    assert rel(step.grad_alpha_src.cpu().numpy(), want_ga) < 1e-5
+    assert rel(step.grad_feat_src.cpu().numpy(), want_gf) < 1e-5
