@@ -108,17 +108,33 @@ __global__ void __launch_bounds__(kPrepWarps * 32) accum_sigmoid_backward_kernel
 // ---------------------------------------------------------------------------
 constexpr int kTabMax = 1024;   // (target sample, level, corner) entries
 constexpr int kTabRows = 256;   // source samples
-constexpr int kTabWarps = 4;
+constexpr int kTabWarps = 8;
 
+// The tables in dynamic shared memory (N entries, S rows), followed by one
+// staging buffer per warp.
 struct LatticeTab {
-    int fidx[kTabMax];
-    float fw[kTabMax];
-    int row[kTabRows + 1];
-    short ck[kTabMax];
-    float cw[kTabMax];
+    int* fidx;
+    float* fw;
+    int* row;
+    float* cw;
+    short* ck;
 };
 
-__device__ void build_lattice_tab(LatticeTab& L, int lo, int hi, int ST, int S) {
+__host__ __device__ inline size_t lattice_tab_bytes(int N, int S) {
+    return ((size_t)N * 12 + (size_t)(S + 1) * 4 + (size_t)N * 2 + 15) & ~(size_t)15;
+}
+
+__device__ inline LatticeTab lattice_tab_at(unsigned char* base, int N, int S) {
+    LatticeTab L;
+    L.fidx = reinterpret_cast<int*>(base);
+    L.fw = reinterpret_cast<float*>(base + (size_t)N * 4);
+    L.cw = reinterpret_cast<float*>(base + (size_t)N * 8);
+    L.row = reinterpret_cast<int*>(base + (size_t)N * 12);
+    L.ck = reinterpret_cast<short*>(base + (size_t)N * 12 + (size_t)(S + 1) * 4);
+    return L;
+}
+
+__device__ void build_lattice_tab(const LatticeTab& L, int lo, int hi, int ST, int S) {
     const int NL = hi - lo + 1, NE = NL * 3, N = ST * NE;
     const float inv_r = 1.f / (float)(1u << hi);  // a power of two: x * inv_r == x / 2^hi exactly
     for (int u = threadIdx.x; u < ST * NL; u += blockDim.x) {
@@ -186,12 +202,12 @@ __global__ void __launch_bounds__(kTabWarps * 32) accum_tab_kernel(int T, int lo
                                                                    float* __restrict__ alpha_out,
                                                                    float* __restrict__ feat_out,
                                                                    __nv_bfloat16* __restrict__ feat_bf16) {
-    __shared__ LatticeTab L;
-    __shared__ float s_src[kTabWarps][kMaxSrc];
+    extern __shared__ __align__(16) unsigned char tab_smem[];
+    const int NE = (hi - lo + 1) * 3;
+    const LatticeTab L = lattice_tab_at(tab_smem, ST * NE, S);
     build_lattice_tab(L, lo, hi, ST, S);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int NE = (hi - lo + 1) * 3;
-    float* sa = s_src[warp];
+    float* sa = reinterpret_cast<float*>(tab_smem + lattice_tab_bytes(ST * NE, S)) + (size_t)warp * S * (C + 1);
     float* sf = sa + S;
     for (int t = blockIdx.x * kTabWarps + warp; t < T; t += gridDim.x * kTabWarps) {
         for (int i = lane; i < S; i += 32) sa[i] = alpha_src[(size_t)t * S + i];
@@ -221,11 +237,12 @@ __global__ void __launch_bounds__(kTabWarps * 32) accum_tab_backward_kernel(
     int T, int lo, int hi, int S, int ST, const float* __restrict__ alpha_sig, const float* __restrict__ alpha_grad,
     const float* __restrict__ feat_sig, const float* __restrict__ feat_grad, float* __restrict__ alpha_src_grad,
     float* __restrict__ feat_src_grad) {
-    __shared__ LatticeTab L;
-    __shared__ float s_gz[kTabWarps][kMaxSrc];
+    extern __shared__ __align__(16) unsigned char tab_smem[];
+    const int NE = (hi - lo + 1) * 3;
+    const LatticeTab L = lattice_tab_at(tab_smem, ST * NE, S);
     build_lattice_tab(L, lo, hi, ST, S);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float* ga = s_gz[warp];
+    float* ga = reinterpret_cast<float*>(tab_smem + lattice_tab_bytes(ST * NE, S)) + (size_t)warp * ST * (C + 1);
     float* gf = ga + ST;
     for (int t = blockIdx.x * kTabWarps + warp; t < T; t += gridDim.x * kTabWarps) {
         for (int i = lane; i < ST; i += 32) {
@@ -252,9 +269,15 @@ __global__ void __launch_bounds__(kTabWarps * 32) accum_tab_backward_kernel(
     }
 }
 
+// Dynamic shared memory of the table kernels: tables + per-warp staging.
+static size_t lattice_tab_smem(int lo, int hi, int S, int ST, int C) {
+    const int N = ST * (hi - lo + 1) * 3;
+    return lattice_tab_bytes(N, S) + (size_t)kTabWarps * (size_t)(S > ST ? S : ST) * (C + 1) * 4;
+}
+
 // Whether the table kernels cover this configuration.
 static bool lattice_tab_fits(int lo, int hi, int S, int ST, int C) {
-    return ST * (hi - lo + 1) * 3 <= kTabMax && S <= kTabRows && S * (C + 1) <= kMaxSrc && ST * (C + 1) <= kMaxSrc;
+    return ST * (hi - lo + 1) * 3 <= kTabMax && S <= kTabRows && lattice_tab_smem(lo, hi, S, ST, C) <= 48 * 1024;
 }
 
 // clip[b][v] = mvp[b] . (verts[v], 1)  (examples/utils.py:412-426)
@@ -543,14 +566,15 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     // prep: opacity and feature accumulation + sigmoid, projection
     const unsigned tb = (unsigned)((c.T + kPrepWarps - 1) / kPrepWarps);
     const bool tab = lattice_tab_fits(c.min_level, c.max_level, S, ST, c.C);
+    const size_t tsm = lattice_tab_smem(c.min_level, c.max_level, S, ST, c.C);
     const int64_t tw = ((int64_t)c.T + kTabWarps - 1) / kTabWarps;
     const unsigned tgrid = (unsigned)(tw < kSMs * 4 ? tw : kSMs * 4);  // persistent: tables built once per CTA
     if (c.T > 0 && tab) {
         if (k8)
-            accum_tab_kernel<8><<<tgrid, kTabWarps * 32, 0, st>>>(c.T, c.min_level, c.max_level, S, ST, alpha_src,
+            accum_tab_kernel<8><<<tgrid, kTabWarps * 32, tsm, st>>>(c.T, c.min_level, c.max_level, S, ST, alpha_src,
                                                                   feat_src, w.alpha_acc, w.feat_acc, w.feat_bf16);
         else
-            accum_tab_kernel<16><<<tgrid, kTabWarps * 32, 0, st>>>(c.T, c.min_level, c.max_level, S, ST, alpha_src,
+            accum_tab_kernel<16><<<tgrid, kTabWarps * 32, tsm, st>>>(c.T, c.min_level, c.max_level, S, ST, alpha_src,
                                                                    feat_src, w.alpha_acc, w.feat_acc, w.feat_bf16);
     } else if (c.T > 0) {
         accum_sigmoid_kernel<false><<<tb, kPrepWarps * 32, 0, st>>>(c.T, c.min_level, c.max_level, c.max_level, S, ST, 1,
@@ -595,11 +619,11 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     // adjoints of sigmoid + level accumulation, and of the projection
     if (c.T > 0 && tab) {
         if (k8)
-            accum_tab_backward_kernel<8><<<tgrid, kTabWarps * 32, 0, st>>>(
+            accum_tab_backward_kernel<8><<<tgrid, kTabWarps * 32, tsm, st>>>(
                 c.T, c.min_level, c.max_level, S, ST, w.alpha_acc, w.grad_alpha_acc, w.feat_acc, w.grad_feat_acc,
                 grad_alpha_src, grad_feat_src);
         else
-            accum_tab_backward_kernel<16><<<tgrid, kTabWarps * 32, 0, st>>>(
+            accum_tab_backward_kernel<16><<<tgrid, kTabWarps * 32, tsm, st>>>(
                 c.T, c.min_level, c.max_level, S, ST, w.alpha_acc, w.grad_alpha_acc, w.feat_acc, w.grad_feat_acc,
                 grad_alpha_src, grad_feat_src);
     } else if (c.T > 0) {

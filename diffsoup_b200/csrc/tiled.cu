@@ -505,19 +505,59 @@ __device__ __forceinline__ void aux_scatter(float b0, float b1, int level, int S
 }
 
 // Opacity auxiliary gradient from the fragment records: one thread per
-// record, blocks stride over the chunks.
+// record, blocks stride over the chunks.  A chunk holds whole 8x4 blocks in
+// walk order, so neighbouring records often share a triangle and a lattice
+// cell: runs of equal (triangle, cell) in a warp are summed with a segmented
+// reduction before the global atomics.
 __global__ void __launch_bounds__(kRecChunk) aux_records_kernel(RecordStore rs, int level, int S,
                                                                const float* __restrict__ alpha_src,
                                                                const float* __restrict__ l1, float scale,
                                                                float* __restrict__ grad_alpha_src) {
+    const int lane = threadIdx.x & 31;
     const int64_t reserved = rs.counters[0];
     const int64_t nchunks = (reserved < rs.capacity ? reserved : rs.capacity) / kRecChunk;
     for (int64_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
-        if ((int)threadIdx.x >= rs.chunk_fill[c]) continue;
-        const int4 r = rs.rec[c * kRecChunk + threadIdx.x];
-        const uint32_t tv = (uint32_t)r.y;
-        aux_scatter(__int_as_float(r.z), __int_as_float(r.w), level, S, alpha_src, (int)(tv & 0x7fffffffu),
-                    l1[(uint32_t)r.x], (tv >> 31) != 0, scale, grad_alpha_src);
+        const bool valid = (int)threadIdx.x < rs.chunk_fill[c];
+        int t = -1 - lane;
+        uint32_t idx[3] = {0u, 0u, 0u};
+        float g[3] = {0.f, 0.f, 0.f};
+        if (valid) {
+            const int4 r = rs.rec[c * kRecChunk + threadIdx.x];
+            const uint32_t tv = (uint32_t)r.y;
+            t = (int)(tv & 0x7fffffffu);
+            const float b0 = __int_as_float(r.z), b1 = __int_as_float(r.w);
+            float w[3];
+            lattice_cell(b0, b1, (uint32_t)level, idx, w);
+            // interp_scalar at one level (the same sum)
+            const float* src = alpha_src + (size_t)t * S;
+            float alpha = 0.f;
+            alpha = madd(alpha, w[0], __ldg(src + idx[0]));
+            alpha = madd(alpha, w[1], __ldg(src + idx[1]));
+            alpha = madd(alpha, w[2], __ldg(src + idx[2]));
+            const float ga = aux_alpha_grad(l1[(uint32_t)r.x], alpha, (tv >> 31) != 0) * scale;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) g[q] = ga * w[q];
+        }
+        const int pt = __shfl_up_sync(0xffffffffu, t, 1);
+        const uint32_t p0 = __shfl_up_sync(0xffffffffu, idx[0], 1), p1 = __shfl_up_sync(0xffffffffu, idx[1], 1),
+                       p2 = __shfl_up_sync(0xffffffffu, idx[2], 1);
+        const bool same = lane > 0 && pt == t && p0 == idx[0] && p1 == idx[1] && p2 == idx[2];
+        const unsigned heads = __ballot_sync(0xffffffffu, !same);
+        const int seg = __popc(heads & ((2u << lane) - 1u));
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int oseg = __shfl_down_sync(0xffffffffu, seg, o);
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                const float v = __shfl_down_sync(0xffffffffu, g[q], o);
+                if (lane + o < 32 && oseg == seg) g[q] += v;
+            }
+        }
+        if (valid && !same) {
+            float* dst = grad_alpha_src + (size_t)t * S;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) atomicAdd(dst + idx[q], g[q]);
+        }
     }
 }
 
