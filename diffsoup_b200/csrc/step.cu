@@ -16,6 +16,7 @@
 
 #include "edge_math.cuh"
 #include "shade.cuh"
+#include "shade_small.cuh"
 #include "tiled.cuh"
 
 namespace dsb {
@@ -410,6 +411,21 @@ static int launch_shade(const ShadeArgs& a, cudaStream_t st) {
     return check_launch("shade_step");
 }
 
+// The register-resident kernel of the 8-16-3 MLP.
+static int launch_shade_small(const ShadeArgs& a, cudaStream_t st) {
+    static int per_sm = 0;  // set on the first (eager) call, before any graph capture
+    if (per_sm == 0) {
+        DS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, shade_small_kernel, kShadeSmallWarps * 32, 0));
+        if (per_sm <= 0) return set_error(DS_ERR_CUDA, "shade_small: kernel does not fit on an SM");
+    }
+    const int64_t chunks = (a.num_pixels + 31) / 32;
+    const int64_t want = (chunks + kShadeSmallWarps - 1) / kShadeSmallWarps;
+    const int64_t cap = (int64_t)kSMs * per_sm;
+    const unsigned grid = (unsigned)(want < 1 ? 1 : (want < cap ? want : cap));
+    shade_small_kernel<<<grid, kShadeSmallWarps * 32, 0, st>>>(a);
+    return check_launch("shade_small");
+}
+
 static inline size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
 
 // Optional phase events (profiling): recorded on the step's stream at the
@@ -603,7 +619,7 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     a.inv_n = (float)(1.0 / ((double)num_pixels * 3.0));
     a.color = color_out ? color_out : w.color; a.grad_color = w.grad_color; a.l1 = w.l1;
     a.grad_feat = w.grad_feat_acc; a.grad_params = grad_mlp_params; a.loss_sum = w.loss_sum;
-    rc = k8 ? launch_shade<ShadeC8H16>(a, st) : launch_shade<ShadeC16H64>(a, st);
+    rc = k8 ? launch_shade_small(a, st) : launch_shade<ShadeC16H64>(a, st);
     if (rc || (rc = mark(4, st))) return rc;
 
     // opacity auxiliary gradient (scaled by 1/numel(colour), rasterize.py:183-195)
