@@ -118,6 +118,66 @@ __device__ __forceinline__ void add_mid_contrib(float mx, float my, const float4
     a.any = true;
 }
 
+// The contribution of add_mid_contrib given the point's barycentrics and
+// interpolated clip z, w.
+__device__ __forceinline__ void add_contrib_at(float b0, float b1, float cz, float cw, float mx, float my, float gx,
+                                               float gy, float gz, bool use_z, EdgeAccum& a) {
+    const float b2 = 1.f - b0 - b1;
+    const float cx = mx * cw, cy = my * cw;
+    const float iw = 1.f / cw, iw2 = iw * iw;
+    const float gsum = use_z ? gx * cx + gy * cy + gz * cz : gx * cx + gy * cy;
+    const float bb[3] = {b0, b1, b2};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        a.g[k * 4 + 0] += bb[k] * gx * iw;
+        a.g[k * 4 + 1] += bb[k] * gy * iw;
+        if (use_z) a.g[k * 4 + 2] += bb[k] * gz * iw;
+        a.g[k * 4 + 3] += -bb[k] * gsum * iw2;
+    }
+    a.any = true;
+}
+
+// The pixel's triangle's edge functions, which are affine in the NDC point:
+// evaluated at the pixel centre as the coverage test does, then stepped to
+// the neighbours' centres and the pair midpoints (the batched step compares
+// with the oracle within a tolerance; points within rounding of an edge may
+// be classified differently from a direct evaluation).
+struct EdgeFrame {
+    float A[3];       // edge functions at the pixel centre
+    float ax[3], ay[3];  // their derivatives along NDC x and y
+    float z[3], w[3];
+};
+
+__device__ __forceinline__ void edge_frame(const float4 P[3], float nx, float ny, EdgeFrame& f) {
+    float As;
+    edge_terms(ny, nx, P[0], P[1], P[2], f.A[0], f.A[1], f.A[2], As);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float4 u = P[(k + 1) % 3], v = P[(k + 2) % 3];
+        f.ax[k] = u.y * v.w - u.w * v.y;
+        f.ay[k] = u.w * v.x - u.x * v.w;
+        f.z[k] = P[k].z;
+        f.w[k] = P[k].w;
+    }
+}
+
+// Coverage test and barycentrics at the centre offset by (dx, dy) in NDC.
+__device__ __forceinline__ bool edge_frame_cover(const EdgeFrame& f, float dx, float dy, float& b0, float& b1,
+                                                 float& z, float& w) {
+    const float A0 = fmaf(f.ay[0], dy, fmaf(f.ax[0], dx, f.A[0]));
+    const float A1 = fmaf(f.ay[1], dy, fmaf(f.ax[1], dx, f.A[1]));
+    const float A2 = fmaf(f.ay[2], dy, fmaf(f.ax[2], dx, f.A[2]));
+    const float A = A0 + A1 + A2;
+    if (!(A != 0.f)) return false;
+    const float inv = 1.f / A;
+    b0 = A0 * inv;
+    b1 = A1 * inv;
+    const float b2 = 1.f - b0 - b1;
+    z = b0 * f.z[0] + b1 * f.z[1] + b2 * f.z[2];
+    w = b0 * f.w[0] + b1 * f.w[1] + b2 * f.w[2];
+    return b0 >= 0.f && b1 >= 0.f && b0 + b1 <= 1.f;
+}
+
 // Edge-gradient estimator of one pixel (rasterize.cu:663-892).  Pixel
 // buffers are addressed as base + y*W + x with `base` the view's first pixel;
 // posb holds the view's clip positions.  Returns the pixel's triangle (or -1)
@@ -271,6 +331,8 @@ __device__ __forceinline__ int edge_grad_pixel_split(int y0, int x0, int H, int 
         const TriVerts v = tverts[it0];
         P0[0] = v.p0; P0[1] = v.p1; P0[2] = v.p2;
     }
+    EdgeFrame fr;
+    edge_frame(P0, nx0, ny0, fr);
     float c0[3], g0[3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) { c0[i] = color[pix0 * 3 + i]; g0[i] = grad_color[pix0 * 3 + i]; }
@@ -295,7 +357,9 @@ __device__ __forceinline__ int edge_grad_pixel_split(int y0, int x0, int H, int 
         const float gy = adj * (float)DY * (float)H / 2.f;
         const float nx1 = -1.f + ((float)x1 + 0.5f) * sx;
         const float ny1 = -1.f + ((float)y1 + 0.5f) * sy;
-        add_mid_contrib(0.5f * (nx0 + nx1), 0.5f * (ny0 + ny1), P0, 2.f * gx, 2.f * gy, 0.f, false, acc);
+        float b0, b1, cz, cw;
+        if (edge_frame_cover(fr, 0.5f * (float)DX * sx, 0.5f * (float)DY * sy, b0, b1, cz, cw))
+            add_contrib_at(b0, b1, cz, cw, 0.5f * (nx0 + nx1), 0.5f * (ny0 + ny1), 2.f * gx, 2.f * gy, 0.f, false, acc);
     }
 #pragma unroll 1
     for (int e = 0; e < 4; ++e) {
@@ -317,8 +381,9 @@ __device__ __forceinline__ int edge_grad_pixel_split(int y0, int x0, int H, int 
         const float nx1 = -1.f + ((float)x1 + 0.5f) * sx;
         const float ny1 = -1.f + ((float)y1 + 0.5f) * sy;
         const float mx = 0.5f * (nx0 + nx1), my = 0.5f * (ny0 + ny1);
+        const float hx = 0.5f * (float)DX * sx, hy = 0.5f * (float)DY * sy;  // centre -> midpoint
         float tb0, tb1, cz1, cw1;
-        if (intersect_triangle(ny1, nx1, P0[0], P0[1], P0[2], tb0, tb1, cz1, cw1)) {
+        if (edge_frame_cover(fr, 2.f * hx, 2.f * hy, tb0, tb1, cz1, cw1)) {
             const float d1_it0 = cz1 / cw1;
             // it1 hides it0 at the neighbour.  Only a triangle intersection
             // contributes, which needs it1 behind it0 at this pixel: never
@@ -346,12 +411,16 @@ __device__ __forceinline__ int edge_grad_pixel_split(int y0, int x0, int H, int 
                                 db_dp_2d(nv[1], nv[2], nf[1], nf[2], dby, dbz);
                                 gyn = gy * dby; gzn = gy * dbz;
                             }
-                            add_mid_contrib(mx, my, P0, gxn, gyn, gzn, true, acc);
+                            float mb0, mb1, mz, mw;
+                            if (edge_frame_cover(fr, hx, hy, mb0, mb1, mz, mw))
+                                add_contrib_at(mb0, mb1, mz, mw, mx, my, gxn, gyn, gzn, true, acc);
                         }
                     }
                 }
             } else if (it1 < 0 || depth0 < depth1) {  // active opacity edge
-                add_mid_contrib(mx, my, P0, gx, gy, 0.f, false, acc);
+                float mb0, mb1, mz, mw;
+                if (edge_frame_cover(fr, hx, hy, mb0, mb1, mz, mw))
+                    add_contrib_at(mb0, mb1, mz, mw, mx, my, gx, gy, 0.f, false, acc);
             }
         } else if (it1 < 0 || depth0 < depth1) {  // active geometric edge
             int i0, i1;

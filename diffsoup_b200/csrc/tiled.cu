@@ -116,21 +116,32 @@ __global__ void __launch_bounds__(kThreads) bin_setup_kernel(int B, const ds_vie
     if (!(r.zlo == r.zlo && r.zhi == r.zhi)) { r.zlo = -INFINITY; r.zhi = INFINITY; }  // NaN: no bounds
     boxes[i] = r;
     verts[i] = v;
+    // tiles the triangle may cover; for rects of at most 64 tiles their bit
+    // mask (row-major over the rect) rides in the NDC record's spare lanes
+    uint64_t m = 0;
+    int tx0, tx1, ty0, ty1;
+    if (box_tiles(r, tx0, tx1, ty0, ty1)) {
+        const int ntx = tx1 - tx0 + 1;
+        const bool small = (ty1 - ty0 + 1) * ntx <= 64;
+        for (int ty = ty0; ty <= ty1; ++ty)
+            for (int tx = tx0; tx <= tx1; ++tx)
+                if (tile_may_cover(v, vd, tx, ty)) {
+                    atomicAdd(counts + vd.tile_base + ty * vd.tiles_x + tx, 1);
+                    if (small) m |= 1ull << ((ty - ty0) * ntx + (tx - tx0));
+                }
+    }
     TriNdc q;
     q.a = make_float4(v.p0.x / v.p0.w, v.p0.y / v.p0.w, v.p1.x / v.p1.w, v.p1.y / v.p1.w);
-    q.b = make_float4(v.p2.x / v.p2.w, v.p2.y / v.p2.w, 0.f, 0.f);
+    q.b = make_float4(v.p2.x / v.p2.w, v.p2.y / v.p2.w, __uint_as_float((uint32_t)m),
+                      __uint_as_float((uint32_t)(m >> 32)));
     ndc[i] = q;
-    int tx0, tx1, ty0, ty1;
-    if (!box_tiles(r, tx0, tx1, ty0, ty1)) return;
-    for (int ty = ty0; ty <= ty1; ++ty)
-        for (int tx = tx0; tx <= tx1; ++tx)
-            if (tile_may_cover(v, vd, tx, ty)) atomicAdd(counts + vd.tile_base + ty * vd.tiles_x + tx, 1);
 }
 
 // Pass 2: scatter record indices into the per-tile lists.
 __global__ void __launch_bounds__(kThreads) bin_fill_kernel(int B, const ds_view_desc* __restrict__ views, int T,
                                                             const TriBox* __restrict__ boxes,
                                                             const TriVerts* __restrict__ verts,
+                                                            const TriNdc* __restrict__ ndc,
                                                             const int64_t* __restrict__ offsets,
                                                             int* __restrict__ cursor, int* __restrict__ list,
                                                             int64_t capacity, int* __restrict__ status) {
@@ -141,11 +152,16 @@ __global__ void __launch_bounds__(kThreads) bin_fill_kernel(int B, const ds_view
     const TriBox rc = boxes[i];
     int tx0, tx1, ty0, ty1;
     if (!box_tiles(rc, tx0, tx1, ty0, ty1)) return;
-    const TriVerts v = verts[i];
+    const int ntx = tx1 - tx0 + 1;
+    const bool small = (ty1 - ty0 + 1) * ntx <= 64;
+    const float4 nb = ndc[i].b;
+    const uint64_t m = (uint64_t)__float_as_uint(nb.z) | ((uint64_t)__float_as_uint(nb.w) << 32);
     bool over = false;
     for (int ty = ty0; ty <= ty1; ++ty)
         for (int tx = tx0; tx <= tx1; ++tx) {
-            if (!tile_may_cover(v, vd, tx, ty)) continue;  // the same test as the count pass
+            // the count pass's decision: its bit, or the test itself for large rects
+            if (small ? !((m >> ((ty - ty0) * ntx + (tx - tx0))) & 1u) : !tile_may_cover(verts[i], vd, tx, ty))
+                continue;
             const int tile = vd.tile_base + ty * vd.tiles_x + tx;
             const int64_t at = offsets[tile] + atomicAdd(cursor + tile, 1);
             if (at < capacity) list[at] = (int)i; else over = true;
@@ -175,7 +191,30 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) sort_lists_kernel(int num_t
         if (lane == 0) sorted[tile] = 1;
         return;
     }
-    int size = 32;
+    if (n <= 32) {  // one entry per lane: bitonic network in registers
+        int ri = -1;
+        float key = INFINITY;
+        if (lane < n) {
+            ri = list[begin + lane];
+            key = fminf(boxes[ri].zlo, 3.0e38f);  // real keys stay below the +inf padding
+        }
+#pragma unroll
+        for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                const float ok = __shfl_xor_sync(0xffffffffu, key, j);
+                const int ov = __shfl_xor_sync(0xffffffffu, ri, j);
+                // the lower lane of the pair keeps the smaller key in ascending runs
+                const bool up = (lane & k) == 0, lower = (lane & j) == 0;
+                const bool take = (lower == up) ? (ok < key) : (ok > key);
+                if (take) { key = ok; ri = ov; }
+            }
+        }
+        if (lane < n) list[begin + lane] = ri;
+        if (lane == 0) sorted[tile] = 1;
+        return;
+    }
+    int size = 64;
     while (size < n) size <<= 1;
     float* key = s_key[warp];
     int* val = s_val[warp];
@@ -697,7 +736,8 @@ int ds_tiles_bin(int B, const ds_view_desc* views, int num_tiles, int V, const f
     // offsets[num_tiles] = total number of entries
     DS_CUDA(cudaMemcpyAsync(w.offsets + num_tiles, total_dev, sizeof(int64_t), cudaMemcpyDeviceToDevice, st));
     if (n > 0)
-        bin_fill_kernel<<<blocks_for(n), kThreads, 0, st>>>(B, views, T, w.boxes, w.verts, w.offsets, w.cursor, w.list,
+        bin_fill_kernel<<<blocks_for(n), kThreads, 0, st>>>(B, views, T, w.boxes, w.verts, w.ndc, w.offsets, w.cursor,
+                                                            w.list,
                                                             list_capacity, status);
     if (num_tiles > 0)
         sort_lists_kernel<<<(unsigned)((num_tiles + kWarpsPerCta - 1) / kWarpsPerCta), kWarpsPerCta * 32, 0, st>>>(

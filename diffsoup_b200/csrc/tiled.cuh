@@ -19,7 +19,8 @@ struct __align__(16) TriBox {
 static_assert(sizeof(TriBox) == 16, "TriBox layout");
 
 // Per (view, triangle): the clip-space vertices, and their NDC x, y
-// (x_k / w_k, y_k / w_k: a = (x0, y0, x1, y1), b = (x2, y2, 0, 0)).
+// (x_k / w_k, y_k / w_k: a = (x0, y0, x1, y1), b = (x2, y2, m_lo, m_hi) with
+// m the binning pass's 64-bit mask of the tiles the triangle may cover).
 struct __align__(16) TriVerts {
     float4 p0, p1, p2;
 };
