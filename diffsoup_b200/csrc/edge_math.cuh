@@ -295,11 +295,60 @@ __device__ __forceinline__ int edge_grad_pixel(int b, int y0, int x0, int H, int
 }
 
 // The estimator of edge_grad_pixel for a colour of 3 channels, reorganised
-// for SIMT execution: each interior pair (both pixels on the same triangle)
-// is evaluated once, from its left/bottom pixel, and counted twice (the
-// adjoint and the pixel offset both change sign, so the two evaluations the
-// reference makes are equal); all interior pairs of a pixel run first as
-// uniform work, then the rarer silhouette / intersection pairs.
+// for SIMT execution.
+//
+// * Each interior pair (both pixels on the same triangle) is evaluated once,
+//   from its left/bottom pixel, and counted twice (the adjoint and the pixel
+//   offset both change sign, so the two evaluations the reference makes are
+//   equal).
+// * The triangle's edge functions A_k are affine in the NDC point (the
+//   w-products of the homogeneous cross product cancel), so they are
+//   evaluated once at the pixel centre with the reference's arithmetic and
+//   stepped to the neighbour centre and the pair midpoint.  The
+//   barycentrics are b_k = A_k / sum A, so coverage is a sign test, and with
+//   cw = sum b_k w_k a midpoint's weights b_k / cw are A_k / sum(A_k w_k):
+//   one reciprocal per point.
+// * A silhouette pair leaves the triangle through the edge whose function
+//   changes sign first along the segment between the two centres: the
+//   crossing parameter is A_k(p0) / (A_k(p0) - A_k(p1)), which replaces the
+//   reference's three segment-segment tests (rasterize.cu:546-604) and gives
+//   the same edge except within rounding of a vertex (ties go to the edge
+//   the reference tests first).  The perspective-correct position along
+//   that edge follows rasterize.cu:585-603.
+// * Every pair type ends in one accumulation: weights on the triangle's
+//   three vertices at the evaluation point and its clip coordinates
+//   (rasterize.cu:727-746 for midpoints, :868-891 for edge crossings).
+// Magnitudes use approximate reciprocals; comparisons that decide a pair's
+// case use correctly rounded divisions, as the reference does.
+
+// The triangle-intersection case (rasterize.cu:760-809): the neighbour's
+// triangle it1 hides it0 there and lies behind it0 at this pixel.  Returns
+// false when the pair contributes nothing; else the gradient direction.
+__device__ __forceinline__ bool intersection_pair(const float4 P0[3], const TriVerts* __restrict__ tverts,
+                                               const TriBox* __restrict__ tboxes, int it1, float depth0, float nx0,
+                                               float ny0, int DX, float gx, float gy, float& gxn, float& gyn,
+                                               float& gzn) {
+    if (tboxes[it1].zhi < depth0) return false;  // it1 lies in front of depth0 everywhere
+    const TriVerts v = tverts[it1];
+    float tb0, tb1, cz0, cw0;
+    if (!intersect_triangle(ny0, nx0, v.p0, v.p1, v.p2, tb0, tb1, cz0, cw0)) return false;
+    if (!(depth0 < cz0 / cw0)) return false;
+    const float4 P1[3] = {v.p0, v.p1, v.p2};
+    float nv[3], nf[3];
+    if (!(tri_normal_ndc(P0, nv) && tri_normal_ndc(P1, nf))) return false;
+    gxn = gyn = gzn = 0.f;
+    if (DX != 0) {
+        float dbx, dbz;
+        db_dp_2d(nv[0], nv[2], nf[0], nf[2], dbx, dbz);
+        gxn = gx * dbx; gzn = gx * dbz;
+    } else {
+        float dby, dbz;
+        db_dp_2d(nv[1], nv[2], nf[1], nf[2], dby, dbz);
+        gyn = gy * dby; gzn = gy * dbz;
+    }
+    return true;
+}
+
 __device__ __forceinline__ float pair_adjoint3(const float* c0, const float* g0, const float* c1, const float* g1) {
     float adj = 0.f;
 #pragma unroll
@@ -311,8 +360,8 @@ __device__ __forceinline__ int edge_grad_pixel_split(int y0, int x0, int H, int 
                                                      const float* __restrict__ grad_color,
                                                      const float* __restrict__ rast,
                                                      const TriVerts* __restrict__ tverts,
-                                                     const TriBox* __restrict__ tboxes,
-                                                     const TriNdc* __restrict__ tndc, int64_t base, EdgeAccum& acc) {
+                                                     const TriBox* __restrict__ tboxes, int64_t base,
+                                                     EdgeAccum& acc) {
 #pragma unroll
     for (int k = 0; k < 12; ++k) acc.g[k] = 0.f;
     acc.any = false;
@@ -331,46 +380,32 @@ __device__ __forceinline__ int edge_grad_pixel_split(int y0, int x0, int H, int 
         const TriVerts v = tverts[it0];
         P0[0] = v.p0; P0[1] = v.p1; P0[2] = v.p2;
     }
-    EdgeFrame fr;
-    edge_frame(P0, nx0, ny0, fr);
+    float A[3], ax[3], ay[3], As;
+    edge_terms(ny0, nx0, P0[0], P0[1], P0[2], A[0], A[1], A[2], As);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float4 u = P0[(k + 1) % 3], v = P0[(k + 2) % 3];
+        ax[k] = u.y * v.w - u.w * v.y;
+        ay[k] = u.w * v.x - u.x * v.w;
+    }
+    if (!(As != 0.f)) return it0;  // cannot happen for a covered pixel; nothing to add
+    const float sgn = As > 0.f ? 1.f : -1.f;  // orientation of the inside near the pixel
     float c0[3], g0[3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) { c0[i] = color[pix0 * 3 + i]; g0[i] = grad_color[pix0 * 3 + i]; }
     // neighbours (+x, -x, -y, +y) as in rasterize.cu:691-692
-    unsigned edge_mask = 0;
-#pragma unroll
+#pragma unroll 1
     for (int e = 0; e < 4; ++e) {
         const int DX = (e == 0) - (e == 1);
         const int DY = (e == 3) - (e == 2);
         const int y1 = y0 + DY, x1 = x0 + DX;
         if (y1 < 0 || y1 >= H || x1 < 0 || x1 >= W) continue;
         const int64_t pix1 = base + (int64_t)y1 * W + x1;
-        const int it1 = (int)reinterpret_cast<const float4*>(rast)[pix1].w - 1;
-        if (it1 != it0) { edge_mask |= 1u << e; continue; }
-        if (DX < 0 || DY < 0) continue;  // interior pair counted by the neighbour
-        float c1[3], g1[3];
-#pragma unroll
-        for (int i = 0; i < 3; ++i) { c1[i] = color[pix1 * 3 + i]; g1[i] = grad_color[pix1 * 3 + i]; }
-        const float adj = pair_adjoint3(c0, g0, c1, g1);
-        if (adj == 0.f) continue;
-        const float gx = adj * (float)DX * (float)W / 2.f;
-        const float gy = adj * (float)DY * (float)H / 2.f;
-        const float nx1 = -1.f + ((float)x1 + 0.5f) * sx;
-        const float ny1 = -1.f + ((float)y1 + 0.5f) * sy;
-        float b0, b1, cz, cw;
-        if (edge_frame_cover(fr, 0.5f * (float)DX * sx, 0.5f * (float)DY * sy, b0, b1, cz, cw))
-            add_contrib_at(b0, b1, cz, cw, 0.5f * (nx0 + nx1), 0.5f * (ny0 + ny1), 2.f * gx, 2.f * gy, 0.f, false, acc);
-    }
-#pragma unroll 1
-    for (int e = 0; e < 4; ++e) {
-        if (!((edge_mask >> e) & 1u)) continue;
-        const int DX = (e == 0) - (e == 1);
-        const int DY = (e == 3) - (e == 2);
-        const int y1 = y0 + DY, x1 = x0 + DX;
-        const int64_t pix1 = base + (int64_t)y1 * W + x1;
         const float4 r1 = reinterpret_cast<const float4*>(rast)[pix1];
-        const float depth1 = r1.z;
         const int it1 = (int)r1.w - 1;
+        const float depth1 = r1.z;
+        const bool interior = it1 == it0;
+        if (interior && (DX < 0 || DY < 0)) continue;  // interior pair counted by the neighbour
         float c1[3], g1[3];
 #pragma unroll
         for (int i = 0; i < 3; ++i) { c1[i] = color[pix1 * 3 + i]; g1[i] = grad_color[pix1 * 3 + i]; }
@@ -378,75 +413,89 @@ __device__ __forceinline__ int edge_grad_pixel_split(int y0, int x0, int H, int 
         if (adj == 0.f) continue;
         const float gx = adj * (float)DX * (float)W / 2.f;
         const float gy = adj * (float)DY * (float)H / 2.f;
-        const float nx1 = -1.f + ((float)x1 + 0.5f) * sx;
-        const float ny1 = -1.f + ((float)y1 + 0.5f) * sy;
-        const float mx = 0.5f * (nx0 + nx1), my = 0.5f * (ny0 + ny1);
         const float hx = 0.5f * (float)DX * sx, hy = 0.5f * (float)DY * sy;  // centre -> midpoint
-        float tb0, tb1, cz1, cw1;
-        if (edge_frame_cover(fr, 2.f * hx, 2.f * hy, tb0, tb1, cz1, cw1)) {
-            const float d1_it0 = cz1 / cw1;
-            // it1 hides it0 at the neighbour.  Only a triangle intersection
-            // contributes, which needs it1 behind it0 at this pixel: never
-            // when it1's depth bound lies in front of depth0.
-            if (it1 >= 0 && depth1 < d1_it0) {
-                if (tboxes[it1].zhi < depth0) continue;
-                float4 P1[3];
-                {
-                    const TriVerts v = tverts[it1];
-                    P1[0] = v.p0; P1[1] = v.p1; P1[2] = v.p2;
-                }
-                float cz0, cw0;
-                if (intersect_triangle(ny0, nx0, P1[0], P1[1], P1[2], tb0, tb1, cz0, cw0)) {
-                    const float d0_it1 = cz0 / cw0;
-                    if (depth0 < d0_it1) {  // triangle intersection
-                        float nv[3], nf[3];
-                        if (tri_normal_ndc(P0, nv) && tri_normal_ndc(P1, nf)) {
-                            float gxn = 0.f, gyn = 0.f, gzn = 0.f;
-                            if (DX != 0) {
-                                float dbx, dbz;
-                                db_dp_2d(nv[0], nv[2], nf[0], nf[2], dbx, dbz);
-                                gxn = gx * dbx; gzn = gx * dbz;
-                            } else {
-                                float dby, dbz;
-                                db_dp_2d(nv[1], nv[2], nf[1], nf[2], dby, dbz);
-                                gyn = gy * dby; gzn = gy * dbz;
-                            }
-                            float mb0, mb1, mz, mw;
-                            if (edge_frame_cover(fr, hx, hy, mb0, mb1, mz, mw))
-                                add_contrib_at(mb0, mb1, mz, mw, mx, my, gxn, gyn, gzn, true, acc);
-                        }
-                    }
-                }
-            } else if (it1 < 0 || depth0 < depth1) {  // active opacity edge
-                float mb0, mb1, mz, mw;
-                if (edge_frame_cover(fr, hx, hy, mb0, mb1, mz, mw))
-                    add_contrib_at(mb0, mb1, mz, mw, mx, my, gx, gy, 0.f, false, acc);
-            }
-        } else if (it1 < 0 || depth0 < depth1) {  // active geometric edge
-            int i0, i1;
-            float s0, s1;
-            const TriNdc q = tndc[it0];
-            const float rx[3] = {q.a.x, q.a.z, q.b.x}, ry[3] = {q.a.y, q.a.w, q.b.y};
-            if (find_edge_intersection_ndc(P0, rx, ry, nx0, ny0, nx1, ny1, i0, i1, s0, s1)) {
-                const float4 A = i0 == 0 ? P0[0] : (i0 == 1 ? P0[1] : P0[2]);
-                const float4 Bv = i1 == 0 ? P0[0] : (i1 == 1 ? P0[1] : P0[2]);
-                const float cx = s0 * A.x + s1 * Bv.x;
-                const float cy = s0 * A.y + s1 * Bv.y;
-                const float cw = s0 * A.w + s1 * Bv.w;
-                const float iw = 1.f / cw, iw2 = iw * iw;
-                const float gsum = gx * cx + gy * cy;
+        float ge_x = gx, ge_y = gy, ge_z = 0.f;
+        bool at_mid = true;
+        // per-vertex weights u_k and the scalar q of the w-component:
+        // g[k] += u_k (ge_x, ge_y, ge_z, -q)
+        float u0 = 0.f, u1 = 0.f, u2 = 0.f, q = 0.f;
+        if (interior) {
+            ge_x = 2.f * gx; ge_y = 2.f * gy;
+        } else {
+            float A1[3];
 #pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    const float s = k == i0 ? s0 : (k == i1 ? s1 : 0.f);
-                    if (k == i0 || k == i1) {
-                        acc.g[k * 4 + 0] += s * gx * iw;
-                        acc.g[k * 4 + 1] += s * gy * iw;
-                        acc.g[k * 4 + 3] += -s * gsum * iw2;
+            for (int k = 0; k < 3; ++k) A1[k] = fmaf(ay[k], 2.f * hy, fmaf(ax[k], 2.f * hx, A[k]));
+            const float S1 = A1[0] + A1[1] + A1[2];
+            if (S1 != 0.f && A1[0] * S1 >= 0.f && A1[1] * S1 >= 0.f && A1[2] * S1 >= 0.f) {
+                // the neighbour centre lies inside it0: implicit edge
+                const float z1 = A1[0] * P0[0].z + A1[1] * P0[1].z + A1[2] * P0[2].z;
+                const float w1 = A1[0] * P0[0].w + A1[1] * P0[1].w + A1[2] * P0[2].w;
+                if (it1 >= 0 && depth1 < z1 / w1) {  // it1 hides it0 at the neighbour
+                    if (!intersection_pair(P0, tverts, tboxes, it1, depth0, nx0, ny0, DX, gx, gy, ge_x, ge_y, ge_z))
+                        continue;
+                } else if (!(it1 < 0 || depth0 < depth1)) {
+                    continue;
+                }
+            } else {
+                // the neighbour centre lies outside it0: geometric edge
+                if (!(it1 < 0 || depth0 < depth1)) continue;
+                // exit edge: the first edge function to change sign along p0 -> p1, in the
+                // reference's test order (0,1) = k 2, (1,2) = k 0, (2,0) = k 1
+                float tb = 2.f;
+                int kb = -1;
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const int k = (j + 2) % 3;
+                    const float s0 = fmaxf(sgn * A[k], 0.f), s1 = sgn * A1[k];
+                    if (s1 <= 0.f && s1 < s0) {
+                        const float t = __fdividef(s0, s0 - s1);
+                        if (t < tb) { tb = t; kb = k; }
                     }
                 }
-                acc.any = true;
+                if (kb < 0) continue;
+                const float ix = nx0 + tb * (2.f * hx), iy = ny0 + tb * (2.f * hy);
+                const float4 Av = kb == 0 ? P0[1] : (kb == 1 ? P0[2] : P0[0]);
+                const float4 Bv = kb == 0 ? P0[2] : (kb == 1 ? P0[0] : P0[1]);
+                const float dx = Bv.x - Av.x, dy = Bv.y - Av.y, dw = Bv.w - Av.w;
+                const float qx = Av.x - ix * Av.w, qy = Av.y - iy * Av.w;
+                const float bx = dx - ix * dw, by = dy - iy * dw;
+                const float den = bx * bx + by * by;
+                const float t = den != 0.f ? -__fdividef(qx * bx + qy * by, den) : 0.5f;
+                const float s0 = 1.f - t, s1 = t;
+                const float cw = s0 * Av.w + s1 * Bv.w;
+                const float iw = __fdividef(1.f, cw);
+                const float cx = s0 * Av.x + s1 * Bv.x, cy = s0 * Av.y + s1 * Bv.y;
+                q = (gx * cx + gy * cy) * iw;
+                // vertices (i0, i1) = (kb + 1, kb + 2) mod 3 carry (s0, s1)
+                const float v0 = s0 * iw, v1 = s1 * iw;
+                u0 = kb == 0 ? 0.f : (kb == 1 ? v1 : v0);
+                u1 = kb == 1 ? 0.f : (kb == 2 ? v1 : v0);
+                u2 = kb == 2 ? 0.f : (kb == 0 ? v1 : v0);
+                at_mid = false;
             }
         }
+        if (at_mid) {
+            float Am[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) Am[k] = fmaf(ay[k], hy, fmaf(ax[k], hx, A[k]));
+            const float Sm = Am[0] + Am[1] + Am[2];
+            if (!(Sm != 0.f && Am[0] * Sm >= 0.f && Am[1] * Sm >= 0.f && Am[2] * Sm >= 0.f)) continue;
+            // b_k / cw = A_k / sum(A_k w_k);  cz / cw = sum(A_k z_k) / sum(A_k w_k)
+            const float Ws = Am[0] * P0[0].w + Am[1] * P0[1].w + Am[2] * P0[2].w;
+            const float Zs = Am[0] * P0[0].z + Am[1] * P0[1].z + Am[2] * P0[2].z;
+            const float iW = __fdividef(1.f, Ws);
+            u0 = Am[0] * iW; u1 = Am[1] * iW; u2 = Am[2] * iW;
+            q = ge_x * (nx0 + hx) + ge_y * (ny0 + hy) + ge_z * (Zs * iW);
+        }
+        const float uv[3] = {u0, u1, u2};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            acc.g[k * 4 + 0] += uv[k] * ge_x;
+            acc.g[k * 4 + 1] += uv[k] * ge_y;
+            acc.g[k * 4 + 2] += uv[k] * ge_z;
+            acc.g[k * 4 + 3] -= uv[k] * q;
+        }
+        acc.any = true;
     }
     return it0;
 }

@@ -351,7 +351,7 @@ __global__ void __launch_bounds__(kEdgeThreads, DSB_EDGE_MIN_CTAS) edge_step_ker
         const int y = local / vd.W, x = local - y * vd.W;
         const size_t tb = (size_t)b * T;
         it0 = edge_grad_pixel_split(y, x, vd.H, vd.W, color, grad_color, rast, tab.verts + tb, tab.boxes + tb,
-                                    tab.ndc + tb, vd.pix_offset, acc);
+                                    vd.pix_offset, acc);
     }
     const int key = (it0 >= 0 && acc.any) ? it0 : -1 - lane;
     const int prev = __shfl_up_sync(0xffffffffu, key, 1);
