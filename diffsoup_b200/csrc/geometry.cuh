@@ -146,6 +146,99 @@ __device__ __forceinline__ bool block_surely_outside(float4 p0, float4 p1, float
     return a2 < -(t2 + 0x1p-19f * (m + tA));
 }
 
+// Per-triangle data of the block test of the rasterizer's staging pass:
+// e[k] = (ox, oy, oc, m) such that, for any block of pixel centres inside
+// the rect the record was built for, no centre can pass the reference's
+// coverage test when  max over the block of ox x + oy y + oc  <  -m  for
+// some k.  (ox, oy, oc) is the exact affine edge function E_k of
+// edge_terms (the w-products cancel), oriented so that the inside is
+// positive, and m bounds the difference between E_k and the reference's
+// FP32 value A_k, the evaluation of the rounded coefficients, and the
+// conditions under which surely_outside() rejects.  A record that
+// rejects nothing has oc = 1, m = 0.
+struct __align__(16) TriEdges {
+    float4 e[3];
+};
+
+// Builds the TriEdges of a triangle over the pixel-centre NDC rect
+// [xa, xb] x [ya, yb] (every |coordinate| <= 1).  The arithmetic is FP64:
+// products of two floats are exact, so the coefficients carry one rounding.
+//  * Bounds: |q| = |p.xy - ndc p.w| over the rect is largest at its ends;
+//    with S_k = Qx_u Qy_v + Qy_u Qx_v, the reference's A_k differs from E_k
+//    by at most t_k = 2^-18 S_k (as in block_surely_outside), and its
+//    A = rn(rn(A0 + A1) + A2) from S = sum E_k by at most
+//    tA = t0 + t1 + t2 + 2^-22 (|E0| + |E1| + |E2|).
+//  * S is affine, so its extremes over the rect lie at corners; the test
+//    needs one sign with 2^-60 <= |A| <= 2^60 over the rect.
+//  * k = 0, 1: A_k of the opposite sign to A with |A_k| > 2^-100 |A|
+//    rejects (surely_outside); margin t_k + 2^-99 max|A|.
+//  * k = 2: A2 of the opposite sign with |A2| > 2^-20 (|A| + |A0| + |A1|)
+//    rejects; margin t_2 + 2^-19 (max|A| + max|A0| + max|A1|).
+//  * The block maximum is computed in FP32 from the rounded coefficients,
+//    within 2^-22 (|ox| + |oy| + |oc|) for |x|, |y| <= 1; margin 2^-21 of it.
+__device__ inline TriEdges tri_edges_over_rect(float4 p0, float4 p1, float4 p2, float xa, float xb, float ya,
+                                               float yb) {
+    TriEdges out;
+    const double4 P[3] = {make_double4(p0.x, p0.y, p0.z, p0.w), make_double4(p1.x, p1.y, p1.z, p1.w),
+                          make_double4(p2.x, p2.y, p2.z, p2.w)};
+    double Qx[3], Qy[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        Qx[i] = fmax(fabs(P[i].x - (double)xa * P[i].w), fabs(P[i].x - (double)xb * P[i].w)) * (1.0 + 0x1p-20);
+        Qy[i] = fmax(fabs(P[i].y - (double)ya * P[i].w), fabs(P[i].y - (double)yb * P[i].w)) * (1.0 + 0x1p-20);
+    }
+    double ax[3], ay[3], c[3], t[3], emax[3];
+    const double cx[2] = {(double)xa, (double)xb}, cy[2] = {(double)ya, (double)yb};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const double4 u = P[(k + 1) % 3], v = P[(k + 2) % 3];
+        ax[k] = u.y * v.w - u.w * v.y;
+        ay[k] = u.w * v.x - u.x * v.w;
+        c[k] = u.x * v.y - u.y * v.x;
+        t[k] = 0x1p-18 * (Qx[(k + 1) % 3] * Qy[(k + 2) % 3] + Qy[(k + 1) % 3] * Qx[(k + 2) % 3]);
+        double m = 0.0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) m = fmax(m, fabs(c[k] + ax[k] * cx[j & 1] + ay[k] * cy[j >> 1]));
+        emax[k] = m + t[k];
+    }
+    const double tA = t[0] + t[1] + t[2] + 0x1p-22 * (emax[0] + emax[1] + emax[2]);
+    const double sx = ax[0] + ax[1] + ax[2], sy = ay[0] + ay[1] + ay[2], sc = c[0] + c[1] + c[2];
+    double slo = INFINITY, shi = -INFINITY;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const double s = sc + sx * cx[j & 1] + sy * cy[j >> 1];
+        slo = fmin(slo, s);
+        shi = fmax(shi, s);
+    }
+    double sgn = 0.0;
+    if (slo - tA >= 0x1p-60 && shi + tA <= 0x1p60) sgn = 1.0;
+    else if (-shi - tA >= 0x1p-60 && -slo + tA <= 0x1p60) sgn = -1.0;
+    const double amax = fmax(fabs(slo), fabs(shi)) + tA;
+    const double m01 = 0x1p-99 * amax, m2 = 0x1p-19 * (amax + emax[0] + emax[1]);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const double m = t[k] + (k == 2 ? m2 : m01) + 0x1p-21 * (fabs(ax[k]) + fabs(ay[k]) + fabs(c[k]));
+        const float mf = (float)(m * (1.0 + 0x1p-20));
+        const bool ok = sgn != 0.0 && isfinite(m) && isfinite(mf);
+        out.e[k] = ok ? make_float4((float)(sgn * ax[k]), (float)(sgn * ay[k]), (float)(sgn * c[k]), mf)
+                      : make_float4(0.f, 0.f, 1.f, 0.f);
+    }
+    return out;
+}
+
+// True when the TriEdges record proves that no pixel centre of the block
+// [xa, xb] x [ya, yb] (inside the record's rect) is covered.
+__device__ __forceinline__ bool edges_reject_block(const TriEdges& r, float xa, float xb, float ya, float yb) {
+    bool out = false;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float4 e = r.e[k];
+        const float v = fmaf(e.x, e.x > 0.f ? xb : xa, fmaf(e.y, e.y > 0.f ? yb : ya, e.z));
+        out = out || v < -e.w;
+    }
+    return out;
+}
+
 // Remainder of intersect_triangle given its edge terms (A != 0).
 __device__ __forceinline__ bool finish_coverage(float A0, float A1, float A, float4 p0, float4 p1, float4 p2,
                                                 float& b0, float& b1, float& z, float& w) {

@@ -32,6 +32,7 @@ struct TileWs {
     TriBox* boxes;
     TriVerts* verts;
     TriNdc* ndc;
+    TriEdges* edges;
     int* counts;
     int64_t* offsets;  // [num_tiles + 1] exclusive prefix of counts
     int* cursor;
@@ -50,6 +51,7 @@ static TileWs carve(void* ws, int B, int T, int num_tiles, int64_t capacity, siz
     w.boxes = reinterpret_cast<TriBox*>(p + o); o += al256((size_t)B * T * sizeof(TriBox));
     w.verts = reinterpret_cast<TriVerts*>(p + o); o += al256((size_t)B * T * sizeof(TriVerts));
     w.ndc = reinterpret_cast<TriNdc*>(p + o); o += al256((size_t)B * T * sizeof(TriNdc));
+    w.edges = reinterpret_cast<TriEdges*>(p + o); o += al256((size_t)B * T * sizeof(TriEdges));
     w.counts = reinterpret_cast<int*>(p + o); o += al256((size_t)num_tiles * sizeof(int));
     w.offsets = reinterpret_cast<int64_t*>(p + o); o += al256((size_t)(num_tiles + 1) * sizeof(int64_t));
     w.cursor = reinterpret_cast<int*>(p + o); o += al256((size_t)num_tiles * sizeof(int));
@@ -92,7 +94,7 @@ __global__ void __launch_bounds__(kThreads) bin_setup_kernel(int B, const ds_vie
                                                              const float* __restrict__ pos, int T,
                                                              const int* __restrict__ tri, TriBox* __restrict__ boxes,
                                                              TriVerts* __restrict__ verts, TriNdc* __restrict__ ndc,
-                                                             int* __restrict__ counts) {
+                                                             TriEdges* __restrict__ edges, int* __restrict__ counts) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (int64_t)B * T) return;
     const int b = (int)(i / T), t = (int)(i % T);
@@ -120,7 +122,12 @@ __global__ void __launch_bounds__(kThreads) bin_setup_kernel(int B, const ds_vie
     // mask (row-major over the rect) rides in the NDC record's spare lanes
     uint64_t m = 0;
     int tx0, tx1, ty0, ty1;
+    TriEdges te;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) te.e[k] = make_float4(0.f, 0.f, 1.f, 0.f);
     if (box_tiles(r, tx0, tx1, ty0, ty1)) {
+        te = tri_edges_over_rect(v.p0, v.p1, v.p2, pix_ndc(r.x0, vd.W), pix_ndc(r.x1 - 1, vd.W), pix_ndc(r.y0, vd.H),
+                                 pix_ndc(r.y1 - 1, vd.H));
         const int ntx = tx1 - tx0 + 1;
         const bool small = (ty1 - ty0 + 1) * ntx <= 64;
         for (int ty = ty0; ty <= ty1; ++ty)
@@ -135,6 +142,7 @@ __global__ void __launch_bounds__(kThreads) bin_setup_kernel(int B, const ds_vie
     q.b = make_float4(v.p2.x / v.p2.w, v.p2.y / v.p2.w, __uint_as_float((uint32_t)m),
                       __uint_as_float((uint32_t)(m >> 32)));
     ndc[i] = q;
+    edges[i] = te;
 }
 
 // Pass 2: scatter record indices into the per-tile lists.
@@ -309,12 +317,14 @@ struct WarpStage {
 };
 
 // Loads entries [g0, g0+32) of the work item's range, keeps those whose box
-// meets the block and whose depth bound passes `zcut` (zlo <= zcut), stages
-// them, and returns how many were staged.  *head_zlo receives the zlo of the
-// group's first entry (the smallest, when the list is ordered).
+// meets the block, whose depth bound passes `zcut` (zlo <= zcut) and whose
+// edge record does not prove the block uncovered, stages them, and returns
+// how many were staged.  *head_zlo receives the zlo of the group's first
+// entry (the smallest, when the list is ordered).
 __device__ __forceinline__ int stage_group(const BlockGeom& g, int64_t g0, const TriBox* __restrict__ boxes,
-                                           const TriVerts* __restrict__ verts, const int* __restrict__ list, int T,
-                                           float zcut, WarpStage& st, float* head_zlo) {
+                                           const TriVerts* __restrict__ verts, const TriEdges* __restrict__ edges,
+                                           const int* __restrict__ list, int T, float zcut, WarpStage& st,
+                                           float* head_zlo) {
     const int lane = threadIdx.x & 31;
     const int64_t e = g0 + lane;
     const bool in = e < g.end;
@@ -327,7 +337,13 @@ __device__ __forceinline__ int stage_group(const BlockGeom& g, int64_t g0, const
         bx = boxes[ri];
     }
     *head_zlo = __shfl_sync(0xffffffffu, bx.zlo, 0);
-    const bool c = in && box_overlaps(bx, g.wx0, g.wy0) && bx.zlo <= zcut;
+    bool c = in && box_overlaps(bx, g.wx0, g.wy0) && bx.zlo <= zcut;
+    if (c) {
+        // pixel-centre extents of the block (clamped to the view)
+        const float xa = pix_ndc(g.wx0, g.W), xb = pix_ndc(min(g.wx0 + 7, g.W - 1), g.W);
+        const float ya = pix_ndc(g.wy0, g.H), yb = pix_ndc(min(g.wy0 + 3, g.H - 1), g.H);
+        c = !edges_reject_block(edges[ri], xa, xb, ya, yb);
+    }
     const unsigned mask = __ballot_sync(0xffffffffu, c);
     if (c) {
         const int k = __popc(mask & ((1u << lane) - 1u));
@@ -430,9 +446,9 @@ __device__ __noinline__ void flush_records(const RecordStore& rs, WarpRecs& R, i
 template <bool REC>
 __global__ void __launch_bounds__(kWarpsPerCta * 32, DSB_RASTER_MIN_CTAS) raster_kernel(
     int B, const ds_view_desc* __restrict__ views, int num_tiles, int T, const TriBox* __restrict__ boxes,
-    const TriVerts* __restrict__ verts, const int64_t* __restrict__ offsets, const int* __restrict__ sorted,
-    const int* __restrict__ list, int64_t capacity, int level, int S, const float* __restrict__ alpha_src,
-    int thr_mode, float thr_const, const uint64_t* __restrict__ rng, int* work, float* __restrict__ rast,
+    const TriVerts* __restrict__ verts, const TriEdges* __restrict__ edges, const int64_t* __restrict__ offsets,
+    const int* __restrict__ sorted, const int* __restrict__ list, int64_t capacity, int level, int S,
+    const float* __restrict__ alpha_src, int thr_mode, float thr_const, const uint64_t* __restrict__ rng, int* work, float* __restrict__ rast,
     RecordStore rs) {
     __shared__ WarpStage s_stage[kWarpsPerCta];
     __shared__ WarpRecs s_rec[REC ? kWarpsPerCta : 1];
@@ -455,7 +471,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, DSB_RASTER_MIN_CTAS) raster
         float warp_far = warp_max(g.valid ? INFINITY : -INFINITY);
         for (int64_t g0 = g.begin; g0 < g.end; g0 += 32) {
             float head;
-            const int nc = stage_group(g, g0, boxes, verts, list, T, warp_far, st, &head);
+            const int nc = stage_group(g, g0, boxes, verts, edges, list, T, warp_far, st, &head);
             if (g.ordered && head > warp_far) break;  // this group and all later ones lie behind
             for (int k = 0; k < nc; ++k) {
                 if (st.box[k].zlo > warp_far) {
@@ -610,8 +626,9 @@ __global__ void __launch_bounds__(kRecChunk) aux_records_kernel(RecordStore rs, 
 // only the blocks listed there (*item_count of them) are processed.
 __global__ void __launch_bounds__(kWarpsPerCta * 32) aux_kernel(
     int B, const ds_view_desc* __restrict__ views, int num_tiles, int T, const TriBox* __restrict__ boxes,
-    const TriVerts* __restrict__ verts, const int64_t* __restrict__ offsets, const int* __restrict__ sorted,
-    const int* __restrict__ list, int64_t capacity, int level, int S, const float* __restrict__ alpha_src, int C,
+    const TriVerts* __restrict__ verts, const TriEdges* __restrict__ edges, const int64_t* __restrict__ offsets,
+    const int* __restrict__ sorted, const int* __restrict__ list, int64_t capacity, int level, int S,
+    const float* __restrict__ alpha_src, int C,
     const float* __restrict__ color, const float* __restrict__ target, const float* __restrict__ rast, float scale,
     const int* __restrict__ item_list, const int* __restrict__ item_count, int* work,
     float* __restrict__ grad_alpha_src) {
@@ -644,7 +661,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) aux_kernel(
         const float warp_far = warp_max(!g.valid ? -INFINITY : (tp >= 0 ? zp : INFINITY));
         for (int64_t g0 = g.begin; g0 < g.end; g0 += 32) {
             float head;
-            const int nc = stage_group(g, g0, boxes, verts, list, T, warp_far, st, &head);
+            const int nc = stage_group(g, g0, boxes, verts, edges, list, T, warp_far, st, &head);
             if (g.ordered && head > warp_far) break;
             for (int k = 0; k < nc; ++k) {
                 const TriBox r = st.box[k];
@@ -729,7 +746,7 @@ int ds_tiles_bin(int B, const ds_view_desc* views, int num_tiles, int V, const f
     const int64_t n = (int64_t)B * T;
     if (n > 0)
         bin_setup_kernel<<<blocks_for(n), kThreads, 0, st>>>(B, views, V, pos, T, tri, w.boxes, w.verts, w.ndc,
-                                                              w.counts);
+                                                              w.edges, w.counts);
     int64_t* total_dev = nullptr;
     rc = device_scan<int, int64_t>(w.counts, num_tiles, w.offsets, false, w.scan, st, &total_dev);
     if (rc) return rc;
@@ -775,12 +792,12 @@ int tiles_rasterize_impl(int B, const ds_view_desc* views, int num_tiles, int T,
     if (rs != nullptr) {
         const void* k = reinterpret_cast<const void*>(&raster_kernel<true>);
         raster_kernel<true><<<block_grid(num_tiles, k, g_occ_raster_rec), kWarpsPerCta * 32, 0, st>>>(
-            B, views, num_tiles, T, w.boxes, w.verts, w.offsets, w.sorted, w.list, list_capacity, level, S,
+            B, views, num_tiles, T, w.boxes, w.verts, w.edges, w.offsets, w.sorted, w.list, list_capacity, level, S,
             alpha_src, thr_mode, thr_const, rng, w.work, rast, *rs);
     } else {
         const void* k = reinterpret_cast<const void*>(&raster_kernel<false>);
         raster_kernel<false><<<block_grid(num_tiles, k, g_occ_raster), kWarpsPerCta * 32, 0, st>>>(
-            B, views, num_tiles, T, w.boxes, w.verts, w.offsets, w.sorted, w.list, list_capacity, level, S,
+            B, views, num_tiles, T, w.boxes, w.verts, w.edges, w.offsets, w.sorted, w.list, list_capacity, level, S,
             alpha_src, thr_mode, thr_const, rng, w.work, rast, RecordStore{});
     }
     return check_launch("tiles_rasterize");
@@ -794,7 +811,8 @@ static int aux_launch(int B, const ds_view_desc* views, int num_tiles, int T, in
     DS_CUDA(cudaMemsetAsync(w.work + 1, 0, sizeof(int), st));
     const void* k = reinterpret_cast<const void*>(&aux_kernel);
     aux_kernel<<<block_grid(num_tiles, k, g_occ_aux), kWarpsPerCta * 32, 0, st>>>(
-        B, views, num_tiles, T, w.boxes, w.verts, w.offsets, w.sorted, w.list, list_capacity, level, S, alpha_src, C,
+        B, views, num_tiles, T, w.boxes, w.verts, w.edges, w.offsets, w.sorted, w.list, list_capacity, level, S,
+        alpha_src, C,
         color, target, rast, scale, item_list, item_count, w.work + 1, grad_alpha_src);
     return check_launch("tiles_opacity_aux");
 }
