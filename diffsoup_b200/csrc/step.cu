@@ -439,6 +439,49 @@ static int mark(int i, cudaStream_t st) {
     return DS_OK;
 }
 
+// A second stream per device for the parts of the step that do not depend on
+// each other (level accumulation beside projection and binning; the opacity
+// auxiliary gradient beside the edge gradients).  The caller's stream forks
+// to it through an event and joins it back before the dependent kernels, so
+// the step stays one ordered unit on the caller's stream and captures into a
+// CUDA graph as parallel branches.  Created on a device's first step.
+constexpr int kMaxDevices = 64;
+struct SideStream {
+    cudaStream_t s = nullptr;
+    cudaEvent_t fork[2] = {nullptr, nullptr}, join[2] = {nullptr, nullptr};
+};
+static SideStream g_side[kMaxDevices];
+
+static SideStream* side_stream() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+    SideStream& x = g_side[dev];
+    if (x.s == nullptr) {
+        SideStream n;
+        if (cudaStreamCreateWithFlags(&n.s, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+        for (int i = 0; i < 2; ++i)
+            if (cudaEventCreateWithFlags(&n.fork[i], cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&n.join[i], cudaEventDisableTiming) != cudaSuccess)
+                return nullptr;
+        x = n;
+    }
+    return &x;
+}
+
+// The side stream starts after everything issued so far on st.
+static int fork_to(SideStream* x, int i, cudaStream_t st) {
+    DS_CUDA(cudaEventRecord(x->fork[i], st));
+    DS_CUDA(cudaStreamWaitEvent(x->s, x->fork[i], 0));
+    return DS_OK;
+}
+
+// Work issued on st from now on starts after the side stream's work.
+static int join_from(SideStream* x, int i, cudaStream_t st) {
+    DS_CUDA(cudaEventRecord(x->join[i], x->s));
+    DS_CUDA(cudaStreamWaitEvent(st, x->join[i], 0));
+    return DS_OK;
+}
+
 struct StepWs {
     float* pos;
     float* alpha_acc;
@@ -579,7 +622,13 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
                             reinterpret_cast<char*>(w.rec_counters + 2) - reinterpret_cast<char*>(w.grad_pos), st));
     DS_CUDA(cudaMemsetAsync(grad_mlp_params, 0, sizeof(float) * ds_mlp_param_count(c.C, c.hidden, c.n_layers), st));
 
-    // prep: opacity and feature accumulation + sigmoid, projection
+    // Side stream for independent parts; the phase events (profiling) time
+    // the phases one after another on st instead.
+    SideStream* side = g_step_nevents == 0 ? side_stream() : nullptr;
+    const cudaStream_t sst = side ? side->s : st;
+    if (side && (rc = fork_to(side, 0, st))) return rc;
+
+    // prep: opacity and feature accumulation + sigmoid (side), projection (st)
     const unsigned tb = (unsigned)((c.T + kPrepWarps - 1) / kPrepWarps);
     const bool tab = lattice_tab_fits(c.min_level, c.max_level, S, ST, c.C);
     const size_t tsm = lattice_tab_smem(c.min_level, c.max_level, S, ST, c.C);
@@ -587,16 +636,16 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     const unsigned tgrid = (unsigned)(tw < kSMs * 4 ? tw : kSMs * 4);  // persistent: tables built once per CTA
     if (c.T > 0 && tab) {
         if (k8)
-            accum_tab_kernel<8><<<tgrid, kTabWarps * 32, tsm, st>>>(c.T, c.min_level, c.max_level, S, ST, alpha_src,
-                                                                  feat_src, w.alpha_acc, w.feat_acc, w.feat_bf16);
-        else
-            accum_tab_kernel<16><<<tgrid, kTabWarps * 32, tsm, st>>>(c.T, c.min_level, c.max_level, S, ST, alpha_src,
+            accum_tab_kernel<8><<<tgrid, kTabWarps * 32, tsm, sst>>>(c.T, c.min_level, c.max_level, S, ST, alpha_src,
                                                                    feat_src, w.alpha_acc, w.feat_acc, w.feat_bf16);
+        else
+            accum_tab_kernel<16><<<tgrid, kTabWarps * 32, tsm, sst>>>(c.T, c.min_level, c.max_level, S, ST, alpha_src,
+                                                                    feat_src, w.alpha_acc, w.feat_acc, w.feat_bf16);
     } else if (c.T > 0) {
-        accum_sigmoid_kernel<false><<<tb, kPrepWarps * 32, 0, st>>>(c.T, c.min_level, c.max_level, c.max_level, S, ST, 1,
-                                                                   alpha_src, w.alpha_acc, nullptr);
-        accum_sigmoid_kernel<true><<<tb, kPrepWarps * 32, 0, st>>>(c.T, c.min_level, c.max_level, c.max_level, S, ST,
-                                                                  c.C, feat_src, w.feat_acc, w.feat_bf16);
+        accum_sigmoid_kernel<false><<<tb, kPrepWarps * 32, 0, sst>>>(c.T, c.min_level, c.max_level, c.max_level, S, ST,
+                                                                    1, alpha_src, w.alpha_acc, nullptr);
+        accum_sigmoid_kernel<true><<<tb, kPrepWarps * 32, 0, sst>>>(c.T, c.min_level, c.max_level, c.max_level, S, ST,
+                                                                   c.C, feat_src, w.feat_acc, w.feat_bf16);
     }
     if ((int64_t)c.B * c.V > 0)
         project_kernel<<<blocks_for((int64_t)c.B * c.V), kThreads, 0, st>>>(c.B, c.V, verts, mvp, w.pos);
@@ -608,6 +657,7 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     rc = ds_tiles_bin(c.B, views, num_tiles, c.V, w.pos, c.T, tri, w.tiles, w.tiles_bytes, list_capacity, status,
                       stream);
     if (rc || (rc = mark(2, st))) return rc;
+    if (side && (rc = join_from(side, 0, st))) return rc;  // the rasterizer reads the accumulated opacities
     rc = tiles_rasterize_impl(c.B, views, num_tiles, c.T, c.max_level, ST, w.alpha_acc, c.stochastic ? 1 : 0,
                               c.thr_const, rng, rast, w.tiles, list_capacity, rs, st);
     if (rc || (rc = mark(3, st))) return rc;
@@ -622,9 +672,11 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     rc = k8 ? launch_shade_small(a, st) : launch_shade<ShadeC16H64>(a, st);
     if (rc || (rc = mark(4, st))) return rc;
 
-    // opacity auxiliary gradient (scaled by 1/numel(colour), rasterize.py:183-195)
+    // opacity auxiliary gradient (scaled by 1/numel(colour), rasterize.py:183-195), on the side
+    // stream beside the edge gradients
+    if (side && (rc = fork_to(side, 1, st))) return rc;
     rc = tiles_aux_impl(c.B, views, num_tiles, c.T, c.max_level, ST, w.alpha_acc, w.l1, rast, a.inv_n,
-                        w.grad_alpha_acc, w.tiles, list_capacity, rs, st);
+                        w.grad_alpha_acc, w.tiles, list_capacity, rs, sst);
     if (rc || (rc = mark(5, st))) return rc;
 
     // edge gradients to clip-space positions
@@ -632,6 +684,7 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
         c.B, views, num_pixels, c.V, c.T, tiles_tables(w.tiles, c.B, c.T, num_tiles, list_capacity), tri, a.color,
         w.grad_color, rast, w.grad_pos);
     if ((rc = mark(6, st))) return rc;
+    if (side && (rc = join_from(side, 1, st))) return rc;  // the adjoints read the opacity gradients
     // adjoints of sigmoid + level accumulation, and of the projection
     if (c.T > 0 && tab) {
         if (k8)
