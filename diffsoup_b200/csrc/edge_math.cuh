@@ -324,11 +324,9 @@ __device__ __forceinline__ int edge_grad_pixel(int b, int y0, int x0, int H, int
 // The triangle-intersection case (rasterize.cu:760-809): the neighbour's
 // triangle it1 hides it0 there and lies behind it0 at this pixel.  Returns
 // false when the pair contributes nothing; else the gradient direction.
-__device__ __forceinline__ bool intersection_pair(const float4 P0[3], const TriVerts* __restrict__ tverts,
-                                               const TriBox* __restrict__ tboxes, int it1, float depth0, float nx0,
-                                               float ny0, int DX, float gx, float gy, float& gxn, float& gyn,
-                                               float& gzn) {
-    if (tboxes[it1].zhi < depth0) return false;  // it1 lies in front of depth0 everywhere
+__device__ __forceinline__ bool intersection_pair(const float4 P0[3], const TriVerts* __restrict__ tverts, int it1,
+                                               float depth0, float nx0, float ny0, int DX, float gx, float gy,
+                                               float& gxn, float& gyn, float& gzn) {
     const TriVerts v = tverts[it1];
     float tb0, tb1, cz0, cw0;
     if (!intersect_triangle(ny0, nx0, v.p0, v.p1, v.p2, tb0, tb1, cz0, cw0)) return false;
@@ -356,20 +354,30 @@ __device__ __forceinline__ float pair_adjoint3(const float* c0, const float* g0,
     return adj;
 }
 
-__device__ __forceinline__ int edge_grad_pixel_split(int y0, int x0, int H, int W, const float* __restrict__ color,
-                                                     const float* __restrict__ grad_color,
-                                                     const float* __restrict__ rast,
-                                                     const TriVerts* __restrict__ tverts,
-                                                     const TriBox* __restrict__ tboxes, int64_t base,
-                                                     EdgeAccum& acc) {
+// A 16x16 screen tile of the pixel buffers with a one-pixel border, staged
+// in shared memory by the edge-gradient kernel: per pixel its triangle
+// (-1 background, kOutside beyond the view), depth, colour, dL/dcolour and
+// the far depth bound of its triangle.
+constexpr int kHaloW = DS_TILE + 2;
+constexpr int kHaloN = kHaloW * kHaloW;
+constexpr int kOutside = -2;
+
+struct EdgeHalo {
+    int it[kHaloN];
+    float dep[kHaloN];
+    float zhi[kHaloN];
+    float c[3][kHaloN];
+    float g[3][kHaloN];
+};
+
+__device__ __forceinline__ int edge_grad_pixel_staged(const EdgeHalo& h, int hidx, int y0, int x0, int H, int W,
+                                                      const TriVerts* __restrict__ tverts, EdgeAccum& acc) {
 #pragma unroll
     for (int k = 0; k < 12; ++k) acc.g[k] = 0.f;
     acc.any = false;
-    const int64_t pix0 = base + (int64_t)y0 * W + x0;
-    const float4 r0 = reinterpret_cast<const float4*>(rast)[pix0];
-    const int it0 = (int)r0.w - 1;
+    const int it0 = h.it[hidx];
     if (it0 < 0) return -1;
-    const float depth0 = r0.z;
+    const float depth0 = h.dep[hidx];
     // pixel-centre NDC with one reciprocal per axis (this path is compared to
     // the oracle with a tolerance; the 1-ulp difference is far below it)
     const float sx = 2.f / (float)W, sy = 2.f / (float)H;
@@ -392,23 +400,21 @@ __device__ __forceinline__ int edge_grad_pixel_split(int y0, int x0, int H, int 
     const float sgn = As > 0.f ? 1.f : -1.f;  // orientation of the inside near the pixel
     float c0[3], g0[3];
 #pragma unroll
-    for (int i = 0; i < 3; ++i) { c0[i] = color[pix0 * 3 + i]; g0[i] = grad_color[pix0 * 3 + i]; }
+    for (int i = 0; i < 3; ++i) { c0[i] = h.c[i][hidx]; g0[i] = h.g[i][hidx]; }
     // neighbours (+x, -x, -y, +y) as in rasterize.cu:691-692
 #pragma unroll 1
     for (int e = 0; e < 4; ++e) {
         const int DX = (e == 0) - (e == 1);
         const int DY = (e == 3) - (e == 2);
-        const int y1 = y0 + DY, x1 = x0 + DX;
-        if (y1 < 0 || y1 >= H || x1 < 0 || x1 >= W) continue;
-        const int64_t pix1 = base + (int64_t)y1 * W + x1;
-        const float4 r1 = reinterpret_cast<const float4*>(rast)[pix1];
-        const int it1 = (int)r1.w - 1;
-        const float depth1 = r1.z;
+        const int n = hidx + DX + DY * kHaloW;
+        const int it1 = h.it[n];
+        if (it1 == kOutside) continue;  // no neighbour in the view
+        const float depth1 = h.dep[n];
         const bool interior = it1 == it0;
         if (interior && (DX < 0 || DY < 0)) continue;  // interior pair counted by the neighbour
         float c1[3], g1[3];
 #pragma unroll
-        for (int i = 0; i < 3; ++i) { c1[i] = color[pix1 * 3 + i]; g1[i] = grad_color[pix1 * 3 + i]; }
+        for (int i = 0; i < 3; ++i) { c1[i] = h.c[i][n]; g1[i] = h.g[i][n]; }
         const float adj = pair_adjoint3(c0, g0, c1, g1);
         if (adj == 0.f) continue;
         const float gx = adj * (float)DX * (float)W / 2.f;
@@ -431,7 +437,10 @@ __device__ __forceinline__ int edge_grad_pixel_split(int y0, int x0, int H, int 
                 const float z1 = A1[0] * P0[0].z + A1[1] * P0[1].z + A1[2] * P0[2].z;
                 const float w1 = A1[0] * P0[0].w + A1[1] * P0[1].w + A1[2] * P0[2].w;
                 if (it1 >= 0 && depth1 < z1 / w1) {  // it1 hides it0 at the neighbour
-                    if (!intersection_pair(P0, tverts, tboxes, it1, depth0, nx0, ny0, DX, gx, gy, ge_x, ge_y, ge_z))
+                    // a triangle intersection needs it1 behind depth0 at this pixel: never when
+                    // it1's far depth bound lies in front of it
+                    if (h.zhi[n] < depth0 ||
+                        !intersection_pair(P0, tverts, it1, depth0, nx0, ny0, DX, gx, gy, ge_x, ge_y, ge_z))
                         continue;
                 } else if (!(it1 < 0 || depth0 < depth1)) {
                     continue;

@@ -320,43 +320,72 @@ __global__ void __launch_bounds__(kThreads) project_backward_kernel(int B, int V
     grad_verts[(size_t)v * 3 + 2] = (float)gz;
 }
 
-// Edge gradients over packed views (rasterize.cu:653-903), one pixel per
-// thread.  Consecutive pixels of a row mostly share a triangle: a segmented
-// warp reduction sums runs of equal (view, triangle) before one FP64 atomic
-// per vertex component.
-constexpr int kEdgeThreads = 128;
+// Edge gradients over packed views (rasterize.cu:653-903): one CTA per
+// 16x16 screen tile, one thread per pixel.  The tile and its one-pixel
+// border are staged in shared memory first (triangle, depth, colour,
+// dL/dcolour and the triangle's far depth bound), so the four neighbours of
+// every pixel are shared-memory reads.  Pixels of a warp (two rows of 16)
+// mostly share a triangle along a row: a segmented warp reduction sums runs
+// of equal triangles before one FP64 atomic per vertex component.
+constexpr int kEdgeThreads = DS_TILE * DS_TILE;
 #ifndef DSB_EDGE_MIN_CTAS
-#define DSB_EDGE_MIN_CTAS 6  // resident 4-warp CTAs per SM the register budget is sized for
+#define DSB_EDGE_MIN_CTAS 3  // resident 8-warp CTAs per SM the register budget is sized for
 #endif
 
-__global__ void __launch_bounds__(kEdgeThreads, DSB_EDGE_MIN_CTAS) edge_step_kernel(int B, const ds_view_desc* __restrict__ views,
-                                                                 int64_t num_pixels, int V, int T,
-                                                                 TileTables tab,
-                                                                 const int* __restrict__ tri,
-                                                                 const float* __restrict__ color,
-                                                                 const float* __restrict__ grad_color,
-                                                                 const float* __restrict__ rast,
-                                                                 double* __restrict__ grad_pos) {
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ int tile_view(const ds_view_desc* __restrict__ views, int B, int tile) {
+    int lo = 0, hi = B - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&views[mid].tile_base) <= tile) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(kEdgeThreads, DSB_EDGE_MIN_CTAS) edge_step_kernel(
+    int B, const ds_view_desc* __restrict__ views, int V, int T, TileTables tab, const int* __restrict__ tri,
+    const float* __restrict__ color, const float* __restrict__ grad_color, const float* __restrict__ rast,
+    double* __restrict__ grad_pos) {
+    __shared__ EdgeHalo h;
+    const int tile = blockIdx.x;
+    const int b = tile_view(views, B, tile);
+    const ds_view_desc vd = views[b];
+    const int tl = tile - vd.tile_base;
+    const int tx0 = (tl % vd.tiles_x) * DS_TILE, ty0 = (tl / vd.tiles_x) * DS_TILE;
+    const TriBox* __restrict__ boxes = tab.boxes + (size_t)b * T;
+    for (int i = threadIdx.x; i < kHaloN; i += kEdgeThreads) {
+        const int hy = i / kHaloW, hx = i - (i / kHaloW) * kHaloW;
+        const int y = ty0 + hy - 1, x = tx0 + hx - 1;
+        int it = kOutside;
+        float dep = 0.f, zh = 0.f, cc[3] = {0.f, 0.f, 0.f}, gg[3] = {0.f, 0.f, 0.f};
+        if (y >= 0 && y < vd.H && x >= 0 && x < vd.W) {
+            const int64_t p = vd.pix_offset + (int64_t)y * vd.W + x;
+            const float4 r = reinterpret_cast<const float4*>(rast)[p];
+            it = (int)r.w - 1;
+            dep = r.z;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) { cc[k] = color[p * 3 + k]; gg[k] = grad_color[p * 3 + k]; }
+            if (it >= 0) zh = boxes[it].zhi;
+        }
+        h.it[i] = it;
+        h.dep[i] = dep;
+        h.zhi[i] = zh;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { h.c[k][i] = cc[k]; h.g[k][i] = gg[k]; }
+    }
+    __syncthreads();
     const int lane = threadIdx.x & 31;
+    const int ly = threadIdx.x / DS_TILE, lx = threadIdx.x % DS_TILE;
+    const int y = ty0 + ly, x = tx0 + lx;
     EdgeAccum acc;
 #pragma unroll
     for (int k = 0; k < 12; ++k) acc.g[k] = 0.f;
     acc.any = false;
-    int b = 0, it0 = -1;
-    if (p < num_pixels) {
-        b = view_of_pixel(views, B, p);
-        const ds_view_desc vd = views[b];
-        const int local = (int)(p - vd.pix_offset);  // < H*W < 2^31: 32-bit division
-        const int y = local / vd.W, x = local - y * vd.W;
-        const size_t tb = (size_t)b * T;
-        it0 = edge_grad_pixel_split(y, x, vd.H, vd.W, color, grad_color, rast, tab.verts + tb, tab.boxes + tb,
-                                    vd.pix_offset, acc);
-    }
+    int it0 = -1;
+    if (y < vd.H && x < vd.W)
+        it0 = edge_grad_pixel_staged(h, (ly + 1) * kHaloW + lx + 1, y, x, vd.H, vd.W, tab.verts + (size_t)b * T, acc);
     const int key = (it0 >= 0 && acc.any) ? it0 : -1 - lane;
     const int prev = __shfl_up_sync(0xffffffffu, key, 1);
-    const int prevb = __shfl_up_sync(0xffffffffu, b, 1);
-    const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || prev != key || prevb != b);
+    const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || prev != key);
     const int seg = __popc(heads & ((2u << lane) - 1u));
     int oseg[5];
 #pragma unroll
@@ -680,9 +709,9 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     if (rc || (rc = mark(5, st))) return rc;
 
     // edge gradients to clip-space positions
-    edge_step_kernel<<<blocks_for(num_pixels, kEdgeThreads), kEdgeThreads, 0, st>>>(
-        c.B, views, num_pixels, c.V, c.T, tiles_tables(w.tiles, c.B, c.T, num_tiles, list_capacity), tri, a.color,
-        w.grad_color, rast, w.grad_pos);
+    edge_step_kernel<<<(unsigned)num_tiles, kEdgeThreads, 0, st>>>(
+        c.B, views, c.V, c.T, tiles_tables(w.tiles, c.B, c.T, num_tiles, list_capacity), tri, a.color, w.grad_color,
+        rast, w.grad_pos);
     if ((rc = mark(6, st))) return rc;
     if (side && (rc = join_from(side, 1, st))) return rc;  // the adjoints read the opacity gradients
     // adjoints of sigmoid + level accumulation, and of the projection
