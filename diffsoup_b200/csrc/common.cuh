@@ -119,6 +119,41 @@ __device__ __forceinline__ float philox_uniform(uint64_t seed, uint32_t iter, ui
     return (float)(c0 >> 8) * (1.0f / 16777216.0f);
 }
 
+// The same draw split in two: with counter (pixel, tri, view, iter), the
+// first two rounds touch the triangle only through one word of round 0, so
+// the rest of them is done once per (view, pixel) by philox_pixel and the
+// per-triangle remainder is one wide multiply and two XORs before rounds
+// 2..9 (philox_uniform_tri(philox_pixel(...), ...) == philox_uniform(...)).
+struct PhiloxPixel {
+    uint32_t c0, c1, x2, u;  // round-2 words 0 and 1, the pixel's part of word 2, the view's part of round 0
+};
+
+__device__ __forceinline__ PhiloxPixel philox_pixel(uint64_t seed, uint32_t iter, uint32_t view, uint32_t pixel) {
+    const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+    PhiloxPixel pp;
+    pp.u = __umulhi(0xCD9E8D57u, view) ^ k0;
+    const uint32_t c2 = __umulhi(0xD2511F53u, pixel) ^ iter ^ k1;
+    pp.c0 = __umulhi(0xCD9E8D57u, c2) ^ (0xCD9E8D57u * view) ^ (k0 + 0x9E3779B9u);
+    pp.c1 = 0xCD9E8D57u * c2;
+    pp.x2 = (0xD2511F53u * pixel) ^ (k1 + 0xBB67AE85u);
+    return pp;
+}
+
+__device__ __forceinline__ float philox_uniform_tri(const PhiloxPixel& pp, uint64_t seed, uint32_t tri) {
+    const uint32_t w = pp.u ^ tri;
+    uint32_t c0 = pp.c0, c1 = pp.c1, c2 = __umulhi(0xD2511F53u, w) ^ pp.x2, c3 = 0xD2511F53u * w;
+    uint32_t k0 = (uint32_t)seed + 2u * 0x9E3779B9u, k1 = (uint32_t)(seed >> 32) + 2u * 0xBB67AE85u;
+#pragma unroll
+    for (int r = 2; r < 10; ++r) {
+        const uint32_t lo0 = 0xD2511F53u * c0, hi0 = __umulhi(0xD2511F53u, c0);
+        const uint32_t lo1 = 0xCD9E8D57u * c2, hi1 = __umulhi(0xCD9E8D57u, c2);
+        const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+        k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+    }
+    return (float)(c0 >> 8) * (1.0f / 16777216.0f);
+}
+
 // Packed depth key of rasterize.cu:308-312: float bits of (z + 2) above a
 // 32-bit tie-break (fragment order, i.e. triangle index within a view).
 __device__ __forceinline__ unsigned long long depth_key(float z, uint32_t tie) {

@@ -463,12 +463,13 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, DSB_RASTER_MIN_CTAS) raster
     for (int item = warp_next(work); item < items; item = warp_next(work)) {
         const BlockGeom g = block_geometry(item, B, views, T, offsets, sorted, capacity);
         const float ndc_x = pix_ndc(g.px, g.W), ndc_y = pix_ndc(g.py, g.H);
-        const uint32_t pixel_id = (uint32_t)(g.py * g.W + g.px);
+        const PhiloxPixel php = philox_pixel(seed, iter, (uint32_t)g.b, (uint32_t)(g.py * g.W + g.px));
         unsigned long long best = ~0ull;
         float bb0 = 0.f, bb1 = 0.f, bz = 0.f;
         int nrec = 0;
         // max over the warp of the lanes' winning depth (+inf while a valid lane has none)
         float warp_far = warp_max(g.valid ? INFINITY : -INFINITY);
+        bool all_won = false;  // every valid lane has a winner (before that, warp_far stays +inf)
         for (int64_t g0 = g.begin; g0 < g.end; g0 += 32) {
             float head;
             const int nc = stage_group(g, g0, boxes, verts, edges, list, T, warp_far, st, &head);
@@ -502,9 +503,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, DSB_RASTER_MIN_CTAS) raster
                             if (depth > -1.f) {
                                 if (key < best) {
                                     const float alpha = interp_scalar(b0, b1, level, level, alpha_src + (size_t)t * S);
-                                    const float thr = thr_mode == 1
-                                                          ? philox_uniform(seed, iter, (uint32_t)g.b, pixel_id, t)
-                                                          : thr_const;
+                                    const float thr = thr_mode == 1 ? philox_uniform_tri(php, seed, t) : thr_const;
                                     if (!(alpha < thr)) {
                                         best = key; bb0 = b0; bb1 = b1; bz = depth;
                                         improved = true;
@@ -525,8 +524,10 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, DSB_RASTER_MIN_CTAS) raster
                         nrec += __popc(m);
                     }
                 }
-                if (__any_sync(0xffffffffu, improved))
-                    warp_far = warp_max(!g.valid ? -INFINITY : (best == ~0ull ? INFINITY : bz));
+                if (__any_sync(0xffffffffu, improved)) {
+                    if (!all_won) all_won = __all_sync(0xffffffffu, !g.valid || best != ~0ull);
+                    if (all_won) warp_far = warp_max(!g.valid ? -INFINITY : bz);
+                }
             }
             __syncwarp();  // the stage is rewritten by the next group
         }
