@@ -481,10 +481,15 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, DSB_RASTER_MIN_CTAS) raster
                 }
                 const float4 p0 = st.v[k].p0, p1 = st.v[k].p1, p2 = st.v[k].p2;
                 const TriBox r = st.box[k];
+                // lanes inside the rect whose winner does not lie in front of the triangle: zlo's
+                // margin exceeds the rounding of z + 2, so with zlo > bz every fragment's depth key
+                // lies strictly behind the winner's (neither a winner nor a record)
+                const bool near = g.valid && g.px >= r.x0 && g.px < r.x1 && g.py >= r.y0 && g.py < r.y1 &&
+                                  !(best != ~0ull && r.zlo > bz);
+                if (!__any_sync(0xffffffffu, near)) continue;  // warp-uniform
                 float A0, A1, A2, A;
                 edge_terms(ndc_y, ndc_x, p0, p1, p2, A0, A1, A2, A);
-                const bool cand = g.valid && g.px >= r.x0 && g.px < r.x1 && g.py >= r.y0 && g.py < r.y1 &&
-                                  !surely_outside(A0, A1, A2, A);
+                const bool cand = near && !surely_outside(A0, A1, A2, A);
                 if (!__any_sync(0xffffffffu, cand)) continue;  // warp-uniform
                 bool improved = false, rec = false;
                 float b0 = 0.f, b1 = 0.f, depth = 0.f;
@@ -668,10 +673,13 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) aux_kernel(
                 const TriBox r = st.box[k];
                 const int t = st.t[k];
                 const float4 p0 = st.v[k].p0, p1 = st.v[k].p1, p2 = st.v[k].p2;
+                // lanes inside the rect whose surface does not lie in front of the triangle
+                const bool near = g.valid && g.px >= r.x0 && g.px < r.x1 && g.py >= r.y0 && g.py < r.y1 &&
+                                  !(tp >= 0 && r.zlo > zp);
+                if (!__any_sync(0xffffffffu, near)) continue;  // warp-uniform
                 float A0, A1, A2, A;
                 edge_terms(ndc_y, ndc_x, p0, p1, p2, A0, A1, A2, A);
-                bool hit = g.valid && g.px >= r.x0 && g.px < r.x1 && g.py >= r.y0 && g.py < r.y1 &&
-                           !surely_outside(A0, A1, A2, A);
+                bool hit = near && !surely_outside(A0, A1, A2, A);
                 if (!__any_sync(0xffffffffu, hit)) continue;  // warp-uniform
                 float b0 = 0.f, b1 = 0.f;
                 if (hit) {
