@@ -137,47 +137,6 @@ __device__ __forceinline__ void add_contrib_at(float b0, float b1, float cz, flo
     a.any = true;
 }
 
-// The pixel's triangle's edge functions, which are affine in the NDC point:
-// evaluated at the pixel centre as the coverage test does, then stepped to
-// the neighbours' centres and the pair midpoints (the batched step compares
-// with the oracle within a tolerance; points within rounding of an edge may
-// be classified differently from a direct evaluation).
-struct EdgeFrame {
-    float A[3];       // edge functions at the pixel centre
-    float ax[3], ay[3];  // their derivatives along NDC x and y
-    float z[3], w[3];
-};
-
-__device__ __forceinline__ void edge_frame(const float4 P[3], float nx, float ny, EdgeFrame& f) {
-    float As;
-    edge_terms(ny, nx, P[0], P[1], P[2], f.A[0], f.A[1], f.A[2], As);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const float4 u = P[(k + 1) % 3], v = P[(k + 2) % 3];
-        f.ax[k] = u.y * v.w - u.w * v.y;
-        f.ay[k] = u.w * v.x - u.x * v.w;
-        f.z[k] = P[k].z;
-        f.w[k] = P[k].w;
-    }
-}
-
-// Coverage test and barycentrics at the centre offset by (dx, dy) in NDC.
-__device__ __forceinline__ bool edge_frame_cover(const EdgeFrame& f, float dx, float dy, float& b0, float& b1,
-                                                 float& z, float& w) {
-    const float A0 = fmaf(f.ay[0], dy, fmaf(f.ax[0], dx, f.A[0]));
-    const float A1 = fmaf(f.ay[1], dy, fmaf(f.ax[1], dx, f.A[1]));
-    const float A2 = fmaf(f.ay[2], dy, fmaf(f.ax[2], dx, f.A[2]));
-    const float A = A0 + A1 + A2;
-    if (!(A != 0.f)) return false;
-    const float inv = 1.f / A;
-    b0 = A0 * inv;
-    b1 = A1 * inv;
-    const float b2 = 1.f - b0 - b1;
-    z = b0 * f.z[0] + b1 * f.z[1] + b2 * f.z[2];
-    w = b0 * f.w[0] + b1 * f.w[1] + b2 * f.w[2];
-    return b0 >= 0.f && b1 >= 0.f && b0 + b1 <= 1.f;
-}
-
 // Edge-gradient estimator of one pixel (rasterize.cu:663-892).  Pixel
 // buffers are addressed as base + y*W + x with `base` the view's first pixel;
 // posb holds the view's clip positions.  Returns the pixel's triangle (or -1)
@@ -347,13 +306,6 @@ __device__ __forceinline__ bool intersection_pair(const float4 P0[3], const TriV
     return true;
 }
 
-__device__ __forceinline__ float pair_adjoint3(const float* c0, const float* g0, const float* c1, const float* g1) {
-    float adj = 0.f;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) adj += 0.5f * (g0[i] + g1[i]) * (c0[i] - c1[i]);
-    return adj;
-}
-
 // A 16x16 screen tile of the pixel buffers with a one-pixel border, staged
 // in shared memory by the edge-gradient kernel: per pixel its triangle
 // (-1 background, kOutside beyond the view), depth, colour, dL/dcolour and
@@ -370,141 +322,188 @@ struct EdgeHalo {
     float g[3][kHaloN];
 };
 
+// One pixel pair of the staged estimator: the pixel's frame (its triangle's
+// clip vertices, the edge functions at its centre and their NDC
+// derivatives) and the pair's neighbour offset.
+struct EdgeFrame {
+    float4 P[3];
+    float A[3], ax[3], ay[3];
+    float nx, ny, depth, sgn;
+};
+
+// Adds u_k (ge_x, ge_y, ge_z, -q) to vertex k's clip-space gradient.
+__device__ __forceinline__ void edge_accumulate(EdgeAccum& acc, float u0, float u1, float u2, float ge_x, float ge_y,
+                                                float ge_z, float q) {
+    const float uv[3] = {u0, u1, u2};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        acc.g[k * 4 + 0] += uv[k] * ge_x;
+        acc.g[k * 4 + 1] += uv[k] * ge_y;
+        acc.g[k * 4 + 2] += uv[k] * ge_z;
+        acc.g[k * 4 + 3] -= uv[k] * q;
+    }
+    acc.any = true;
+}
+
+// Contribution at the pair midpoint (centre + (hx, hy)): b_k / cw =
+// A_k / sum(A_k w_k) and cz / cw = sum(A_k z_k) / sum(A_k w_k).  Nothing
+// when the midpoint lies outside the triangle.
+__device__ __forceinline__ void edge_midpoint(const EdgeFrame& f, float hx, float hy, float ge_x, float ge_y,
+                                              float ge_z, EdgeAccum& acc) {
+    float Am[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) Am[k] = fmaf(f.ay[k], hy, fmaf(f.ax[k], hx, f.A[k]));
+    const float Sm = Am[0] + Am[1] + Am[2];
+    if (!(Sm != 0.f && Am[0] * Sm >= 0.f && Am[1] * Sm >= 0.f && Am[2] * Sm >= 0.f)) return;
+    const float Ws = Am[0] * f.P[0].w + Am[1] * f.P[1].w + Am[2] * f.P[2].w;
+    const float Zs = Am[0] * f.P[0].z + Am[1] * f.P[1].z + Am[2] * f.P[2].z;
+    const float iW = __fdividef(1.f, Ws);
+    const float q = ge_x * (f.nx + hx) + ge_y * (f.ny + hy) + ge_z * (Zs * iW);
+    edge_accumulate(acc, Am[0] * iW, Am[1] * iW, Am[2] * iW, ge_x, ge_y, ge_z, q);
+}
+
+// The pair's neighbour offset, adjoint direction and edge functions at the
+// neighbour centre (recomputed from the staged tile).
+struct EdgePair {
+    int DX, DY, n;
+    float gx, gy, hx, hy;
+    float A1[3];
+};
+
+__device__ __forceinline__ EdgePair edge_pair(const EdgeHalo& h, const EdgeFrame& f, int hidx, int e, int H, int W,
+                                              float sx, float sy) {
+    EdgePair p;
+    p.DX = (e == 0) - (e == 1);
+    p.DY = (e == 3) - (e == 2);
+    p.n = hidx + p.DX + p.DY * kHaloW;
+    float adj = 0.f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) adj += 0.5f * (h.g[i][hidx] + h.g[i][p.n]) * (h.c[i][hidx] - h.c[i][p.n]);
+    p.gx = adj * (float)p.DX * (float)W / 2.f;
+    p.gy = adj * (float)p.DY * (float)H / 2.f;
+    p.hx = 0.5f * (float)p.DX * sx;
+    p.hy = 0.5f * (float)p.DY * sy;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) p.A1[k] = fmaf(f.ay[k], 2.f * p.hy, fmaf(f.ax[k], 2.f * p.hx, f.A[k]));
+    return p;
+}
+
+// Edge-gradient estimator of one pixel from the staged tile: the pixel's
+// triangle (or -1) is returned and its clip-space vertex gradients are in
+// acc.g[vertex*4 + xyzw].  Interior and opacity-edge pairs (midpoint
+// contributions) are evaluated in the first pass over the four neighbours;
+// geometric-edge pairs and pairs that may be triangle intersections are
+// only marked there and evaluated in two further passes, where pass k takes
+// each lane's k-th marked pair, so that lanes run the rarer cases together.
 __device__ __forceinline__ int edge_grad_pixel_staged(const EdgeHalo& h, int hidx, int y0, int x0, int H, int W,
                                                       const TriVerts* __restrict__ tverts, EdgeAccum& acc) {
 #pragma unroll
     for (int k = 0; k < 12; ++k) acc.g[k] = 0.f;
     acc.any = false;
     const int it0 = h.it[hidx];
-    if (it0 < 0) return -1;
-    const float depth0 = h.dep[hidx];
+    unsigned geo = 0u, isect = 0u;  // pairs (bit e) of the second and third passes
+    EdgeFrame f;
     // pixel-centre NDC with one reciprocal per axis (this path is compared to
     // the oracle with a tolerance; the 1-ulp difference is far below it)
     const float sx = 2.f / (float)W, sy = 2.f / (float)H;
-    const float nx0 = -1.f + ((float)x0 + 0.5f) * sx;
-    const float ny0 = -1.f + ((float)y0 + 0.5f) * sy;
-    float4 P0[3];
-    {
-        const TriVerts v = tverts[it0];
-        P0[0] = v.p0; P0[1] = v.p1; P0[2] = v.p2;
-    }
-    float A[3], ax[3], ay[3], As;
-    edge_terms(ny0, nx0, P0[0], P0[1], P0[2], A[0], A[1], A[2], As);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const float4 u = P0[(k + 1) % 3], v = P0[(k + 2) % 3];
-        ax[k] = u.y * v.w - u.w * v.y;
-        ay[k] = u.w * v.x - u.x * v.w;
-    }
-    if (!(As != 0.f)) return it0;  // cannot happen for a covered pixel; nothing to add
-    const float sgn = As > 0.f ? 1.f : -1.f;  // orientation of the inside near the pixel
-    float c0[3], g0[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) { c0[i] = h.c[i][hidx]; g0[i] = h.g[i][hidx]; }
-    // neighbours (+x, -x, -y, +y) as in rasterize.cu:691-692
-#pragma unroll 1
-    for (int e = 0; e < 4; ++e) {
-        const int DX = (e == 0) - (e == 1);
-        const int DY = (e == 3) - (e == 2);
-        const int n = hidx + DX + DY * kHaloW;
-        const int it1 = h.it[n];
-        if (it1 == kOutside) continue;  // no neighbour in the view
-        const float depth1 = h.dep[n];
-        const bool interior = it1 == it0;
-        if (interior && (DX < 0 || DY < 0)) continue;  // interior pair counted by the neighbour
-        float c1[3], g1[3];
-#pragma unroll
-        for (int i = 0; i < 3; ++i) { c1[i] = h.c[i][n]; g1[i] = h.g[i][n]; }
-        const float adj = pair_adjoint3(c0, g0, c1, g1);
-        if (adj == 0.f) continue;
-        const float gx = adj * (float)DX * (float)W / 2.f;
-        const float gy = adj * (float)DY * (float)H / 2.f;
-        const float hx = 0.5f * (float)DX * sx, hy = 0.5f * (float)DY * sy;  // centre -> midpoint
-        float ge_x = gx, ge_y = gy, ge_z = 0.f;
-        bool at_mid = true;
-        // per-vertex weights u_k and the scalar q of the w-component:
-        // g[k] += u_k (ge_x, ge_y, ge_z, -q)
-        float u0 = 0.f, u1 = 0.f, u2 = 0.f, q = 0.f;
-        if (interior) {
-            ge_x = 2.f * gx; ge_y = 2.f * gy;
-        } else {
-            float A1[3];
-#pragma unroll
-            for (int k = 0; k < 3; ++k) A1[k] = fmaf(ay[k], 2.f * hy, fmaf(ax[k], 2.f * hx, A[k]));
-            const float S1 = A1[0] + A1[1] + A1[2];
-            if (S1 != 0.f && A1[0] * S1 >= 0.f && A1[1] * S1 >= 0.f && A1[2] * S1 >= 0.f) {
-                // the neighbour centre lies inside it0: implicit edge
-                const float z1 = A1[0] * P0[0].z + A1[1] * P0[1].z + A1[2] * P0[2].z;
-                const float w1 = A1[0] * P0[0].w + A1[1] * P0[1].w + A1[2] * P0[2].w;
-                if (it1 >= 0 && depth1 < z1 / w1) {  // it1 hides it0 at the neighbour
-                    // a triangle intersection needs it1 behind depth0 at this pixel: never when
-                    // it1's far depth bound lies in front of it
-                    if (h.zhi[n] < depth0 ||
-                        !intersection_pair(P0, tverts, it1, depth0, nx0, ny0, DX, gx, gy, ge_x, ge_y, ge_z))
-                        continue;
-                } else if (!(it1 < 0 || depth0 < depth1)) {
-                    continue;
-                }
-            } else {
-                // the neighbour centre lies outside it0: geometric edge
-                if (!(it1 < 0 || depth0 < depth1)) continue;
-                // exit edge: the first edge function to change sign along p0 -> p1, in the
-                // reference's test order (0,1) = k 2, (1,2) = k 0, (2,0) = k 1
-                float tb = 2.f;
-                int kb = -1;
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    const int k = (j + 2) % 3;
-                    const float s0 = fmaxf(sgn * A[k], 0.f), s1 = sgn * A1[k];
-                    if (s1 <= 0.f && s1 < s0) {
-                        const float t = __fdividef(s0, s0 - s1);
-                        if (t < tb) { tb = t; kb = k; }
-                    }
-                }
-                if (kb < 0) continue;
-                const float ix = nx0 + tb * (2.f * hx), iy = ny0 + tb * (2.f * hy);
-                const float4 Av = kb == 0 ? P0[1] : (kb == 1 ? P0[2] : P0[0]);
-                const float4 Bv = kb == 0 ? P0[2] : (kb == 1 ? P0[0] : P0[1]);
-                const float dx = Bv.x - Av.x, dy = Bv.y - Av.y, dw = Bv.w - Av.w;
-                const float qx = Av.x - ix * Av.w, qy = Av.y - iy * Av.w;
-                const float bx = dx - ix * dw, by = dy - iy * dw;
-                const float den = bx * bx + by * by;
-                const float t = den != 0.f ? -__fdividef(qx * bx + qy * by, den) : 0.5f;
-                const float s0 = 1.f - t, s1 = t;
-                const float cw = s0 * Av.w + s1 * Bv.w;
-                const float iw = __fdividef(1.f, cw);
-                const float cx = s0 * Av.x + s1 * Bv.x, cy = s0 * Av.y + s1 * Bv.y;
-                q = (gx * cx + gy * cy) * iw;
-                // vertices (i0, i1) = (kb + 1, kb + 2) mod 3 carry (s0, s1)
-                const float v0 = s0 * iw, v1 = s1 * iw;
-                u0 = kb == 0 ? 0.f : (kb == 1 ? v1 : v0);
-                u1 = kb == 1 ? 0.f : (kb == 2 ? v1 : v0);
-                u2 = kb == 2 ? 0.f : (kb == 0 ? v1 : v0);
-                at_mid = false;
-            }
+    if (it0 >= 0) {
+        f.depth = h.dep[hidx];
+        f.nx = -1.f + ((float)x0 + 0.5f) * sx;
+        f.ny = -1.f + ((float)y0 + 0.5f) * sy;
+        {
+            const TriVerts v = tverts[it0];
+            f.P[0] = v.p0; f.P[1] = v.p1; f.P[2] = v.p2;
         }
-        if (at_mid) {
-            float Am[3];
-#pragma unroll
-            for (int k = 0; k < 3; ++k) Am[k] = fmaf(ay[k], hy, fmaf(ax[k], hx, A[k]));
-            const float Sm = Am[0] + Am[1] + Am[2];
-            if (!(Sm != 0.f && Am[0] * Sm >= 0.f && Am[1] * Sm >= 0.f && Am[2] * Sm >= 0.f)) continue;
-            // b_k / cw = A_k / sum(A_k w_k);  cz / cw = sum(A_k z_k) / sum(A_k w_k)
-            const float Ws = Am[0] * P0[0].w + Am[1] * P0[1].w + Am[2] * P0[2].w;
-            const float Zs = Am[0] * P0[0].z + Am[1] * P0[1].z + Am[2] * P0[2].z;
-            const float iW = __fdividef(1.f, Ws);
-            u0 = Am[0] * iW; u1 = Am[1] * iW; u2 = Am[2] * iW;
-            q = ge_x * (nx0 + hx) + ge_y * (ny0 + hy) + ge_z * (Zs * iW);
-        }
-        const float uv[3] = {u0, u1, u2};
+        float As;
+        edge_terms(f.ny, f.nx, f.P[0], f.P[1], f.P[2], f.A[0], f.A[1], f.A[2], As);
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            acc.g[k * 4 + 0] += uv[k] * ge_x;
-            acc.g[k * 4 + 1] += uv[k] * ge_y;
-            acc.g[k * 4 + 2] += uv[k] * ge_z;
-            acc.g[k * 4 + 3] -= uv[k] * q;
+            const float4 u = f.P[(k + 1) % 3], v = f.P[(k + 2) % 3];
+            f.ax[k] = u.y * v.w - u.w * v.y;
+            f.ay[k] = u.w * v.x - u.x * v.w;
         }
-        acc.any = true;
+        f.sgn = As > 0.f ? 1.f : -1.f;  // orientation of the inside near the pixel
+        // neighbours (+x, -x, -y, +y) as in rasterize.cu:691-692
+#pragma unroll 1
+        for (int e = 0; e < 4 && As != 0.f; ++e) {
+            const int DX = (e == 0) - (e == 1);
+            const int DY = (e == 3) - (e == 2);
+            const int n = hidx + DX + DY * kHaloW;
+            const int it1 = h.it[n];
+            if (it1 == kOutside) continue;  // no neighbour in the view
+            const bool interior = it1 == it0;
+            if (interior && (DX < 0 || DY < 0)) continue;  // interior pair counted by the neighbour
+            const EdgePair p = edge_pair(h, f, hidx, e, H, W, sx, sy);
+            if (p.gx == 0.f && p.gy == 0.f) continue;  // zero adjoint
+            if (interior) {
+                edge_midpoint(f, p.hx, p.hy, 2.f * p.gx, 2.f * p.gy, 0.f, acc);
+                continue;
+            }
+            const float depth1 = h.dep[n];
+            const float S1 = p.A1[0] + p.A1[1] + p.A1[2];
+            if (S1 != 0.f && p.A1[0] * S1 >= 0.f && p.A1[1] * S1 >= 0.f && p.A1[2] * S1 >= 0.f) {
+                // the neighbour centre lies inside it0: implicit edge
+                const float z1 = p.A1[0] * f.P[0].z + p.A1[1] * f.P[1].z + p.A1[2] * f.P[2].z;
+                const float w1 = p.A1[0] * f.P[0].w + p.A1[1] * f.P[1].w + p.A1[2] * f.P[2].w;
+                if (it1 >= 0 && depth1 < z1 / w1) {
+                    // it1 hides it0 at the neighbour: a triangle intersection, which needs it1
+                    // behind depth0 at this pixel (never when its far depth bound is in front)
+                    if (!(h.zhi[n] < f.depth)) isect |= 1u << e;
+                } else if (it1 < 0 || f.depth < depth1) {  // active opacity edge
+                    edge_midpoint(f, p.hx, p.hy, p.gx, p.gy, 0.f, acc);
+                }
+            } else if (it1 < 0 || f.depth < depth1) {  // active geometric edge
+                geo |= 1u << e;
+            }
+        }
+    }
+    // geometric edges: the exit edge is the first edge function to change sign along p0 -> p1,
+    // in the reference's test order (0,1) = k 2, (1,2) = k 0, (2,0) = k 1
+    const int ngeo = __reduce_max_sync(0xffffffffu, (unsigned)__popc(geo));
+    for (int r = 0; r < ngeo; ++r) {
+        if (geo == 0u) continue;
+        const int e = __ffs(geo) - 1;
+        geo &= geo - 1u;
+        const EdgePair p = edge_pair(h, f, hidx, e, H, W, sx, sy);
+        float tb = 2.f;
+        int kb = -1;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const int k = (j + 2) % 3;
+            const float s0 = fmaxf(f.sgn * f.A[k], 0.f), s1 = f.sgn * p.A1[k];
+            if (s1 <= 0.f && s1 < s0) {
+                const float t = __fdividef(s0, s0 - s1);
+                if (t < tb) { tb = t; kb = k; }
+            }
+        }
+        if (kb < 0) continue;
+        const float ix = f.nx + tb * (2.f * p.hx), iy = f.ny + tb * (2.f * p.hy);
+        const float4 Av = kb == 0 ? f.P[1] : (kb == 1 ? f.P[2] : f.P[0]);
+        const float4 Bv = kb == 0 ? f.P[2] : (kb == 1 ? f.P[0] : f.P[1]);
+        const float dx = Bv.x - Av.x, dy = Bv.y - Av.y, dw = Bv.w - Av.w;
+        const float qx = Av.x - ix * Av.w, qy = Av.y - iy * Av.w;
+        const float bx = dx - ix * dw, by = dy - iy * dw;
+        const float den = bx * bx + by * by;
+        const float t = den != 0.f ? -__fdividef(qx * bx + qy * by, den) : 0.5f;
+        const float s0 = 1.f - t, s1 = t;
+        const float cw = s0 * Av.w + s1 * Bv.w;
+        const float iw = __fdividef(1.f, cw);
+        const float cx = s0 * Av.x + s1 * Bv.x, cy = s0 * Av.y + s1 * Bv.y;
+        // vertices (i0, i1) = (kb + 1, kb + 2) mod 3 carry (s0, s1)
+        const float v0 = s0 * iw, v1 = s1 * iw;
+        edge_accumulate(acc, kb == 0 ? 0.f : (kb == 1 ? v1 : v0), kb == 1 ? 0.f : (kb == 2 ? v1 : v0),
+                        kb == 2 ? 0.f : (kb == 0 ? v1 : v0), p.gx, p.gy, 0.f, (p.gx * cx + p.gy * cy) * iw);
+    }
+    // possible triangle intersections (rasterize.cu:760-809)
+    const int nisect = __reduce_max_sync(0xffffffffu, (unsigned)__popc(isect));
+    for (int r = 0; r < nisect; ++r) {
+        if (isect == 0u) continue;
+        const int e = __ffs(isect) - 1;
+        isect &= isect - 1u;
+        const EdgePair p = edge_pair(h, f, hidx, e, H, W, sx, sy);
+        float ge_x, ge_y, ge_z;
+        if (intersection_pair(f.P, tverts, h.it[p.n], f.depth, f.nx, f.ny, p.DX, p.gx, p.gy, ge_x, ge_y, ge_z))
+            edge_midpoint(f, p.hx, p.hy, ge_x, ge_y, ge_z, acc);
     }
     return it0;
 }

@@ -377,12 +377,10 @@ __global__ void __launch_bounds__(kEdgeThreads, DSB_EDGE_MIN_CTAS) edge_step_ker
     const int ly = threadIdx.x / DS_TILE, lx = threadIdx.x % DS_TILE;
     const int y = ty0 + ly, x = tx0 + lx;
     EdgeAccum acc;
-#pragma unroll
-    for (int k = 0; k < 12; ++k) acc.g[k] = 0.f;
-    acc.any = false;
-    int it0 = -1;
-    if (y < vd.H && x < vd.W)
-        it0 = edge_grad_pixel_staged(h, (ly + 1) * kHaloW + lx + 1, y, x, vd.H, vd.W, tab.verts + (size_t)b * T, acc);
+    // every lane takes part (warp-wide reductions inside); pixels beyond the view are staged as
+    // kOutside and contribute nothing
+    const int it0 = edge_grad_pixel_staged(h, (ly + 1) * kHaloW + lx + 1, y, x, vd.H, vd.W,
+                                           tab.verts + (size_t)b * T, acc);
     const int key = (it0 >= 0 && acc.any) ? it0 : -1 - lane;
     const int prev = __shfl_up_sync(0xffffffffu, key, 1);
     const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || prev != key);
