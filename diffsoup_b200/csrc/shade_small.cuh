@@ -96,13 +96,28 @@ __global__ void __launch_bounds__(kShadeSmallWarps * 32, DSB_SHADE_SMALL_MIN_CTA
 
     ShadeSmallWarp& ws = sm.w[warp];
     const int64_t nchunks = (a.num_pixels + 31) / 32;
-    for (int64_t chunk = (int64_t)blockIdx.x * kShadeSmallWarps + warp; chunk < nchunks;
-         chunk += (int64_t)gridDim.x * kShadeSmallWarps) {
+    const int64_t cstride = (int64_t)gridDim.x * kShadeSmallWarps;
+    // the rast entry of the warp's next chunk is requested one chunk ahead
+    float4 r_next = make_float4(0.f, 0.f, 0.f, 0.f);
+    {
+        const int64_t p0 = ((int64_t)blockIdx.x * kShadeSmallWarps + warp) * 32 + lane;
+        if (p0 < a.num_pixels) r_next = reinterpret_cast<const float4*>(a.rast)[p0];
+    }
+    for (int64_t chunk = (int64_t)blockIdx.x * kShadeSmallWarps + warp; chunk < nchunks; chunk += cstride) {
         // ---------------- pixel front: gather features, view direction ----------
         const int64_t p = chunk * 32 + lane;
         const bool valid = p < a.num_pixels;
-        float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (valid) r = reinterpret_cast<const float4*>(a.rast)[p];
+        const float4 r = r_next;
+        {
+            const int64_t pn = p + cstride * 32;
+            r_next = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (pn < a.num_pixels) r_next = reinterpret_cast<const float4*>(a.rast)[pn];
+        }
+        float tgt[3] = {0.f, 0.f, 0.f};  // requested here, used after the MLP forward
+        if (valid) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) tgt[c] = a.target[p * 3 + c];
+        }
         const int t = (int)r.w - 1;
         const bool mask = valid && t >= 0;
         float x[IN];
@@ -178,7 +193,7 @@ __global__ void __launch_bounds__(kShadeSmallWarps * 32, DSB_SHADE_SMALL_MIN_CTA
             for (int c = 0; c < 3; ++c) {
                 const float s = 1.f / (1.f + expf(-(ws.scr[lane * 17 + c] + bo[c])));
                 const float col = mask ? (1.f - res) * x[c] + res * s : 1.f;
-                const float diff = col - a.target[p * 3 + c];
+                const float diff = col - tgt[c];
                 loss_acc += diff * diff;
                 const float gc = 2.f * diff * a.inv_n;
                 a.color[p * 3 + c] = col;
