@@ -149,3 +149,43 @@ def test_level_accumulation_matches_oracle(config, kw):
     want_gf = cpu.accumulate_backward(lo, hi, hi, sc.T, gf * f * (1 - f))
     assert rel(step.grad_alpha_src.cpu().numpy(), want_ga) < 1e-5
     assert rel(step.grad_feat_src.cpu().numpy(), want_gf) < 1e-5
+
+
+@pytest.mark.parametrize("config", [1, 5])
+def test_train_step_gradients_match_central_differences(config):
+    """The BF16 step's feature and MLP gradients against FP64 central
+    differences (step 1e-4) of the oracle's loss over the step's own ID
+    buffer; relative L2 over the sampled entries within GRAD_TOL (BF16)."""
+    from test_fd_gradients import fd_feature, fd_mlp, fd_scene, feature_entries
+
+    sc, inp, _ = fd_scene(2, config)
+    hw = list(inp.hw)
+    step = TrainStep(sc.T, sc.verts.shape[0], hw, sc.feat_dim, sc.min_level, sc.max_level, sc.hidden_dim,
+                     sc.n_layers, stochastic=True, seed=inp.seed)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(DEV)  # noqa: E731
+    mlp32 = [(W.astype(np.float32), b.astype(np.float32)) for W, b in inp.mlp]
+    rast = torch.empty(step.num_pixels, 4, device=DEV)
+    step.run(verts=t(sc.verts), tri=t(sc.tri), mvp=t(sc.mvps()), inv_mvp=t(sc.inv_mvps()),
+             feat_src=t(sc.feat_src), alpha_src=t(sc.alpha_src[..., 0]), mlp_params=_mlp_flat(mlp32).to(DEV),
+             target=t(np.concatenate([x.reshape(-1, 3) for x in sc.targets])), rast_out=rast)
+    torch.cuda.synchronize()
+    rasts = [rast.cpu().numpy()[step.pix_offsets[b]:step.pix_offsets[b] + h * w].reshape(1, h, w, 4)
+             for b, (h, w) in enumerate(hw)]
+    gf = step.grad_feat_src.cpu().numpy().astype(np.float64)
+    gm = step.grad_mlp.cpu().numpy().astype(np.float64)
+    rng = np.random.default_rng(1)
+    got, want = [], []
+    for idx in feature_entries(gf, 12, rng):
+        got.append(gf[idx])
+        want.append(fd_feature(inp, rasts, idx))
+    assert rel(got, want) <= GRAD_TOL["grad_feat_src"], (got, want)
+    # MLP parameters, packed as [W0, b0, (W, b)..., Wo, bo] like the step's grad_mlp
+    got, want, off = [], [], 0
+    for layer, (W, b) in enumerate(inp.mlp):
+        for which, arr in ((0, W), (1, b)):
+            g = gm[off:off + arr.size].reshape(arr.shape)
+            for idx in feature_entries(g, 4, rng):
+                got.append(g[idx])
+                want.append(fd_mlp(inp, rasts, layer, which, idx))
+            off += arr.size
+    assert rel(got, want) <= GRAD_TOL["mlp"], (got, want)
