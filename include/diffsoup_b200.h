@@ -277,6 +277,34 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
 int ds_encode_view_dir(int B, int H, int W, const float* rast, const float* inv_mvp, float* encoding,
                        ds_stream_t stream);
 
+/* ===================================================================== */
+/*  Optimiser updates                                                     */
+/* ===================================================================== */
+
+/* Adam as torch.optim.Adam computes it (examples/02_synthetic.py:310-315
+ * uses it for features, opacities and the MLP): for the n elements of param,
+ * with t = *step + 1,
+ *   exp_avg    <- exp_avg + (1 - beta1) (grad - exp_avg)
+ *   exp_avg_sq <- beta2 exp_avg_sq + (1 - beta2) grad^2
+ *   param      <- param - lr / (1 - beta1^t) * exp_avg
+ *                         / (sqrt(exp_avg_sq) / sqrt(1 - beta2^t) + eps)
+ * then *step <- t.  step is a device int32 (the state's step count), so the
+ * update captures into a CUDA graph.  The hyperparameters are doubles, as
+ * torch's Python scalars are (1 - beta is formed before rounding to FP32).
+ * Not host-synchronising. */
+int ds_adam_step(float* param, const float* grad, float* exp_avg, float* exp_avg_sq, int64_t n, double lr,
+                 double beta1, double beta2, double eps, int* step, ds_stream_t stream);
+
+/* replaces VectorAdam.step (python/diffsoup/optimize.py:36-68) for one
+ * parameter of `rows` vectors of `dim` components (vertex positions: dim 3):
+ * with t = *step + 1, per row
+ *   g1 <- beta1 g1 + (1 - beta1) grad          g1 [rows, dim]
+ *   g2 <- beta2 g2 + (1 - beta2) |grad|^2      g2 [rows, 1]
+ *   param <- param - lr (g1 / (1 - beta1^t)) / (sqrt(g2 / (1 - beta2^t)) + 1e-8)
+ * then *step <- t (device int32).  Not host-synchronising. */
+int ds_vector_adam_step(float* param, const float* grad, float* g1, float* g2, int64_t rows, int dim, double lr,
+                        double beta1, double beta2, int* step, ds_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
