@@ -11,6 +11,7 @@ from __future__ import annotations
 
 from . import _core
 from . import optimize
+from . import visibility
 from ._core import __version__
 from .rasterize import (
     count_triangle_ids,

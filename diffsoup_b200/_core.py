@@ -59,6 +59,7 @@ _sig("ds_backward_edge_grad", _i32, _i32, _i32, _i32, _i32, _vp, _vp, _vp, _i32,
 _sig("ds_backward_opacity_aux_loss", _i32, _i32, _i32, _i32, _i32, _vp, _vp, _vp, _i32, _vp, _vp, _vp, _vp, _vp)
 _sig("ds_encode_view_dir_sh2", _i32, _i32, _i32, _i32, _vp, _vp, _vp, _vp)
 _sig("ds_encode_view_dir", _i32, _i32, _i32, _i32, _vp, _vp, _vp, _vp)
+_sig("ds_count_triangle_ids", _i32, _i64, _vp, _i32, _vp, _vp, _vp)
 _sig("ds_multires_triangle_alpha", _i32, _i32, _vp, _i32, _i32, _i32, _vp, _vp, _vp)
 _sig("ds_backward_multires_triangle_alpha", _i32, _i32, _vp, _i32, _i32, _i32, _vp, _vp, _vp)
 _sig("ds_multires_triangle_color", _i32, _i32, _i32, _i32, _vp, _i32, _i32, _i32, _i32, _vp, _vp, _vp)

@@ -183,9 +183,15 @@ def encode_view_dir(rast, inv_mvp) -> torch.Tensor:
 # ---------------------------------------------------------------------------
 
 def count_triangle_ids(rast: torch.Tensor, num_tris: int) -> torch.Tensor:
-    """Pixels covered per triangle in a rasterisation buffer: (num_tris,) int64."""
-    ids = rast[..., -1].long()
-    ids = ids[ids > 0] - 1
-    count = torch.bincount(ids, minlength=num_tris)
-    assert count.shape[0] == num_tris
+    """Pixels covered per triangle in a rasterisation buffer: (num_tris,) int64
+    (rasterize.py:348-366; one kernel, ds_count_triangle_ids).  Like the
+    reference's bincount, an ID beyond num_tris fails the assertion; checking
+    it synchronises with the device."""
+    assert rast.is_cuda and rast.dtype == torch.float32 and rast.shape[-1] == 4
+    r = rast.contiguous()
+    count = torch.zeros(num_tris, dtype=torch.int64, device=rast.device)
+    status = torch.zeros(1, dtype=torch.int32, device=rast.device)
+    _core.check(_core.lib.ds_count_triangle_ids(r.numel() // 4, _core.ptr(r), int(num_tris), _core.ptr(count),
+                                                _core.ptr(status), _core.stream()))
+    assert int(status.item()) == 0, "triangle id beyond num_tris"
     return count

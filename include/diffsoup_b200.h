@@ -277,6 +277,15 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
 int ds_encode_view_dir(int B, int H, int W, const float* rast, const float* inv_mvp, float* encoding,
                        ds_stream_t stream);
 
+/* Pixels per triangle of an ID buffer: counts[id] += number of pixels of
+ * rast [num_pixels,4] whose rast[..,3] == id + 1 (count_triangle_ids,
+ * python/diffsoup/rasterize.py:348-366, computed there with torch.bincount).
+ * counts [num_tris] int64 accumulates (the caller zeroes it).  An ID at or
+ * above num_tris is not counted and sets *status |= 1 (status may be NULL);
+ * the reference asserts on that case.  Not host-synchronising. */
+int ds_count_triangle_ids(int64_t num_pixels, const float* rast, int num_tris, int64_t* counts, int* status,
+                          ds_stream_t stream);
+
 /* ===================================================================== */
 /*  Optimiser updates                                                     */
 /* ===================================================================== */
