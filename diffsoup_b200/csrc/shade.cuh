@@ -24,7 +24,12 @@
 
 namespace dsb {
 
-template <int C_, int IN_PAD_, int HID_, int NL_>
+// SPLIT_: every MLP operand is carried as two bf16 planes, hi = bf16(v) and
+// lo = bf16(v - hi) (16 significant bits together), features are gathered from
+// the fp32 copy, and each product is hi*hi + hi*lo + lo*hi on the BF16 tensor
+// cores with fp32 accumulation -- the precision mode whose gradients agree with
+// the FP64 oracle to ~1e-5 (the lo*lo term is below 2^-16 of the product).
+template <int C_, int IN_PAD_, int HID_, int NL_, bool SPLIT_ = false>
 struct ShadeCfg {
     static constexpr int C = C_;             // feature channels
     static constexpr int IN_REAL = C_ + 3;   // features + view direction
@@ -36,7 +41,10 @@ struct ShadeCfg {
     static constexpr int LDH = HID + 8;
     static constexpr int LDO = 16 + 8;
     static constexpr int LDS = (IN_PAD > 16 ? IN_PAD : 16) + 1;  // fp32 scratch stride
-    static constexpr int WARPS = 4;
+    static constexpr bool SPLIT = SPLIT_;
+    static constexpr int NS = SPLIT_ ? 2 : 1;  // bf16 planes per operand
+    // warps per CTA: the split planes of the large MLP need twice the shared memory
+    static constexpr int WARPS = (SPLIT_ && HID_ > 32) ? 2 : 4;
     static constexpr int NH = NL > 1 ? NL - 1 : 1;  // hidden-to-hidden matrices (at least 1 slot)
     // packed fp32 parameter offsets: W0[HID][IN_REAL] b0[HID] (Wl[HID][HID] bl[HID])* Wo[3][HID] bo[3]
     static constexpr int P_W0 = 0;
@@ -55,20 +63,21 @@ struct ShadeCfg {
 
 // Every ldmatrix row address must be 16-byte aligned: all tiles start on
 // 16-byte boundaries and their row strides are multiples of 8 bf16.
+// [plane][...]: plane 0 holds bf16(v), plane 1 (SPLIT only) bf16(v - plane 0).
 template <class K>
 struct __align__(16) ShadeWarpSmem {
-    __align__(16) __nv_bfloat16 X[32 * K::LDX];
-    __align__(16) __nv_bfloat16 H[K::NL][32 * K::LDH];
-    __align__(16) __nv_bfloat16 DZO[32 * K::LDO];
-    __align__(16) __nv_bfloat16 DH[2][32 * K::LDH];
+    __align__(16) __nv_bfloat16 X[K::NS][32 * K::LDX];
+    __align__(16) __nv_bfloat16 H[K::NL][K::NS][32 * K::LDH];
+    __align__(16) __nv_bfloat16 DZO[K::NS][32 * K::LDO];
+    __align__(16) __nv_bfloat16 DH[2][K::NS][32 * K::LDH];
     __align__(16) float scr[32 * K::LDS];
 };
 
 template <class K>
 struct __align__(16) ShadeSmem {
-    __align__(16) __nv_bfloat16 W0[K::HID * K::LDX];
-    __align__(16) __nv_bfloat16 WH[K::NH][K::HID * K::LDH];
-    __align__(16) __nv_bfloat16 WO[16 * K::LDH];
+    __align__(16) __nv_bfloat16 W0[K::NS][K::HID * K::LDX];
+    __align__(16) __nv_bfloat16 WH[K::NH][K::NS][K::HID * K::LDH];
+    __align__(16) __nv_bfloat16 WO[K::NS][16 * K::LDH];
     float b0[K::HID];
     float bh[K::NH][K::HID];
     float bo[4];
@@ -84,6 +93,7 @@ struct ShadeArgs {
     int64_t num_pixels;
     const float* rast;            // [P,4]
     const __nv_bfloat16* feat;    // [T,S,C] sigmoid features, bf16
+    const float* feat_f32;        // [T,S,C] the same in fp32 (read by the SPLIT kernels)
     int level, S;
     const float* inv_mvp;         // [B,16]
     const float* target;          // [P,3]
@@ -106,6 +116,38 @@ __device__ __forceinline__ int view_of_pixel(const ds_view_desc* __restrict__ vi
     return lo;
 }
 
+// bf16 planes of two values: hi = bf16(v), lo = bf16(v - hi).
+__device__ __forceinline__ void split_bf16(float v0, float v1, uint32_t& hi, uint32_t& lo) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(v0, v1);
+    const float2 hf = __bfloat1622float2(h);
+    const __nv_bfloat162 l = __floats2bfloat162_rn(v0 - hf.x, v1 - hf.y);
+    hi = *reinterpret_cast<const uint32_t*>(&h);
+    lo = *reinterpret_cast<const uint32_t*>(&l);
+}
+
+// Stores (v0, v1) at element `off` of an operand tile's planes.
+template <class K, class Tile>
+__device__ __forceinline__ void put2(Tile& t, int off, float v0, float v1) {
+    if (K::SPLIT) {
+        uint32_t hi, lo;
+        split_bf16(v0, v1, hi, lo);
+        *reinterpret_cast<uint32_t*>(&t[0][off]) = hi;
+        *reinterpret_cast<uint32_t*>(&t[K::NS - 1][off]) = lo;
+    } else {
+        *reinterpret_cast<uint32_t*>(&t[0][off]) = pack_bf16(v0, v1);
+    }
+}
+
+// acc += A B over the planes: hi*hi (+ hi*lo + lo*hi with SPLIT).
+template <class K>
+__device__ __forceinline__ void mma_planes(float acc[4], const uint32_t a[K::NS][4], const uint32_t b[K::NS][2]) {
+    mma_16816(acc, a[0], b[0]);
+    if (K::SPLIT) {
+        mma_16816(acc, a[0], b[K::NS - 1]);
+        mma_16816(acc, a[K::NS - 1], b[0]);
+    }
+}
+
 // Relu mask of an activation element stored as bf16 in smem.
 __device__ __forceinline__ float2 relu_gate(const __nv_bfloat16* h, float2 v) {
     const __nv_bfloat162 hv = *reinterpret_cast<const __nv_bfloat162*>(h);
@@ -124,19 +166,28 @@ __global__ void __launch_bounds__(K::WARPS * 32, K::REG_GRADS ? DSB_SHADE_MIN_CT
     const int g = lane >> 2, q = lane & 3;
     constexpr int HID = K::HID, IN_PAD = K::IN_PAD;
 
-    // ---- weights to shared memory (bf16, zero padded), biases fp32 --------
+    // ---- weights to shared memory (bf16 planes, zero padded), biases fp32 ---
     for (int i = threadIdx.x; i < HID * K::LDX; i += blockDim.x) {
         const int r = i / K::LDX, c = i % K::LDX;
-        sm.W0[i] = __float2bfloat16_rn(c < K::IN_REAL ? a.params[K::P_W0 + r * K::IN_REAL + c] : 0.f);
+        const float v = c < K::IN_REAL ? a.params[K::P_W0 + r * K::IN_REAL + c] : 0.f;
+        const __nv_bfloat16 h = __float2bfloat16_rn(v);
+        sm.W0[0][i] = h;
+        if (K::SPLIT) sm.W0[K::NS - 1][i] = __float2bfloat16_rn(v - __bfloat162float(h));
     }
     for (int l = 0; l < K::NL - 1; ++l)
         for (int i = threadIdx.x; i < HID * K::LDH; i += blockDim.x) {
             const int r = i / K::LDH, c = i % K::LDH;
-            sm.WH[l][i] = __float2bfloat16_rn(c < HID ? a.params[K::P_WH + l * (HID * HID + HID) + r * HID + c] : 0.f);
+            const float v = c < HID ? a.params[K::P_WH + l * (HID * HID + HID) + r * HID + c] : 0.f;
+            const __nv_bfloat16 h = __float2bfloat16_rn(v);
+            sm.WH[l][0][i] = h;
+            if (K::SPLIT) sm.WH[l][K::NS - 1][i] = __float2bfloat16_rn(v - __bfloat162float(h));
         }
     for (int i = threadIdx.x; i < 16 * K::LDH; i += blockDim.x) {
         const int r = i / K::LDH, c = i % K::LDH;
-        sm.WO[i] = __float2bfloat16_rn(r < K::OUT && c < HID ? a.params[K::P_WO + r * HID + c] : 0.f);
+        const float v = r < K::OUT && c < HID ? a.params[K::P_WO + r * HID + c] : 0.f;
+        const __nv_bfloat16 h = __float2bfloat16_rn(v);
+        sm.WO[0][i] = h;
+        if (K::SPLIT) sm.WO[K::NS - 1][i] = __float2bfloat16_rn(v - __bfloat162float(h));
     }
     for (int i = threadIdx.x; i < HID; i += blockDim.x) {
         sm.b0[i] = a.params[K::P_B0 + i];
@@ -182,8 +233,21 @@ __global__ void __launch_bounds__(K::WARPS * 32, K::REG_GRADS ? DSB_SHADE_MIN_CT
         if (mask) {
             lattice_cell(r.x, r.y, (uint32_t)a.level, idx, wgt);
             const __nv_bfloat16* tf = a.feat + (size_t)t * a.S * K::C;
+            const float* tf32 = a.feat_f32 + (size_t)t * a.S * K::C;
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
+                if (K::SPLIT) {  // fp32 features
+                    const float* fv = tf32 + (size_t)idx[k] * K::C;
+#pragma unroll
+                    for (int c = 0; c < K::C; c += 4) {
+                        const float4 u = __ldg(reinterpret_cast<const float4*>(fv + c));
+                        x[c] = __fmaf_rn(wgt[k], u.x, x[c]);
+                        x[c + 1] = __fmaf_rn(wgt[k], u.y, x[c + 1]);
+                        x[c + 2] = __fmaf_rn(wgt[k], u.z, x[c + 2]);
+                        x[c + 3] = __fmaf_rn(wgt[k], u.w, x[c + 3]);
+                    }
+                    continue;
+                }
                 const __nv_bfloat16* fv = tf + (size_t)idx[k] * K::C;
 #pragma unroll
                 for (int c = 0; c < K::C; c += 8) {
@@ -211,18 +275,20 @@ __global__ void __launch_bounds__(K::WARPS * 32, K::REG_GRADS ? DSB_SHADE_MIN_CT
         {
             // 16-byte stores: rows are 16-byte aligned and, at these strides,
             // the 8 lanes of each store phase hit distinct bank groups
-            __nv_bfloat16* xr = ws.X + lane * K::LDX;
 #pragma unroll
             for (int c = 0; c < IN_PAD; c += 8) {
-                uint32_t u[4];
+                uint32_t u[4], ul[4];
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     const int c0 = c + 2 * j, c1 = c + 2 * j + 1;
                     const float v0 = c0 < K::IN_REAL ? x[c0 < K::IN_REAL ? c0 : 0] : 0.f;
                     const float v1 = c1 < K::IN_REAL ? x[c1 < K::IN_REAL ? c1 : 0] : 0.f;
-                    u[j] = pack_bf16(v0, v1);
+                    if (K::SPLIT) split_bf16(v0, v1, u[j], ul[j]);
+                    else u[j] = pack_bf16(v0, v1);
                 }
-                *reinterpret_cast<uint4*>(xr + c) = make_uint4(u[0], u[1], u[2], u[3]);
+                *reinterpret_cast<uint4*>(ws.X[0] + lane * K::LDX + c) = make_uint4(u[0], u[1], u[2], u[3]);
+                if (K::SPLIT)
+                    *reinterpret_cast<uint4*>(ws.X[K::NS - 1] + lane * K::LDX + c) = make_uint4(ul[0], ul[1], ul[2], ul[3]);
             }
         }
         __syncwarp();
@@ -235,18 +301,18 @@ __global__ void __launch_bounds__(K::WARPS * 32, K::REG_GRADS ? DSB_SHADE_MIN_CT
                 float acc[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
                 for (int kt = 0; kt < IN_PAD / 16; ++kt) {
-                    uint32_t af[4], bf[2];
-                    load_a(af, ws.X, K::LDX, mt * 16, kt * 16);
-                    load_b(bf, sm.W0, K::LDX, nt * 8, kt * 16);
-                    mma_16816(acc, af, bf);
+                    uint32_t af[K::NS][4], bf[K::NS][2];
+#pragma unroll
+                    for (int s = 0; s < K::NS; ++s) {
+                        load_a(af[s], ws.X[s], K::LDX, mt * 16, kt * 16);
+                        load_b(bf[s], sm.W0[s], K::LDX, nt * 8, kt * 16);
+                    }
+                    mma_planes<K>(acc, af, bf);
                 }
                 const int col = nt * 8 + 2 * q;
                 const float b0v = sm.b0[col], b1v = sm.b0[col + 1];
-                __nv_bfloat16* h = ws.H[0];
-                *reinterpret_cast<uint32_t*>(h + (mt * 16 + g) * K::LDH + col) =
-                    pack_bf16(fmaxf(acc[0] + b0v, 0.f), fmaxf(acc[1] + b1v, 0.f));
-                *reinterpret_cast<uint32_t*>(h + (mt * 16 + g + 8) * K::LDH + col) =
-                    pack_bf16(fmaxf(acc[2] + b0v, 0.f), fmaxf(acc[3] + b1v, 0.f));
+                put2<K>(ws.H[0], (mt * 16 + g) * K::LDH + col, fmaxf(acc[0] + b0v, 0.f), fmaxf(acc[1] + b1v, 0.f));
+                put2<K>(ws.H[0], (mt * 16 + g + 8) * K::LDH + col, fmaxf(acc[2] + b0v, 0.f), fmaxf(acc[3] + b1v, 0.f));
             }
         }
         __syncwarp();
@@ -259,18 +325,19 @@ __global__ void __launch_bounds__(K::WARPS * 32, K::REG_GRADS ? DSB_SHADE_MIN_CT
                     float acc[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
                     for (int kt = 0; kt < HID / 16; ++kt) {
-                        uint32_t af[4], bf[2];
-                        load_a(af, ws.H[l - 1], K::LDH, mt * 16, kt * 16);
-                        load_b(bf, sm.WH[l - 1], K::LDH, nt * 8, kt * 16);
-                        mma_16816(acc, af, bf);
+                        uint32_t af[K::NS][4], bf[K::NS][2];
+#pragma unroll
+                        for (int s = 0; s < K::NS; ++s) {
+                            load_a(af[s], ws.H[l - 1][s], K::LDH, mt * 16, kt * 16);
+                            load_b(bf[s], sm.WH[l - 1][s], K::LDH, nt * 8, kt * 16);
+                        }
+                        mma_planes<K>(acc, af, bf);
                     }
                     const int col = nt * 8 + 2 * q;
                     const float b0v = sm.bh[l - 1][col], b1v = sm.bh[l - 1][col + 1];
-                    __nv_bfloat16* h = ws.H[l];
-                    *reinterpret_cast<uint32_t*>(h + (mt * 16 + g) * K::LDH + col) =
-                        pack_bf16(fmaxf(acc[0] + b0v, 0.f), fmaxf(acc[1] + b1v, 0.f));
-                    *reinterpret_cast<uint32_t*>(h + (mt * 16 + g + 8) * K::LDH + col) =
-                        pack_bf16(fmaxf(acc[2] + b0v, 0.f), fmaxf(acc[3] + b1v, 0.f));
+                    put2<K>(ws.H[l], (mt * 16 + g) * K::LDH + col, fmaxf(acc[0] + b0v, 0.f), fmaxf(acc[1] + b1v, 0.f));
+                    put2<K>(ws.H[l], (mt * 16 + g + 8) * K::LDH + col, fmaxf(acc[2] + b0v, 0.f),
+                            fmaxf(acc[3] + b1v, 0.f));
                 }
             }
             __syncwarp();
@@ -280,10 +347,13 @@ __global__ void __launch_bounds__(K::WARPS * 32, K::REG_GRADS ? DSB_SHADE_MIN_CT
             float acc[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
             for (int kt = 0; kt < HID / 16; ++kt) {
-                uint32_t af[4], bf[2];
-                load_a(af, ws.H[K::NL - 1], K::LDH, mt * 16, kt * 16);
-                load_b(bf, sm.WO, K::LDH, 0, kt * 16);
-                mma_16816(acc, af, bf);
+                uint32_t af[K::NS][4], bf[K::NS][2];
+#pragma unroll
+                for (int s = 0; s < K::NS; ++s) {
+                    load_a(af[s], ws.H[K::NL - 1][s], K::LDH, mt * 16, kt * 16);
+                    load_b(bf[s], sm.WO[s], K::LDH, 0, kt * 16);
+                }
+                mma_planes<K>(acc, af, bf);
             }
             if (q < 2) {
                 const int col = 2 * q;
@@ -321,9 +391,14 @@ __global__ void __launch_bounds__(K::WARPS * 32, K::REG_GRADS ? DSB_SHADE_MIN_CT
             }
             a.l1[p] = l1;
         }
-        {
-            __nv_bfloat16* dr = ws.DZO + lane * K::LDO;
-            *reinterpret_cast<uint4*>(dr) = make_uint4(pack_bf16(dz[0], dz[1]), pack_bf16(dz[2], 0.f), 0u, 0u);
+#pragma unroll
+        for (int s = 0; s < K::NS; ++s) {
+            uint32_t h01, l01, h2, l2;
+            split_bf16(dz[0], dz[1], h01, l01);
+            split_bf16(dz[2], 0.f, h2, l2);
+            if (!K::SPLIT) { h01 = pack_bf16(dz[0], dz[1]); h2 = pack_bf16(dz[2], 0.f); }
+            __nv_bfloat16* dr = ws.DZO[s] + lane * K::LDO;
+            *reinterpret_cast<uint4*>(dr) = s == 0 ? make_uint4(h01, h2, 0u, 0u) : make_uint4(l01, l2, 0u, 0u);
             *reinterpret_cast<uint4*>(dr + 8) = make_uint4(0u, 0u, 0u, 0u);
         }
         // output-layer bias gradient: column sums of dz over the warp
@@ -349,10 +424,13 @@ __global__ void __launch_bounds__(K::WARPS * 32, K::REG_GRADS ? DSB_SHADE_MIN_CT
             float* d = K::REG_GRADS ? gwo[nt < GWO ? nt : 0] : acc;
 #pragma unroll
             for (int kt = 0; kt < 2; ++kt) {
-                uint32_t af[4], bf[2];
-                load_a_t(af, ws.DZO, K::LDO, kt * 16, 0);
-                load_b_t(bf, ws.H[K::NL - 1], K::LDH, kt * 16, nt * 8);
-                mma_16816(d, af, bf);
+                uint32_t af[K::NS][4], bf[K::NS][2];
+#pragma unroll
+                for (int s = 0; s < K::NS; ++s) {
+                    load_a_t(af[s], ws.DZO[s], K::LDO, kt * 16, 0);
+                    load_b_t(bf[s], ws.H[K::NL - 1][s], K::LDH, kt * 16, nt * 8);
+                }
+                mma_planes<K>(d, af, bf);
             }
             if (!K::REG_GRADS && g < K::OUT) {
                 atomicAdd(&sm.g[K::P_WO + g * HID + nt * 8 + 2 * q], acc[0]);
@@ -366,16 +444,19 @@ __global__ void __launch_bounds__(K::WARPS * 32, K::REG_GRADS ? DSB_SHADE_MIN_CT
 #pragma unroll
             for (int nt = 0; nt < HID / 8; ++nt) {
                 float acc[4] = {0.f, 0.f, 0.f, 0.f};
-                uint32_t af[4], bf[2];
-                load_a(af, ws.DZO, K::LDO, mt * 16, 0);
-                load_b_t(bf, sm.WO, K::LDH, 0, nt * 8);
-                mma_16816(acc, af, bf);
+                uint32_t af[K::NS][4], bf[K::NS][2];
+#pragma unroll
+                for (int s = 0; s < K::NS; ++s) {
+                    load_a(af[s], ws.DZO[s], K::LDO, mt * 16, 0);
+                    load_b_t(bf[s], sm.WO[s], K::LDH, 0, nt * 8);
+                }
+                mma_planes<K>(acc, af, bf);
                 const int col = nt * 8 + 2 * q;
-                const __nv_bfloat16* h = ws.H[K::NL - 1];
+                const __nv_bfloat16* h = ws.H[K::NL - 1][0];
                 const float2 lo = relu_gate(h + (mt * 16 + g) * K::LDH + col, make_float2(acc[0], acc[1]));
                 const float2 hi = relu_gate(h + (mt * 16 + g + 8) * K::LDH + col, make_float2(acc[2], acc[3]));
-                *reinterpret_cast<uint32_t*>(ws.DH[cur] + (mt * 16 + g) * K::LDH + col) = pack_bf16(lo.x, lo.y);
-                *reinterpret_cast<uint32_t*>(ws.DH[cur] + (mt * 16 + g + 8) * K::LDH + col) = pack_bf16(hi.x, hi.y);
+                put2<K>(ws.DH[cur], (mt * 16 + g) * K::LDH + col, lo.x, lo.y);
+                put2<K>(ws.DH[cur], (mt * 16 + g + 8) * K::LDH + col, hi.x, hi.y);
                 const int pb = K::NL == 1 ? K::P_B0 : K::P_WH + (K::NL - 2) * (HID * HID + HID) + HID * HID;
                 float s0 = lo.x + hi.x, s1 = lo.y + hi.y;
                 if (K::REG_GRADS) {
@@ -398,10 +479,15 @@ __global__ void __launch_bounds__(K::WARPS * 32, K::REG_GRADS ? DSB_SHADE_MIN_CT
         // hidden layers, last to first
 #pragma unroll
         for (int l = K::NL - 1; l >= 0; --l) {
-            const __nv_bfloat16* ain = l == 0 ? ws.X : ws.H[l > 0 ? l - 1 : 0];
+            const __nv_bfloat16* ain[K::NS];
+            const __nv_bfloat16* wl[K::NS];
+#pragma unroll
+            for (int s = 0; s < K::NS; ++s) {
+                ain[s] = l == 0 ? ws.X[s] : ws.H[l > 0 ? l - 1 : 0][s];
+                wl[s] = l == 0 ? sm.W0[s] : sm.WH[l > 0 ? l - 1 : 0][s];
+            }
             const int ldin = l == 0 ? K::LDX : K::LDH;
             const int nin = l == 0 ? IN_PAD : HID;
-            const __nv_bfloat16* wl = l == 0 ? sm.W0 : sm.WH[l > 0 ? l - 1 : 0];
             const int ldw = l == 0 ? K::LDX : K::LDH;
             const int pw = l == 0 ? K::P_W0 : K::P_WH + (l - 1) * (HID * HID + HID);
             const int win = l == 0 ? K::IN_REAL : HID;  // row length of the packed W_l
@@ -414,10 +500,13 @@ __global__ void __launch_bounds__(K::WARPS * 32, K::REG_GRADS ? DSB_SHADE_MIN_CT
                     float* d = K::REG_GRADS ? gw0[mh < GW0M ? mh : 0][ni < GW0N ? ni : 0] : acc;
 #pragma unroll
                     for (int kt = 0; kt < 2; ++kt) {
-                        uint32_t af[4], bf[2];
-                        load_a_t(af, ws.DH[cur], K::LDH, kt * 16, mh * 16);
-                        load_b_t(bf, ain, ldin, kt * 16, ni * 8);
-                        mma_16816(d, af, bf);
+                        uint32_t af[K::NS][4], bf[K::NS][2];
+#pragma unroll
+                        for (int s = 0; s < K::NS; ++s) {
+                            load_a_t(af[s], ws.DH[cur][s], K::LDH, kt * 16, mh * 16);
+                            load_b_t(bf[s], ain[s], ldin, kt * 16, ni * 8);
+                        }
+                        mma_planes<K>(d, af, bf);
                     }
                     if (K::REG_GRADS) continue;
                     const int i0 = ni * 8 + 2 * q;
@@ -440,10 +529,13 @@ __global__ void __launch_bounds__(K::WARPS * 32, K::REG_GRADS ? DSB_SHADE_MIN_CT
                     float acc[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
                     for (int kt = 0; kt < HID / 16; ++kt) {
-                        uint32_t af[4], bf[2];
-                        load_a(af, ws.DH[cur], K::LDH, mt * 16, kt * 16);
-                        load_b_t(bf, wl, ldw, kt * 16, ni * 8);
-                        mma_16816(acc, af, bf);
+                        uint32_t af[K::NS][4], bf[K::NS][2];
+#pragma unroll
+                        for (int s = 0; s < K::NS; ++s) {
+                            load_a(af[s], ws.DH[cur][s], K::LDH, mt * 16, kt * 16);
+                            load_b_t(bf[s], wl[s], ldw, kt * 16, ni * 8);
+                        }
+                        mma_planes<K>(acc, af, bf);
                     }
                     const int col = ni * 8 + 2 * q;
                     if (l == 0) {
@@ -452,11 +544,11 @@ __global__ void __launch_bounds__(K::WARPS * 32, K::REG_GRADS ? DSB_SHADE_MIN_CT
                         ws.scr[(mt * 16 + g + 8) * K::LDS + col] = acc[2];
                         ws.scr[(mt * 16 + g + 8) * K::LDS + col + 1] = acc[3];
                     } else {
-                        const __nv_bfloat16* h = ws.H[l > 0 ? l - 1 : 0];
+                        const __nv_bfloat16* h = ws.H[l > 0 ? l - 1 : 0][0];
                         const float2 lo = relu_gate(h + (mt * 16 + g) * K::LDH + col, make_float2(acc[0], acc[1]));
                         const float2 hi = relu_gate(h + (mt * 16 + g + 8) * K::LDH + col, make_float2(acc[2], acc[3]));
-                        *reinterpret_cast<uint32_t*>(ws.DH[cur ^ 1] + (mt * 16 + g) * K::LDH + col) = pack_bf16(lo.x, lo.y);
-                        *reinterpret_cast<uint32_t*>(ws.DH[cur ^ 1] + (mt * 16 + g + 8) * K::LDH + col) = pack_bf16(hi.x, hi.y);
+                        put2<K>(ws.DH[cur ^ 1], (mt * 16 + g) * K::LDH + col, lo.x, lo.y);
+                        put2<K>(ws.DH[cur ^ 1], (mt * 16 + g + 8) * K::LDH + col, hi.x, hi.y);
                         const int pb = l - 1 == 0 ? K::P_B0 : K::P_WH + (l - 2) * (HID * HID + HID) + HID * HID;
                         float s0 = lo.x + hi.x, s1 = lo.y + hi.y;
 #pragma unroll

@@ -582,6 +582,8 @@ using namespace dsb;
 
 using ShadeC8H16 = ShadeCfg<8, 16, 16, 1>;    // configs 1-3: 8 features + 3 view dir -> 16 -> 3
 using ShadeC16H64 = ShadeCfg<16, 32, 64, 2>;  // configs 4-5: 16 + 3 -> 64 -> 64 -> 3
+using ShadeC8H16Split = ShadeCfg<8, 16, 16, 1, true>;    // the same MLPs in split BF16
+using ShadeC16H64Split = ShadeCfg<16, 32, 64, 2, true>;
 
 extern "C" {
 
@@ -627,6 +629,7 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     DS_CHECK_ARG(c.B > 0 && c.T >= 0 && c.V >= 0 && num_tiles > 0 && num_pixels > 0, "train_step: bad sizes");
     DS_CHECK_ARG(c.min_level >= 0 && c.max_level >= c.min_level && c.max_level <= 8, "train_step: bad levels");
     DS_CHECK_ARG(c.stochastic == 0 || rng != nullptr, "train_step: stochastic opacity needs the rng state");
+    DS_CHECK_ARG(c.precision == 0 || c.precision == 1, "train_step: precision must be 0 (bf16) or 1 (split bf16)");
     const bool k8 = shade_dispatch_check<ShadeC8H16>(c), k16 = shade_dispatch_check<ShadeC16H64>(c);
     DS_CHECK_ARG(k8 || k16, "train_step: unsupported MLP (C=%d hidden=%d layers=%d); built: 8/16/1, 16/64/2", c.C,
                  c.hidden, c.n_layers);
@@ -692,11 +695,15 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     // fused shading forward + backward
     ShadeArgs a;
     a.B = c.B; a.views = views; a.num_pixels = num_pixels; a.rast = rast; a.feat = w.feat_bf16;
+    a.feat_f32 = w.feat_acc;
     a.level = c.max_level; a.S = ST; a.inv_mvp = inv_mvp; a.target = target; a.params = mlp_params;
     a.inv_n = (float)(1.0 / ((double)num_pixels * 3.0));
     a.color = color_out ? color_out : w.color; a.grad_color = w.grad_color; a.l1 = w.l1;
     a.grad_feat = w.grad_feat_acc; a.grad_params = grad_mlp_params; a.loss_sum = w.loss_sum;
-    rc = k8 ? launch_shade_small(a, st) : launch_shade<ShadeC16H64>(a, st);
+    if (c.precision == 1)
+        rc = k8 ? launch_shade<ShadeC8H16Split>(a, st) : launch_shade<ShadeC16H64Split>(a, st);
+    else
+        rc = k8 ? launch_shade_small(a, st) : launch_shade<ShadeC16H64>(a, st);
     if (rc || (rc = mark(4, st))) return rc;
 
     // opacity auxiliary gradient (scaled by 1/numel(colour), rasterize.py:183-195), on the side

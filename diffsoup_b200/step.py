@@ -34,7 +34,8 @@ from . import tiles as _tiles
 class StepConfig(C.Structure):
     _fields_ = [("B", C.c_int32), ("T", C.c_int32), ("V", C.c_int32), ("C", C.c_int32), ("min_level", C.c_int32),
                 ("max_level", C.c_int32), ("hidden", C.c_int32), ("n_layers", C.c_int32),
-                ("stochastic", C.c_int32), ("thr_const", C.c_float), ("frag_records", C.c_float)]
+                ("stochastic", C.c_int32), ("thr_const", C.c_float), ("frag_records", C.c_float),
+                ("precision", C.c_int32)]
 
 
 _L = _core.lib
@@ -84,14 +85,18 @@ class TrainStep:
     def __init__(self, T: int, V: int, hw: Sequence[Tuple[int, int]], C_: int, min_level: int, max_level: int,
                  hidden: int, n_layers: int, stochastic: bool = True, seed: int = 0,
                  device: Optional[torch.device] = None, list_capacity: Optional[int] = None,
-                 frag_records: float = 2.0):
+                 frag_records: float = 2.0, precision: str = "bf16"):
         self.device = torch.device(device or "cuda")
         self.hw = [(int(h), int(w)) for h, w in hw]
         self.B = len(self.hw)
         # frag_records: fragment records per pixel kept by the rasterizer for the
         # opacity auxiliary gradient (0: that pass re-enumerates the tiles)
+        # precision: "bf16" (BF16 operands) or "split" (every MLP operand as bf16 hi + lo, three
+        # tensor-core products each; gradients within ~1e-5 of FP64)
+        if precision not in ("bf16", "split"):
+            raise ValueError(f"precision must be 'bf16' or 'split', not {precision!r}")
         self.cfg = StepConfig(self.B, T, V, C_, min_level, max_level, hidden, n_layers, int(stochastic), 0.5,
-                              float(frag_records))
+                              float(frag_records), 1 if precision == "split" else 0)
         self.views, self.num_tiles, self.num_pixels, self.pix_offsets = _tiles.view_table(self.hw, self.device)
         self.S = sum(_core.feats_at_level(l) for l in range(min_level, max_level + 1))
         self.nparam = mlp_param_count(C_, hidden, n_layers)

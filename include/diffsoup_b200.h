@@ -233,6 +233,12 @@ typedef struct {
      * result, status bit DS_STATUS_RECORD_FALLBACK).  0 re-enumerates every
      * block.  2 covers the benchmark scenes. */
     float frag_records;
+    /* Shading precision.  0: features gathered as BF16, MLP operands BF16
+     * (one mma per product).  1: split BF16 -- fp32 features, every MLP
+     * operand as bf16 hi + bf16 lo and each product hi*hi + hi*lo + lo*hi on
+     * the BF16 tensor cores (FP32 accumulation), gradients within ~1e-5 of
+     * FP64 instead of the ~5e-3 that BF16 inputs alone cause. */
+    int32_t precision;
 } ds_step_config;
 
 /* Packed MLP parameter layout (fp32): W0[hidden][C+3] b0[hidden]

@@ -31,7 +31,7 @@ def _mlp_flat(mlp):
     return torch.from_numpy(np.concatenate([np.concatenate([W.reshape(-1), b]) for W, b in mlp])).float()
 
 
-def _setup(config, seed, **kw):
+def _setup(config, seed, precision="bf16", **kw):
     sc = scenes.make_scene(config, seed=seed, **kw)
     hw = [(v.height, v.width) for v in sc.views]
     # per-view projection (views may have different aspect ratios)
@@ -40,7 +40,7 @@ def _setup(config, seed, **kw):
                        feat_src=sc.feat_src, alpha_src=sc.alpha_src[..., 0], mlp=mlp, targets=sc.targets,
                        min_level=sc.min_level, max_level=sc.max_level, stochastic=True, seed=4242, iteration=0)
     step = TrainStep(sc.T, sc.verts.shape[0], hw, sc.feat_dim, sc.min_level, sc.max_level, sc.hidden_dim,
-                     sc.n_layers, stochastic=True, seed=4242)
+                     sc.n_layers, stochastic=True, seed=4242, precision=precision)
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(DEV)  # noqa: E731
     dev_inputs = dict(verts=t(sc.verts), tri=t(sc.tri), mvp=t(sc.mvps()), inv_mvp=t(sc.inv_mvps()),
                       feat_src=t(sc.feat_src), alpha_src=t(sc.alpha_src[..., 0]), mlp_params=_mlp_flat(mlp).to(DEV),
@@ -48,14 +48,21 @@ def _setup(config, seed, **kw):
     return sc, hw, inp, step, dev_inputs
 
 
-@pytest.mark.parametrize("config,seed,kw", [
+STEP_CASES = [
     (1, 0, dict(num_tris=1500, num_views=2, resolution=(96, 128))),
     (2, 1, dict(num_tris=3000, num_views=3, resolution=(160, 160))),
     (3, 2, dict(num_tris=2000, num_views=3)),
     (4, 3, dict(num_tris=800, num_views=2, resolution=(80, 96))),
-])
-def test_train_step_matches_fp64_oracle(config, seed, kw):
-    sc, hw, inp, step, d = _setup(config, seed, **kw)
+]
+# precision "split": every MLP operand as bf16 hi + lo -- the image and every
+# gradient group within 1e-3 of the FP64 oracle
+SPLIT_TOL = {"grad_verts": 1e-3, "grad_feat_src": 1e-3, "grad_alpha_src": 1e-3, "mlp": 1e-3}
+
+
+@pytest.mark.parametrize("precision", ["bf16", "split"])
+@pytest.mark.parametrize("config,seed,kw", STEP_CASES)
+def test_train_step_matches_fp64_oracle(config, seed, kw, precision):
+    sc, hw, inp, step, d = _setup(config, seed, precision, **kw)
     rast = torch.empty(step.num_pixels, 4, device=DEV)
     color = torch.empty(step.num_pixels, 3, device=DEV)
     loss = step.run(**d, rast_out=rast, color_out=color)
@@ -89,10 +96,10 @@ def test_train_step_matches_fp64_oracle(config, seed, kw):
         "grad_alpha_src": rel(step.grad_alpha_src.cpu().numpy(), ref.grad_alpha_src),
         "mlp": rel(step.grad_mlp.cpu().numpy(), np.concatenate([np.concatenate([W.reshape(-1), b]) for W, b in ref.grad_mlp])),
     }
-    print(f"config{config} errors vs FP64 oracle: " + ", ".join(f"{k}={v:.2e}" for k, v in errs.items()))
+    print(f"config{config} {precision} errors vs FP64 oracle: " + ", ".join(f"{k}={v:.2e}" for k, v in errs.items()))
     assert errs["image_rms"] <= 1e-3
     assert errs["loss"] <= 1e-3
-    for k, tol in GRAD_TOL.items():
+    for k, tol in (SPLIT_TOL if precision == "split" else GRAD_TOL).items():
         assert errs[k] <= tol, (k, errs[k])
 
 
