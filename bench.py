@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-split", dest="split", action="store_false",
+                    help="skip timing the split-BF16 precision mode beside the BF16 step")
     ap.add_argument("--views", type=int, default=8, help="views per step (8 is the benchmark workload; "
                     "fewer only for small profiling cases)")
     return ap.parse_args()
@@ -358,6 +360,28 @@ def run_ours(args):
     achieved = alg / (phase_ms[dom] / 1000.0) / 1e9
     traffic = read_traffic(dom)
 
+    # ---------------- split-BF16 precision mode (same workload) ---------------
+    split = None
+    if rank == 0 and args.split:
+        sstep = TrainStep(T, V, hw, sc.feat_dim, sc.min_level, sc.max_level, sc.hidden_dim, sc.n_layers,
+                          stochastic=True, seed=1234 + rank, device=dev, precision="split")
+        sstep.capacity = step.capacity
+        sstep._alloc()
+        sg = [sstep.capture(**kw(s)) for s in dsets]
+        for i in range(3):
+            sg[i % N_INPUT_SETS].replay()
+        torch.cuda.synchronize()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        nsplit = max(10, args.steps // 4)
+        s0.record()
+        for i in range(nsplit):
+            sg[i % N_INPUT_SETS].replay()
+        s1.record()
+        torch.cuda.synchronize()
+        split = {"value": B * nsplit / (s0.elapsed_time(s1) / 1000.0), "unit": "views/s", "steps": nsplit,
+                 "precision": "split bf16 (every MLP operand as bf16 hi + lo; gradients within 3e-5 of FP64)"}
+        del sg, sstep
+
     # ---------------- plain FP32 single-view path (denominator) ---------------
     plain = None
     if not args.no_plain and rank == 0:
@@ -384,6 +408,8 @@ def run_ours(args):
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                      "algorithmic_bytes": alg},
     }
+    if split is not None:
+        line["split_precision"] = split
     if plain is not None:
         line["plain_fp32"] = plain
         line["speedup_vs_plain_fp32"] = value / plain["value"]
