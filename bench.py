@@ -210,19 +210,12 @@ def algorithmic_bytes(phase: str, P_: int, B: int, T: int, V: int, ST: int, C_: 
 
 
 def run_ours(args):
-    import torch.distributed as dist
-    from diffsoup_b200 import scenes, _core
+    from diffsoup_b200 import scenes, _core, replicas
     from diffsoup_b200.step import TrainStep
     import diffsoup_b200 as ds
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    rep = replicas.init()  # one process per GPU, NCCL process group for N > 1
+    world, rank, local, dev = rep.world, rep.rank, rep.local_rank, rep.device
 
     sc, mlp, sets = make_inputs(rank, args.views)
     B, T, V = args.views, sc.T, sc.verts.shape[0]
@@ -246,6 +239,16 @@ def run_ours(args):
         if step.overflowed():
             step.capacity *= 2
             step._alloc()
+    # covered fragments per step (every (pixel, triangle) pair passing the coverage test, before the
+    # depth test), counted by the library's fragment operators, averaged over the input sets
+    nfrag = 0
+    for s in dsets:
+        step.run(**kw(s))
+        pos = step.intermediate("pos").clone()
+        for b in range(B):
+            fp, _ = ds.rasterize._compute_fragments(hw[b], pos[b:b + 1].contiguous(), tri)
+            nfrag += fp.shape[0]
+    nfrag /= len(dsets)
     graphs = [step.capture(**kw(s)) for s in dsets]
     torch.cuda.synchronize()
 
@@ -256,8 +259,7 @@ def run_ours(args):
     sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.25)
-    if world > 1:
-        dist.barrier()
+    replicas.barrier(rep)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
@@ -265,16 +267,11 @@ def run_ours(args):
         graphs[i % N_INPUT_SETS].replay()
     e1.record()
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    replicas.barrier(rep)
     clocks = sampler.stop()
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        tt = torch.tensor([ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = replicas.max_over_ranks(rep, e0.elapsed_time(e1))
     overflow = step.overflowed()
-    value = B * args.steps * world / (ms / 1000.0)
+    value = replicas.job_throughput(rep, B * args.steps, ms)
 
     # ---------------- end to end through the public API -----------------------
     # pinned host inputs; each step copies its cameras and targets H2D on a copy
@@ -313,20 +310,15 @@ def run_ours(args):
 
     e2e_loop(min(args.warmup, 4) or 1)
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    replicas.barrier(rep)
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record()
     cs.wait_event(f0)
     e2e_loop(args.steps)
     f1.record()
     torch.cuda.synchronize()
-    ems = f0.elapsed_time(f1)
-    if world > 1:
-        tt = torch.tensor([ems], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ems = float(tt.item())
-    e2e = B * args.steps * world / (ems / 1000.0)
+    ems = replicas.max_over_ranks(rep, f0.elapsed_time(f1))
+    e2e = replicas.job_throughput(rep, B * args.steps, ems)
     assert np.isfinite(loss_host[: args.steps].numpy()).all()
 
     # ---------------- per-phase kernel time (roofline) ------------------------
@@ -401,6 +393,8 @@ def run_ours(args):
                    "l2": f"{N_INPUT_SETS} rotating input sets (4 x 61 MB targets) larger than L2",
                    "list_overflow": overflow},
         "e2e": {"value": e2e, "unit": "views/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 4},
+        "mfragments_per_s": nfrag * args.steps * world / (ms / 1000.0) / 1e6,
+        "fragments_per_step": int(nfrag),
         "gpu_launches": KERNELS_PER_STEP * args.steps,
         "clocks": clocks,
         "phase_ms": {k: round(v, 4) for k, v in phase_ms.items()},
@@ -418,9 +412,7 @@ def run_ours(args):
     if rank == 0:
         print(json.dumps(line), flush=True)
     del graphs, egraphs
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.shutdown(rep)
 
 
 def ctypes_void_p_array(events):
