@@ -232,7 +232,7 @@ def run_ours(args):
         return dict(verts=verts, tri=tri, mvp=s[0], inv_mvp=s[1], feat_src=feat_src, alpha_src=alpha_src,
                     mlp_params=params, target=s[2])
 
-    step.fit_capacity(**kw(dsets[0]))
+    tuned = step.autotune(**kw(dsets[0]))  # list capacity, record store, warp pixel block
     for s in dsets[1:]:
         step.status.zero_()
         step.run(**kw(s))
@@ -358,6 +358,8 @@ def run_ours(args):
         sstep = TrainStep(T, V, hw, sc.feat_dim, sc.min_level, sc.max_level, sc.hidden_dim, sc.n_layers,
                           stochastic=True, seed=1234 + rank, device=dev, precision="split")
         sstep.capacity = step.capacity
+        sstep.cfg.frag_records = step.cfg.frag_records
+        sstep.cfg.block_shape = step.cfg.block_shape
         sstep._alloc()
         sg = [sstep.capture(**kw(s)) for s in dsets]
         for i in range(3):
@@ -391,7 +393,10 @@ def run_ours(args):
         "config": {"workload": WORKLOAD if B == 8 else WORKLOAD.replace("8 views", f"{B} views"), "views_per_step": B, "triangles": T, "resolution": "800x800",
                    "parallelism": f"replicas x{world}", "graph": "one CUDA graph per step",
                    "l2": f"{N_INPUT_SETS} rotating input sets (4 x 61 MB targets) larger than L2",
-                   "list_overflow": overflow},
+                   "list_overflow": overflow,
+                   "autotuned": {"block": tuned["block"], "frag_records_per_px": round(tuned["frag_records"], 3),
+                                 "list_capacity": tuned["list_capacity"],
+                                 "ms_per_step_by_block": {k: round(v, 4) for k, v in tuned["ms_per_step"].items()}}},
         "e2e": {"value": e2e, "unit": "views/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 4},
         "mfragments_per_s": nfrag * args.steps * world / (ms / 1000.0) / 1e6,
         "fragments_per_step": int(nfrag),

@@ -571,6 +571,11 @@ static StepWs carve_step(void* ws, const ds_step_config& c, int num_tiles, int64
     return w;
 }
 
+// log2 of the width of the tiled kernels' pixel blocks for ds_step_config.block_shape
+static int block_shape_log2(const ds_step_config& c) {
+    return c.block_shape == 1 ? 4 : (c.block_shape == 2 ? 2 : kDefaultBlockShape);
+}
+
 template <class K>
 static int shade_dispatch_check(const ds_step_config& c) {
     return (c.C == K::C && c.hidden == K::HID && c.n_layers == K::NL) ? 1 : 0;
@@ -630,6 +635,7 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     DS_CHECK_ARG(c.min_level >= 0 && c.max_level >= c.min_level && c.max_level <= 8, "train_step: bad levels");
     DS_CHECK_ARG(c.stochastic == 0 || rng != nullptr, "train_step: stochastic opacity needs the rng state");
     DS_CHECK_ARG(c.precision == 0 || c.precision == 1, "train_step: precision must be 0 (bf16) or 1 (split bf16)");
+    DS_CHECK_ARG(c.block_shape >= 0 && c.block_shape <= 2, "train_step: block_shape must be 0 (8x4), 1 (16x2) or 2 (4x8)");
     const bool k8 = shade_dispatch_check<ShadeC8H16>(c), k16 = shade_dispatch_check<ShadeC16H64>(c);
     DS_CHECK_ARG(k8 || k16, "train_step: unsupported MLP (C=%d hidden=%d layers=%d); built: 8/16/1, 16/64/2", c.C,
                  c.hidden, c.n_layers);
@@ -689,7 +695,7 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     if (rc || (rc = mark(2, st))) return rc;
     if (side && (rc = join_from(side, 0, st))) return rc;  // the rasterizer reads the accumulated opacities
     rc = tiles_rasterize_impl(c.B, views, num_tiles, c.T, c.max_level, ST, w.alpha_acc, c.stochastic ? 1 : 0,
-                              c.thr_const, rng, rast, w.tiles, list_capacity, rs, st);
+                              c.thr_const, rng, rast, w.tiles, list_capacity, rs, st, block_shape_log2(c));
     if (rc || (rc = mark(3, st))) return rc;
 
     // fused shading forward + backward
@@ -710,7 +716,7 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     // stream beside the edge gradients
     if (side && (rc = fork_to(side, 1, st))) return rc;
     rc = tiles_aux_impl(c.B, views, num_tiles, c.T, c.max_level, ST, w.alpha_acc, w.l1, rast, a.inv_n,
-                        w.grad_alpha_acc, w.tiles, list_capacity, rs, sst);
+                        w.grad_alpha_acc, w.tiles, list_capacity, rs, sst, block_shape_log2(c));
     if (rc || (rc = mark(5, st))) return rc;
 
     // edge gradients to clip-space positions

@@ -24,7 +24,7 @@
 namespace dsb {
 
 constexpr int kWarpsPerCta = 8;
-constexpr int kBlocksPerTile = 8;  // 8x4 pixel blocks of a 16x16 tile
+constexpr int kBlocksPerTile = 8;  // 32-pixel blocks of a 16x16 tile, one warp each
 constexpr int kSortMax = 512;      // longest tile list sorted by depth
 constexpr int kAuxSmemS = 160;     // per-warp shared accumulator for lattices up to level 4
 
@@ -257,19 +257,23 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) sort_lists_kernel(int num_t
     if (lane == 0) sorted[tile] = 1;
 }
 
-// Geometry of one work item (tile, 8x4 block) for the calling lane.
+// Geometry of one work item (tile, 32-pixel block) for the calling lane.
+// Blocks are 2^bwl pixels wide and 32 / 2^bwl high (bwl = 3: 8x4, 4: 16x2,
+// 2: 4x8); a tile holds 8 of them, row-major, and lane l takes pixel
+// (l mod width, l div width) of its block.
 struct BlockGeom {
     int b, px, py, H, W;
     int64_t pix;          // packed pixel index
     bool valid;
     int wx0, wy0;         // block origin
+    int bw, bh;           // block width and height
     int64_t begin, end;   // list range, or [b*T, b*T+T) records when exhaustive
     bool exhaustive, ordered;
 };
 
 __device__ __forceinline__ BlockGeom block_geometry(int item, int B, const ds_view_desc* __restrict__ views, int T,
                                                     const int64_t* __restrict__ offsets,
-                                                    const int* __restrict__ sorted, int64_t capacity) {
+                                                    const int* __restrict__ sorted, int64_t capacity, int bwl) {
     BlockGeom g;
     const int tile = item / kBlocksPerTile, blk = item % kBlocksPerTile;
     g.b = find_view(views, B, tile);
@@ -277,10 +281,13 @@ __device__ __forceinline__ BlockGeom block_geometry(int item, int B, const ds_vi
     const int tl = tile - vd.tile_base;
     const int tx = tl % vd.tiles_x, ty = tl / vd.tiles_x;
     const int lane = threadIdx.x & 31;
-    g.wx0 = tx * DS_TILE + (blk & 1) * 8;
-    g.wy0 = ty * DS_TILE + (blk >> 1) * 4;
-    g.px = g.wx0 + (lane & 7);
-    g.py = g.wy0 + (lane >> 3);
+    g.bw = 1 << bwl;
+    g.bh = 32 >> bwl;
+    const int rl = 4 - bwl;  // log2 of the blocks per tile row (DS_TILE = 16)
+    g.wx0 = tx * DS_TILE + ((blk & ((1 << rl) - 1)) << bwl);
+    g.wy0 = ty * DS_TILE + (blk >> rl) * g.bh;
+    g.px = g.wx0 + (lane & (g.bw - 1));
+    g.py = g.wy0 + (lane >> bwl);
     g.H = vd.H; g.W = vd.W;
     g.valid = g.px < vd.W && g.py < vd.H;
     g.pix = vd.pix_offset + (int64_t)g.py * vd.W + g.px;
@@ -292,8 +299,8 @@ __device__ __forceinline__ BlockGeom block_geometry(int item, int B, const ds_vi
     return g;
 }
 
-__device__ __forceinline__ bool box_overlaps(const TriBox& r, int wx0, int wy0) {
-    return r.y0 < wy0 + 4 && r.y1 > wy0 && r.x0 < wx0 + 8 && r.x1 > wx0;
+__device__ __forceinline__ bool box_overlaps(const TriBox& r, const BlockGeom& g) {
+    return r.y0 < g.wy0 + g.bh && r.y1 > g.wy0 && r.x0 < g.wx0 + g.bw && r.x1 > g.wx0;
 }
 
 __device__ __forceinline__ int warp_next(int* work) {
@@ -337,11 +344,11 @@ __device__ __forceinline__ int stage_group(const BlockGeom& g, int64_t g0, const
         bx = boxes[ri];
     }
     *head_zlo = __shfl_sync(0xffffffffu, bx.zlo, 0);
-    bool c = in && box_overlaps(bx, g.wx0, g.wy0) && bx.zlo <= zcut;
+    bool c = in && box_overlaps(bx, g) && bx.zlo <= zcut;
     if (c) {
         // pixel-centre extents of the block (clamped to the view)
-        const float xa = pix_ndc(g.wx0, g.W), xb = pix_ndc(min(g.wx0 + 7, g.W - 1), g.W);
-        const float ya = pix_ndc(g.wy0, g.H), yb = pix_ndc(min(g.wy0 + 3, g.H - 1), g.H);
+        const float xa = pix_ndc(g.wx0, g.W), xb = pix_ndc(min(g.wx0 + g.bw - 1, g.W - 1), g.W);
+        const float ya = pix_ndc(g.wy0, g.H), yb = pix_ndc(min(g.wy0 + g.bh - 1, g.H - 1), g.H);
         c = !edges_reject_block(edges[ri], xa, xb, ya, yb);
     }
     const unsigned mask = __ballot_sync(0xffffffffu, c);
@@ -449,7 +456,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, DSB_RASTER_MIN_CTAS) raster
     const TriVerts* __restrict__ verts, const TriEdges* __restrict__ edges, const int64_t* __restrict__ offsets,
     const int* __restrict__ sorted, const int* __restrict__ list, int64_t capacity, int level, int S,
     const float* __restrict__ alpha_src, int thr_mode, float thr_const, const uint64_t* __restrict__ rng, int* work, float* __restrict__ rast,
-    RecordStore rs) {
+    RecordStore rs, int bwl) {
     __shared__ WarpStage s_stage[kWarpsPerCta];
     __shared__ WarpRecs s_rec[REC ? kWarpsPerCta : 1];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -461,7 +468,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, DSB_RASTER_MIN_CTAS) raster
     int cid = -1, cfill = 0;  // REC: the warp's current record chunk
     const int items = num_tiles * kBlocksPerTile;
     for (int item = warp_next(work); item < items; item = warp_next(work)) {
-        const BlockGeom g = block_geometry(item, B, views, T, offsets, sorted, capacity);
+        const BlockGeom g = block_geometry(item, B, views, T, offsets, sorted, capacity, bwl);
         const float ndc_x = pix_ndc(g.px, g.W), ndc_y = pix_ndc(g.py, g.H);
         const PhiloxPixel php = philox_pixel(seed, iter, (uint32_t)g.b, (uint32_t)(g.py * g.W + g.px));
         unsigned long long best = ~0ull;
@@ -637,7 +644,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) aux_kernel(
     const float* __restrict__ alpha_src, int C,
     const float* __restrict__ color, const float* __restrict__ target, const float* __restrict__ rast, float scale,
     const int* __restrict__ item_list, const int* __restrict__ item_count, int* work,
-    float* __restrict__ grad_alpha_src) {
+    float* __restrict__ grad_alpha_src, int bwl) {
     __shared__ WarpStage s_stage[kWarpsPerCta];
     __shared__ float s_acc[kWarpsPerCta][kAuxSmemS];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -649,7 +656,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) aux_kernel(
     const int items = item_list ? *item_count : num_tiles * kBlocksPerTile;
     for (int n = warp_next(work); n < items; n = warp_next(work)) {
         const int item = item_list ? item_list[n] : n;
-        const BlockGeom g = block_geometry(item, B, views, T, offsets, sorted, capacity);
+        const BlockGeom g = block_geometry(item, B, views, T, offsets, sorted, capacity, bwl);
         const float ndc_x = pix_ndc(g.px, g.W), ndc_y = pix_ndc(g.py, g.H);
         int tp = -1;
         float zp = 0.f, loss = 0.f;
@@ -794,7 +801,7 @@ static int g_occ_raster = 0, g_occ_raster_rec = 0, g_occ_aux = 0;
 
 int tiles_rasterize_impl(int B, const ds_view_desc* views, int num_tiles, int T, int level, int S,
                          const float* alpha_src, int thr_mode, float thr_const, const uint64_t* rng, float* rast,
-                         void* workspace, int64_t list_capacity, const RecordStore* rs, cudaStream_t st) {
+                         void* workspace, int64_t list_capacity, const RecordStore* rs, cudaStream_t st, int bwl) {
     if (num_tiles == 0) return DS_OK;
     TileWs w = carve(workspace, B, T, num_tiles, list_capacity, nullptr);
     DS_CUDA(cudaMemsetAsync(w.work, 0, sizeof(int), st));
@@ -802,12 +809,12 @@ int tiles_rasterize_impl(int B, const ds_view_desc* views, int num_tiles, int T,
         const void* k = reinterpret_cast<const void*>(&raster_kernel<true>);
         raster_kernel<true><<<block_grid(num_tiles, k, g_occ_raster_rec), kWarpsPerCta * 32, 0, st>>>(
             B, views, num_tiles, T, w.boxes, w.verts, w.edges, w.offsets, w.sorted, w.list, list_capacity, level, S,
-            alpha_src, thr_mode, thr_const, rng, w.work, rast, *rs);
+            alpha_src, thr_mode, thr_const, rng, w.work, rast, *rs, bwl);
     } else {
         const void* k = reinterpret_cast<const void*>(&raster_kernel<false>);
         raster_kernel<false><<<block_grid(num_tiles, k, g_occ_raster), kWarpsPerCta * 32, 0, st>>>(
             B, views, num_tiles, T, w.boxes, w.verts, w.edges, w.offsets, w.sorted, w.list, list_capacity, level, S,
-            alpha_src, thr_mode, thr_const, rng, w.work, rast, RecordStore{});
+            alpha_src, thr_mode, thr_const, rng, w.work, rast, RecordStore{}, bwl);
     }
     return check_launch("tiles_rasterize");
 }
@@ -815,14 +822,14 @@ int tiles_rasterize_impl(int B, const ds_view_desc* views, int num_tiles, int T,
 static int aux_launch(int B, const ds_view_desc* views, int num_tiles, int T, int level, int S,
                       const float* alpha_src, int C, const float* color, const float* target, const float* rast,
                       float scale, float* grad_alpha_src, void* workspace, int64_t list_capacity,
-                      const int* item_list, const int* item_count, cudaStream_t st) {
+                      const int* item_list, const int* item_count, cudaStream_t st, int bwl) {
     TileWs w = carve(workspace, B, T, num_tiles, list_capacity, nullptr);
     DS_CUDA(cudaMemsetAsync(w.work + 1, 0, sizeof(int), st));
     const void* k = reinterpret_cast<const void*>(&aux_kernel);
     aux_kernel<<<block_grid(num_tiles, k, g_occ_aux), kWarpsPerCta * 32, 0, st>>>(
         B, views, num_tiles, T, w.boxes, w.verts, w.edges, w.offsets, w.sorted, w.list, list_capacity, level, S,
         alpha_src, C,
-        color, target, rast, scale, item_list, item_count, w.work + 1, grad_alpha_src);
+        color, target, rast, scale, item_list, item_count, w.work + 1, grad_alpha_src, bwl);
     return check_launch("tiles_opacity_aux");
 }
 
@@ -833,16 +840,16 @@ TileTables tiles_tables(void* workspace, int B, int T, int num_tiles, int64_t li
 
 int tiles_aux_impl(int B, const ds_view_desc* views, int num_tiles, int T, int level, int S, const float* alpha_src,
                    const float* l1, const float* rast, float scale, float* grad_alpha_src, void* workspace,
-                   int64_t list_capacity, const RecordStore* rs, cudaStream_t st) {
+                   int64_t list_capacity, const RecordStore* rs, cudaStream_t st, int bwl) {
     if (num_tiles == 0) return DS_OK;
     if (rs == nullptr)
         return aux_launch(B, views, num_tiles, T, level, S, alpha_src, 1, l1, nullptr, rast, scale, grad_alpha_src,
-                          workspace, list_capacity, nullptr, nullptr, st);
+                          workspace, list_capacity, nullptr, nullptr, st, bwl);
     aux_records_kernel<<<kSMs * 8, kRecChunk, 0, st>>>(*rs, level, S, alpha_src, l1, scale, grad_alpha_src);
     const int rc = check_launch("tiles_opacity_aux records");
     if (rc) return rc;
     return aux_launch(B, views, num_tiles, T, level, S, alpha_src, 1, l1, nullptr, rast, scale, grad_alpha_src,
-                      workspace, list_capacity, rs->fallback, rs->counters + 1, st);
+                      workspace, list_capacity, rs->fallback, rs->counters + 1, st, bwl);
 }
 
 }  // namespace dsb
@@ -860,7 +867,7 @@ int ds_tiles_rasterize(int B, const ds_view_desc* views, int num_tiles, int V, c
     DS_CHECK_ARG(thr_mode == 0 || (thr_mode == 1 && rng != nullptr), "tiles_rasterize: bad threshold mode");
     DS_CHECK_ARG(((uintptr_t)rast & 15) == 0, "tiles_rasterize: rast not 16-byte aligned");
     return tiles_rasterize_impl(B, views, num_tiles, T, level, S, alpha_src, thr_mode, thr_const, rng, rast,
-                                workspace, list_capacity, nullptr, (cudaStream_t)stream);
+                                workspace, list_capacity, nullptr, (cudaStream_t)stream, kDefaultBlockShape);
 }
 
 int ds_tiles_opacity_aux(int B, const ds_view_desc* views, int num_tiles, int V, const float* pos, int T,
@@ -876,7 +883,7 @@ int ds_tiles_opacity_aux(int B, const ds_view_desc* views, int num_tiles, int V,
     DS_CHECK_ARG(((uintptr_t)rast & 15) == 0, "tiles_opacity_aux: rast not 16-byte aligned");
     if (num_tiles == 0) return DS_OK;
     return aux_launch(B, views, num_tiles, T, level, S, alpha_src, C, color, target, rast, scale, grad_alpha_src,
-                      workspace, list_capacity, nullptr, nullptr, (cudaStream_t)stream);
+                      workspace, list_capacity, nullptr, nullptr, (cudaStream_t)stream, kDefaultBlockShape);
 }
 
 }  // extern "C"

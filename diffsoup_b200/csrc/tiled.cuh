@@ -58,17 +58,23 @@ struct RecordStore {
     int64_t capacity;  // multiple of kRecChunk
 };
 
+// Pixel blocks of the tiled kernels: a warp takes 32 pixels of a 16x16 tile,
+// 2^bwl wide and 32 / 2^bwl high (bwl 3: 8x4, the default; 4: 16x2; 2: 4x8).
+// The rasterizer and the opacity pass of one step must use the same shape
+// (re-enumerated blocks are named by block index).
+constexpr int kDefaultBlockShape = 3;
+
 // Rasterizer of ds_tiles_rasterize; records fragments when rs != nullptr.
 int tiles_rasterize_impl(int B, const ds_view_desc* views, int num_tiles, int T, int level, int S,
                          const float* alpha_src, int thr_mode, float thr_const, const uint64_t* rng, float* rast,
-                         void* workspace, int64_t list_capacity, const RecordStore* rs, cudaStream_t st);
+                         void* workspace, int64_t list_capacity, const RecordStore* rs, cudaStream_t st, int bwl);
 
 // Opacity auxiliary gradient with a per-pixel loss l1 [pixels]: from the
 // records plus the fallback blocks when rs != nullptr, else by
 // re-enumerating every block.
 int tiles_aux_impl(int B, const ds_view_desc* views, int num_tiles, int T, int level, int S, const float* alpha_src,
                    const float* l1, const float* rast, float scale, float* grad_alpha_src, void* workspace,
-                   int64_t list_capacity, const RecordStore* rs, cudaStream_t st);
+                   int64_t list_capacity, const RecordStore* rs, cudaStream_t st, int bwl);
 
 // Upper bound on the warps of a tiled-kernel grid (148 SMs x 8 CTAs x 8
 // warps): the record counter ends at most one chunk per warp past capacity.

@@ -35,7 +35,7 @@ class StepConfig(C.Structure):
     _fields_ = [("B", C.c_int32), ("T", C.c_int32), ("V", C.c_int32), ("C", C.c_int32), ("min_level", C.c_int32),
                 ("max_level", C.c_int32), ("hidden", C.c_int32), ("n_layers", C.c_int32),
                 ("stochastic", C.c_int32), ("thr_const", C.c_float), ("frag_records", C.c_float),
-                ("precision", C.c_int32)]
+                ("precision", C.c_int32), ("block_shape", C.c_int32)]
 
 
 _L = _core.lib
@@ -78,6 +78,10 @@ def unpack_mlp_grads(flat: torch.Tensor, mlp: nn.Module) -> None:
             o += n
 
 
+# Launch-layout choices of TrainStep.autotune, per (device, workload).
+autotune_cache: Dict[Tuple, Dict[str, object]] = {}
+
+
 class TrainStep:
     """Workspace and launch state of the batched training step for a fixed
     batch layout (triangle count, vertex count, view resolutions)."""
@@ -96,7 +100,7 @@ class TrainStep:
         if precision not in ("bf16", "split"):
             raise ValueError(f"precision must be 'bf16' or 'split', not {precision!r}")
         self.cfg = StepConfig(self.B, T, V, C_, min_level, max_level, hidden, n_layers, int(stochastic), 0.5,
-                              float(frag_records), 1 if precision == "split" else 0)
+                              float(frag_records), 1 if precision == "split" else 0, 0)
         self.views, self.num_tiles, self.num_pixels, self.pix_offsets = _tiles.view_table(self.hw, self.device)
         self.S = sum(_core.feats_at_level(l) for l in range(min_level, max_level + 1))
         self.nparam = mlp_param_count(C_, hidden, n_layers)
@@ -176,6 +180,63 @@ class TrainStep:
             self.capacity *= 2
             self._alloc()
         raise RuntimeError("tile list capacity did not converge")
+
+    BLOCK_SHAPES = {0: "8x4", 1: "16x2", 2: "4x8"}
+
+    def autotune(self, *args, steps: int = 5, shapes: Sequence[int] = (0, 1, 2), **kwargs) -> Dict[str, object]:
+        """Chooses the launch layout of this step for its inputs (the step's own
+        autotuner, run eagerly before training and before any capture):
+
+          * the tile-list capacity (triangles per bin), doubled until no list
+            overflows (fit_capacity);
+          * the fragment-record store, sized to the records a step reserves
+            plus a quarter, so that no block is re-enumerated;
+          * the pixel block of a rasterizer warp (8x4, 16x2 or 4x8 pixels of a
+            16x16 tile, 8 warps per tile): each is timed with CUDA events over
+            `steps` eager steps after a warm-up, and the fastest kept.
+
+        Results do not depend on the choices.  The RNG iteration is restored,
+        so tuning does not advance the training state.  Choices are cached per
+        device and workload (`autotune_cache`).  Returns them."""
+        key = (torch.cuda.get_device_name(self.device), self.B, tuple(self.hw), self.cfg.T, self.cfg.V, self.cfg.C,
+               self.cfg.min_level, self.cfg.max_level, self.cfg.hidden, self.cfg.n_layers, self.cfg.precision,
+               self.cfg.stochastic)
+        it0 = self.rng[1].clone()
+        hit = autotune_cache.get(key)
+        if hit is not None:
+            self.capacity = max(self.capacity, hit["list_capacity"])
+            self.cfg.frag_records = hit["frag_records"]
+            self.cfg.block_shape = hit["block_shape"]
+            self._alloc()
+            return dict(hit)
+        self.fit_capacity(*args, **kwargs)
+        # records reserved by one step -> records per pixel with a margin
+        self.run(*args, **kwargs)
+        counters = self.intermediate("record_counters").cpu() if self.record_capacity else None
+        if counters is not None:
+            need = (int(counters[0]) + int(counters[1]) * 256) / max(self.num_pixels, 1)
+            self.cfg.frag_records = float(min(max(1.25 * need, 0.5), 16.0))
+            self._alloc()
+        times = {}
+        for shape in shapes:
+            self.cfg.block_shape = int(shape)
+            for _ in range(2):
+                self.run(*args, **kwargs)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(steps):
+                self.run(*args, **kwargs)
+            e1.record()
+            torch.cuda.synchronize()
+            times[self.BLOCK_SHAPES[int(shape)]] = e0.elapsed_time(e1) / steps
+        best = min(shapes, key=lambda sh: times[self.BLOCK_SHAPES[int(sh)]])
+        self.cfg.block_shape = int(best)
+        self.rng[1].copy_(it0)
+        self.status.zero_()
+        out = {"list_capacity": int(self.capacity), "frag_records": float(self.cfg.frag_records),
+               "block_shape": int(best), "block": self.BLOCK_SHAPES[int(best)], "ms_per_step": times}
+        autotune_cache[key] = dict(out)
+        return out
 
     def capture(self, *args, **kwargs) -> torch.cuda.CUDAGraph:
         """Capture one step over fixed buffers into a CUDA graph (replay with

@@ -239,6 +239,10 @@ typedef struct {
      * the BF16 tensor cores (FP32 accumulation), gradients within ~1e-5 of
      * FP64 instead of the ~5e-3 that BF16 inputs alone cause. */
     int32_t precision;
+    /* Pixel block of one rasterizer warp (8 per 16x16 tile): 0 = 8x4,
+     * 1 = 16x2, 2 = 4x8.  Same results; the fastest depends on the scene
+     * (diffsoup_b200.step.TrainStep.autotune times them). */
+    int32_t block_shape;
 } ds_step_config;
 
 /* Packed MLP parameter layout (fp32): W0[hidden][C+3] b0[hidden]

@@ -196,3 +196,27 @@ def test_train_step_gradients_match_central_differences(config):
                 want.append(fd_mlp(inp, rasts, layer, which, idx))
             off += arr.size
     assert rel(got, want) <= GRAD_TOL["mlp"], (got, want)
+
+
+def test_block_shapes_give_identical_results_and_autotune_picks_one():
+    """The three pixel-block shapes of the rasterizer warps (8x4, 16x2, 4x8)
+    give bit-identical ID buffers and the same loss; the autotuner times them,
+    keeps one and leaves the RNG iteration where it was."""
+    sc, hw, inp, step, d = _setup(2, 6, num_tris=3000, num_views=2, resolution=(128, 160))
+    outs = []
+    for shape in (0, 1, 2):
+        step.cfg.block_shape = shape
+        step.rng[1] = 0
+        rast = torch.empty(step.num_pixels, 4, device=DEV)
+        loss = float(step.run(**d, rast_out=rast).item())
+        torch.cuda.synchronize()
+        outs.append((rast.cpu().numpy().view(np.uint32), loss, step.grad_alpha_src.clone()))
+    for r, l, ga in outs[1:]:
+        assert np.array_equal(r, outs[0][0])
+        assert abs(l - outs[0][1]) <= 1e-6 * outs[0][1]
+        assert rel(ga.cpu().numpy(), outs[0][2].cpu().numpy()) < 1e-5
+    step.rng[1] = 3
+    choice = step.autotune(**d, steps=2)
+    assert choice["block_shape"] in (0, 1, 2) and set(choice["ms_per_step"]) == {"8x4", "16x2", "4x8"}
+    assert int(step.rng[1].item()) == 3
+    assert step.autotune(**d, steps=2)["block_shape"] == choice["block_shape"]  # cached
