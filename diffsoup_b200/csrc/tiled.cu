@@ -25,6 +25,7 @@ namespace dsb {
 
 constexpr int kWarpsPerCta = 8;
 constexpr int kBlocksPerTile = 8;  // 32-pixel blocks of a 16x16 tile, one warp each
+static_assert(DS_TILE == 16, "the block decode of block_geometry assumes 16x16 tiles");
 constexpr int kSortMax = 512;      // longest tile list sorted by depth
 constexpr int kAuxSmemS = 160;     // per-warp shared accumulator for lattices up to level 4
 
