@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark of the DiffSoup training step on B200.
 
-Workload (BASELINE configuration "plain method, object scale"): 15,000
+Workload (the "plain method, object scale" benchmark configuration): 15,000
 triangles on a noisy unit sphere shell, 8 views of 800x800 on a ring of radius
 4, multires features at levels 0..2 x 8 channels, shading MLP 11 -> 16 -> 3,
 stochastic binary opacity, MSE against a U[0,1] target, full forward+backward
@@ -192,7 +192,8 @@ def run_reference(args):
 
 # ---------------------------------------------------------------------------
 def algorithmic_bytes(phase: str, P_: int, B: int, T: int, V: int, ST: int, C_: int) -> float:
-    """Minimal DRAM bytes of one launch of each step kernel."""
+    """Minimal DRAM bytes of one launch of each step kernel: what the kernel must read and write
+    once (per-pixel buffers, per-(view, triangle) records, lattice samples), no re-reads."""
     if phase == "shade":  # rast 16 R, target 12 R, colour 12 W, dL/dcolour 12 W, |c-t| 4 W; bf16 features + fp32 grads
         return P_ * 56.0 + T * ST * C_ * (2 + 8)
     # fragment records: 16 B each, about one per pixel on this workload (fragments in front of the surface)
