@@ -90,54 +90,113 @@ __device__ __forceinline__ bool tile_may_cover(const TriVerts& v, const ds_view_
                                  pix_ndc(y + DS_TILE - 1, vd.H));
 }
 
-// Pass 1: boxes, vertices and per-tile counts.
+// The items of a warp, 32 at a time: lane j owns n_j consecutive items and
+// f(valid, owner, k) is called by every lane for one item each pass (k-th
+// item of lane `owner`; valid is false for the lanes past the last item).
+// Every lane must call this (f may shuffle).
+template <class F>
+__device__ __forceinline__ void warp_items(int n, F&& f) {
+    const int lane = threadIdx.x & 31;
+    int excl = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, excl, o);
+        if (lane >= o) excl += v;
+    }
+    const int total = __shfl_sync(0xffffffffu, excl, 31);
+    excl -= n;  // first item of this lane
+    for (int base = 0; base < total; base += 32) {
+        const int slot = base + lane;
+        int owner = 0;  // the last lane whose first item is at or before slot
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+            const int e = __shfl_sync(0xffffffffu, excl, owner + step);
+            if (e <= slot) owner += step;
+        }
+        const int k = slot - __shfl_sync(0xffffffffu, excl, owner);
+        f(slot < total, owner, k);
+    }
+}
+
+// Pass 1: boxes, vertices, depth bounds, edge records and per-tile counts.
+// The (triangle, tile) pairs of a warp's 32 triangles are tested 32 at a
+// time (warp_items), so lanes do not wait on the lane with the largest rect.
 __global__ void __launch_bounds__(kThreads) bin_setup_kernel(int B, const ds_view_desc* __restrict__ views, int V,
                                                              const float* __restrict__ pos, int T,
                                                              const int* __restrict__ tri, TriBox* __restrict__ boxes,
                                                              TriVerts* __restrict__ verts, TriNdc* __restrict__ ndc,
                                                              TriEdges* __restrict__ edges, int* __restrict__ counts) {
+    __shared__ unsigned long long s_mask[kThreads];
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (int64_t)B * T) return;
-    const int b = (int)(i / T), t = (int)(i % T);
+    const bool live = i < (int64_t)B * T;
+    const int b = live ? (int)(i / T) : 0, t = live ? (int)(i % T) : 0;
     const ds_view_desc vd = views[b];
-    const float* P = pos + (size_t)b * V * 4;
     TriVerts v;
-    v.p0 = load_vertex(P, __ldg(tri + t * 3 + 0));
-    v.p1 = load_vertex(P, __ldg(tri + t * 3 + 1));
-    v.p2 = load_vertex(P, __ldg(tri + t * 3 + 2));
-    int h0, hl, w0, wl;
-    triangle_rect(vd.H, vd.W, v.p0, v.p1, v.p2, h0, hl, w0, wl);
     TriBox r;
-    r.y0 = (short)h0; r.y1 = (short)(h0 + hl); r.x0 = (short)w0; r.x1 = (short)(w0 + wl);
-    // depth bounds (only used when the rect is non-empty, i.e. every w > 0)
-    const float d0 = v.p0.z / v.p0.w, d1 = v.p1.z / v.p1.w, d2 = v.p2.z / v.p2.w;
-    const float mz = fmaxf(fmaxf(fabsf(v.p0.z), fabsf(v.p1.z)), fabsf(v.p2.z));
-    const float mw = fminf(fminf(v.p0.w, v.p1.w), v.p2.w);
-    const float margin = 1e-5f + 4e-6f * (mz / mw + fmaxf(fmaxf(fabsf(d0), fabsf(d1)), fabsf(d2)));
-    r.zlo = fminf(fminf(d0, d1), d2) - margin;
-    r.zhi = fmaxf(fmaxf(d0, d1), d2) + margin;
-    if (!(r.zlo == r.zlo && r.zhi == r.zhi)) { r.zlo = -INFINITY; r.zhi = INFINITY; }  // NaN: no bounds
-    boxes[i] = r;
-    verts[i] = v;
+    r.y0 = r.y1 = r.x0 = r.x1 = 0;
+    r.zlo = r.zhi = 0.f;
+    int tx0 = 0, tx1 = -1, ty0 = 0, ty1 = -1;
+    if (live) {
+        const float* P = pos + (size_t)b * V * 4;
+        v.p0 = load_vertex(P, __ldg(tri + t * 3 + 0));
+        v.p1 = load_vertex(P, __ldg(tri + t * 3 + 1));
+        v.p2 = load_vertex(P, __ldg(tri + t * 3 + 2));
+        int h0, hl, w0, wl;
+        triangle_rect(vd.H, vd.W, v.p0, v.p1, v.p2, h0, hl, w0, wl);
+        r.y0 = (short)h0; r.y1 = (short)(h0 + hl); r.x0 = (short)w0; r.x1 = (short)(w0 + wl);
+        // depth bounds (only used when the rect is non-empty, i.e. every w > 0)
+        const float d0 = v.p0.z / v.p0.w, d1 = v.p1.z / v.p1.w, d2 = v.p2.z / v.p2.w;
+        const float mz = fmaxf(fmaxf(fabsf(v.p0.z), fabsf(v.p1.z)), fabsf(v.p2.z));
+        const float mw = fminf(fminf(v.p0.w, v.p1.w), v.p2.w);
+        const float margin = 1e-5f + 4e-6f * (mz / mw + fmaxf(fmaxf(fabsf(d0), fabsf(d1)), fabsf(d2)));
+        r.zlo = fminf(fminf(d0, d1), d2) - margin;
+        r.zhi = fmaxf(fmaxf(d0, d1), d2) + margin;
+        if (!(r.zlo == r.zlo && r.zhi == r.zhi)) { r.zlo = -INFINITY; r.zhi = INFINITY; }  // NaN: no bounds
+        boxes[i] = r;
+        verts[i] = v;
+        if (!box_tiles(r, tx0, tx1, ty0, ty1)) { tx1 = tx0 - 1; ty1 = ty0 - 1; }
+    } else {
+        v.p0 = v.p1 = v.p2 = make_float4(0.f, 0.f, 0.f, 1.f);
+    }
     // tiles the triangle may cover; for rects of at most 64 tiles their bit
     // mask (row-major over the rect) rides in the NDC record's spare lanes
-    uint64_t m = 0;
-    int tx0, tx1, ty0, ty1;
+    const int ntx = tx1 - tx0 + 1, nty = ty1 - ty0 + 1;
+    const int ntiles = ntx > 0 && nty > 0 ? ntx * nty : 0;
+    s_mask[threadIdx.x] = 0ull;
+    __syncwarp();
+    const int wbase = threadIdx.x & ~31;
+    warp_items(ntiles, [&](bool valid, int owner, int k) {
+        float4 q[3];
+        const float4 mine[3] = {v.p0, v.p1, v.p2};
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            q[j].x = __shfl_sync(0xffffffffu, mine[j].x, owner);
+            q[j].y = __shfl_sync(0xffffffffu, mine[j].y, owner);
+            q[j].z = __shfl_sync(0xffffffffu, mine[j].z, owner);
+            q[j].w = __shfl_sync(0xffffffffu, mine[j].w, owner);
+        }
+        const int otx0 = __shfl_sync(0xffffffffu, tx0, owner), oty0 = __shfl_sync(0xffffffffu, ty0, owner);
+        const int ontx = __shfl_sync(0xffffffffu, ntx, owner), ont = __shfl_sync(0xffffffffu, ntiles, owner);
+        const int ob = __shfl_sync(0xffffffffu, b, owner);
+        if (!valid) return;
+        const ds_view_desc ovd = views[ob];
+        const int ty = oty0 + k / ontx, tx = otx0 + k % ontx;
+        TriVerts ov;
+        ov.p0 = q[0]; ov.p1 = q[1]; ov.p2 = q[2];
+        if (tile_may_cover(ov, ovd, tx, ty)) {
+            atomicAdd(counts + ovd.tile_base + ty * ovd.tiles_x + tx, 1);
+            if (ont <= 64) atomicOr(&s_mask[wbase + owner], 1ull << k);
+        }
+    });
+    __syncwarp();
+    if (!live) return;
+    const uint64_t m = ntiles <= 64 ? s_mask[threadIdx.x] : 0ull;
     TriEdges te;
 #pragma unroll
     for (int k = 0; k < 3; ++k) te.e[k] = make_float4(0.f, 0.f, 1.f, 0.f);
-    if (box_tiles(r, tx0, tx1, ty0, ty1)) {
+    if (ntiles > 0)
         te = tri_edges_over_rect(v.p0, v.p1, v.p2, pix_ndc(r.x0, vd.W), pix_ndc(r.x1 - 1, vd.W), pix_ndc(r.y0, vd.H),
                                  pix_ndc(r.y1 - 1, vd.H));
-        const int ntx = tx1 - tx0 + 1;
-        const bool small = (ty1 - ty0 + 1) * ntx <= 64;
-        for (int ty = ty0; ty <= ty1; ++ty)
-            for (int tx = tx0; tx <= tx1; ++tx)
-                if (tile_may_cover(v, vd, tx, ty)) {
-                    atomicAdd(counts + vd.tile_base + ty * vd.tiles_x + tx, 1);
-                    if (small) m |= 1ull << ((ty - ty0) * ntx + (tx - tx0));
-                }
-    }
     TriNdc q;
     q.a = make_float4(v.p0.x / v.p0.w, v.p0.y / v.p0.w, v.p1.x / v.p1.w, v.p1.y / v.p1.w);
     q.b = make_float4(v.p2.x / v.p2.w, v.p2.y / v.p2.w, __uint_as_float((uint32_t)m),
@@ -146,7 +205,9 @@ __global__ void __launch_bounds__(kThreads) bin_setup_kernel(int B, const ds_vie
     edges[i] = te;
 }
 
-// Pass 2: scatter record indices into the per-tile lists.
+// Pass 2: scatter record indices into the per-tile lists: the tiles of the
+// count pass's masks, distributed over the warp (warp_items), and for rects
+// of more than 64 tiles the test itself, per triangle.
 __global__ void __launch_bounds__(kThreads) bin_fill_kernel(int B, const ds_view_desc* __restrict__ views, int T,
                                                             const TriBox* __restrict__ boxes,
                                                             const TriVerts* __restrict__ verts,
@@ -155,26 +216,49 @@ __global__ void __launch_bounds__(kThreads) bin_fill_kernel(int B, const ds_view
                                                             int* __restrict__ cursor, int* __restrict__ list,
                                                             int64_t capacity, int* __restrict__ status) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (int64_t)B * T) return;
-    const int b = (int)(i / T);
+    const bool live = i < (int64_t)B * T;
+    const int b = live ? (int)(i / T) : 0;
     const ds_view_desc vd = views[b];
-    const TriBox rc = boxes[i];
-    int tx0, tx1, ty0, ty1;
-    if (!box_tiles(rc, tx0, tx1, ty0, ty1)) return;
-    const int ntx = tx1 - tx0 + 1;
-    const bool small = (ty1 - ty0 + 1) * ntx <= 64;
-    const float4 nb = ndc[i].b;
-    const uint64_t m = (uint64_t)__float_as_uint(nb.z) | ((uint64_t)__float_as_uint(nb.w) << 32);
-    bool over = false;
-    for (int ty = ty0; ty <= ty1; ++ty)
-        for (int tx = tx0; tx <= tx1; ++tx) {
-            // the count pass's decision: its bit, or the test itself for large rects
-            if (small ? !((m >> ((ty - ty0) * ntx + (tx - tx0))) & 1u) : !tile_may_cover(verts[i], vd, tx, ty))
-                continue;
-            const int tile = vd.tile_base + ty * vd.tiles_x + tx;
-            const int64_t at = offsets[tile] + atomicAdd(cursor + tile, 1);
-            if (at < capacity) list[at] = (int)i; else over = true;
+    int tx0 = 0, tx1 = -1, ty0 = 0, ty1 = -1;
+    uint64_t m = 0;
+    if (live) {
+        const TriBox rc = boxes[i];
+        if (box_tiles(rc, tx0, tx1, ty0, ty1)) {
+            const float4 nb = ndc[i].b;
+            m = (uint64_t)__float_as_uint(nb.z) | ((uint64_t)__float_as_uint(nb.w) << 32);
+        } else {
+            tx1 = tx0 - 1;
+            ty1 = ty0 - 1;
         }
+    }
+    const int ntx = tx1 - tx0 + 1, nty = ty1 - ty0 + 1;
+    const int ntiles = ntx > 0 && nty > 0 ? ntx * nty : 0;
+    const bool small = ntiles <= 64;
+    bool over = false;
+    const uint32_t mlo = (uint32_t)m, mhi = (uint32_t)(m >> 32);
+    warp_items(small ? __popcll(m) : 0, [&](bool valid, int owner, int k) {
+        const uint32_t olo = __shfl_sync(0xffffffffu, mlo, owner), ohi = __shfl_sync(0xffffffffu, mhi, owner);
+        const int otx0 = __shfl_sync(0xffffffffu, tx0, owner), oty0 = __shfl_sync(0xffffffffu, ty0, owner);
+        const int ontx = __shfl_sync(0xffffffffu, ntx, owner), ob = __shfl_sync(0xffffffffu, b, owner);
+        if (!valid) return;
+        // the k-th tile of the owner's mask
+        const int nlo = __popc(olo);
+        const int bit = k < nlo ? (int)__fns(olo, 0, k + 1) : 32 + (int)__fns(ohi, 0, k - nlo + 1);
+        const ds_view_desc ovd = views[ob];
+        const int tile = ovd.tile_base + (oty0 + bit / ontx) * ovd.tiles_x + otx0 + bit % ontx;
+        const int64_t at = offsets[tile] + atomicAdd(cursor + tile, 1);
+        if (at < capacity) list[at] = (int)((int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31) + owner);
+        else over = true;
+    });
+    if (live && !small) {  // large rects: the test itself
+        for (int ty = ty0; ty <= ty1; ++ty)
+            for (int tx = tx0; tx <= tx1; ++tx) {
+                if (!tile_may_cover(verts[i], vd, tx, ty)) continue;
+                const int tile = vd.tile_base + ty * vd.tiles_x + tx;
+                const int64_t at = offsets[tile] + atomicAdd(cursor + tile, 1);
+                if (at < capacity) list[at] = (int)i; else over = true;
+            }
+    }
     if (over) atomicOr(status, DS_STATUS_LIST_OVERFLOW);
 }
 
