@@ -27,6 +27,17 @@ constexpr int kWarpsPerCta = 8;
 constexpr int kBlocksPerTile = 8;  // 32-pixel blocks of a 16x16 tile, one warp each
 static_assert(DS_TILE == 16, "the block decode of block_geometry assumes 16x16 tiles");
 constexpr int kSortMax = 512;      // longest tile list sorted by depth
+constexpr int kSortWarps = 8;      // warps (tiles) per CTA of the sort pass
+
+// One entry of a tile's list: the (view, triangle) record's pixel rect and
+// near depth bound, and the record index -- what the rasterizer's staging
+// and the sort by depth read, without a second, dependent load.
+struct __align__(16) ListEntry {
+    short y0, y1, x0, x1;
+    float zlo;
+    int ri;
+};
+static_assert(sizeof(ListEntry) == 16, "ListEntry layout");
 constexpr int kAuxSmemS = 160;     // per-warp shared accumulator for lattices up to level 4
 
 struct TileWs {
@@ -38,7 +49,8 @@ struct TileWs {
     int64_t* offsets;  // [num_tiles + 1] exclusive prefix of counts
     int* cursor;
     int* sorted;       // per tile: 1 when its list is ordered by zlo
-    int* list;
+    ListEntry* list;
+    ListEntry* fill;   // the fill pass's unsorted lists (same offsets)
     int* work;         // persistent-kernel work counters [2]
     void* scan;
 };
@@ -59,7 +71,8 @@ static TileWs carve(void* ws, int B, int T, int num_tiles, int64_t capacity, siz
     w.sorted = reinterpret_cast<int*>(p + o); o += al256((size_t)num_tiles * sizeof(int));
     w.work = reinterpret_cast<int*>(p + o); o += 256;
     w.scan = p + o; o += al256(scan_workspace_bytes(num_tiles));
-    w.list = reinterpret_cast<int*>(p + o); o += al256((size_t)capacity * sizeof(int));
+    w.list = reinterpret_cast<ListEntry*>(p + o); o += al256((size_t)capacity * sizeof(ListEntry));
+    w.fill = reinterpret_cast<ListEntry*>(p + o); o += al256((size_t)capacity * sizeof(ListEntry));
     if (total) *total = o;
     return w;
 }
@@ -213,7 +226,7 @@ __global__ void __launch_bounds__(kThreads) bin_fill_kernel(int B, const ds_view
                                                             const TriVerts* __restrict__ verts,
                                                             const TriNdc* __restrict__ ndc,
                                                             const int64_t* __restrict__ offsets,
-                                                            int* __restrict__ cursor, int* __restrict__ list,
+                                                            int* __restrict__ cursor, ListEntry* __restrict__ list,
                                                             int64_t capacity, int* __restrict__ status) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const bool live = i < (int64_t)B * T;
@@ -221,8 +234,14 @@ __global__ void __launch_bounds__(kThreads) bin_fill_kernel(int B, const ds_view
     const ds_view_desc vd = views[b];
     int tx0 = 0, tx1 = -1, ty0 = 0, ty1 = -1;
     uint64_t m = 0;
+    ListEntry le;
+    le.y0 = le.y1 = le.x0 = le.x1 = 0;
+    le.zlo = 0.f;
+    le.ri = (int)i;
     if (live) {
         const TriBox rc = boxes[i];
+        le.y0 = rc.y0; le.y1 = rc.y1; le.x0 = rc.x0; le.x1 = rc.x1;
+        le.zlo = rc.zlo;
         if (box_tiles(rc, tx0, tx1, ty0, ty1)) {
             const float4 nb = ndc[i].b;
             m = (uint64_t)__float_as_uint(nb.z) | ((uint64_t)__float_as_uint(nb.w) << 32);
@@ -236,8 +255,11 @@ __global__ void __launch_bounds__(kThreads) bin_fill_kernel(int B, const ds_view
     const bool small = ntiles <= 64;
     bool over = false;
     const uint32_t mlo = (uint32_t)m, mhi = (uint32_t)(m >> 32);
+    const int4 lw = *reinterpret_cast<const int4*>(&le);
     warp_items(small ? __popcll(m) : 0, [&](bool valid, int owner, int k) {
         const uint32_t olo = __shfl_sync(0xffffffffu, mlo, owner), ohi = __shfl_sync(0xffffffffu, mhi, owner);
+        const int4 ole = make_int4(__shfl_sync(0xffffffffu, lw.x, owner), __shfl_sync(0xffffffffu, lw.y, owner),
+                                   __shfl_sync(0xffffffffu, lw.z, owner), __shfl_sync(0xffffffffu, lw.w, owner));
         const int otx0 = __shfl_sync(0xffffffffu, tx0, owner), oty0 = __shfl_sync(0xffffffffu, ty0, owner);
         const int ontx = __shfl_sync(0xffffffffu, ntx, owner), ob = __shfl_sync(0xffffffffu, b, owner);
         if (!valid) return;
@@ -247,7 +269,7 @@ __global__ void __launch_bounds__(kThreads) bin_fill_kernel(int B, const ds_view
         const ds_view_desc ovd = views[ob];
         const int tile = ovd.tile_base + (oty0 + bit / ontx) * ovd.tiles_x + otx0 + bit % ontx;
         const int64_t at = offsets[tile] + atomicAdd(cursor + tile, 1);
-        if (at < capacity) list[at] = (int)((int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31) + owner);
+        if (at < capacity) *reinterpret_cast<int4*>(list + at) = ole;
         else over = true;
     });
     if (live && !small) {  // large rects: the test itself
@@ -256,70 +278,75 @@ __global__ void __launch_bounds__(kThreads) bin_fill_kernel(int B, const ds_view
                 if (!tile_may_cover(verts[i], vd, tx, ty)) continue;
                 const int tile = vd.tile_base + ty * vd.tiles_x + tx;
                 const int64_t at = offsets[tile] + atomicAdd(cursor + tile, 1);
-                if (at < capacity) list[at] = (int)i; else over = true;
+                if (at < capacity) list[at] = le; else over = true;
             }
     }
     if (over) atomicOr(status, DS_STATUS_LIST_OVERFLOW);
 }
 
-// Pass 3: sort each tile's list by zlo (warp per tile, bitonic in shared
-// memory).  Lists longer than kSortMax, or cut by the capacity, stay as they
-// are and are marked unsorted.
-__global__ void __launch_bounds__(kWarpsPerCta * 32) sort_lists_kernel(int num_tiles, const TriBox* __restrict__ boxes,
-                                                                       const int64_t* __restrict__ offsets,
-                                                                       int* __restrict__ list, int64_t capacity,
-                                                                       int* __restrict__ sorted) {
-    __shared__ float s_key[kWarpsPerCta][kSortMax];
-    __shared__ int s_val[kWarpsPerCta][kSortMax];
+// Pass 3: each tile's list ordered by zlo, from the fill pass's lists into
+// the rasterizer's (warp per tile): the (key, position) pairs are sorted by a
+// bitonic network in registers (up to 32 entries) or in shared memory (up to
+// kSortMax), and each entry is then gathered once.  Longer lists are copied
+// as they are and marked unsorted; lists cut by the capacity are not used.
+__global__ void __launch_bounds__(kSortWarps * 32) sort_lists_kernel(int num_tiles,
+                                                                     const int64_t* __restrict__ offsets,
+                                                                     const ListEntry* __restrict__ fill,
+                                                                     ListEntry* __restrict__ list, int64_t capacity,
+                                                                     int* __restrict__ sorted) {
+    __shared__ float s_key[kSortWarps][kSortMax];
+    __shared__ short s_pos[kSortWarps][kSortMax];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int tile = blockIdx.x * kWarpsPerCta + warp;
+    const int tile = blockIdx.x * kSortWarps + warp;
     if (tile >= num_tiles) return;
     const int64_t begin = offsets[tile], end = offsets[tile + 1];
     const int n = (int)(end - begin);
-    if (end > capacity || n > kSortMax) {
+    if (end > capacity) {  // cut: the tile runs the exhaustive path
         if (lane == 0) sorted[tile] = 0;
         return;
     }
-    if (n <= 1) {
-        if (lane == 0) sorted[tile] = 1;
+    const int4* F = reinterpret_cast<const int4*>(fill + begin);
+    int4* L = reinterpret_cast<int4*>(list + begin);
+    if (n > kSortMax) {
+        for (int i = lane; i < n; i += 32) L[i] = F[i];
+        if (lane == 0) sorted[tile] = 0;
         return;
     }
-    if (n <= 32) {  // one entry per lane: bitonic network in registers
-        int ri = -1;
+    if (n <= 32) {  // one entry per lane: bitonic network on (key, lane) in registers
+        int4 ent = make_int4(0, 0, 0, 0);
         float key = INFINITY;
+        int src = lane;
         if (lane < n) {
-            ri = list[begin + lane];
-            key = fminf(boxes[ri].zlo, 3.0e38f);  // real keys stay below the +inf padding
+            ent = F[lane];
+            key = fminf(__int_as_float(ent.z), 3.0e38f);  // real keys stay below the +inf padding
         }
+        if (n > 1) {
 #pragma unroll
-        for (int k = 2; k <= 32; k <<= 1) {
+            for (int k = 2; k <= 32; k <<= 1) {
 #pragma unroll
-            for (int j = k >> 1; j > 0; j >>= 1) {
-                const float ok = __shfl_xor_sync(0xffffffffu, key, j);
-                const int ov = __shfl_xor_sync(0xffffffffu, ri, j);
-                // the lower lane of the pair keeps the smaller key in ascending runs
-                const bool up = (lane & k) == 0, lower = (lane & j) == 0;
-                const bool take = (lower == up) ? (ok < key) : (ok > key);
-                if (take) { key = ok; ri = ov; }
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    const float ok = __shfl_xor_sync(0xffffffffu, key, j);
+                    const int os = __shfl_xor_sync(0xffffffffu, src, j);
+                    // the lower lane of the pair keeps the smaller key in ascending runs
+                    const bool up = (lane & k) == 0, lower = (lane & j) == 0;
+                    const bool take = (lower == up) ? (ok < key) : (ok > key);
+                    if (take) { key = ok; src = os; }
+                }
             }
         }
-        if (lane < n) list[begin + lane] = ri;
+        const int4 out = make_int4(__shfl_sync(0xffffffffu, ent.x, src), __shfl_sync(0xffffffffu, ent.y, src),
+                                   __shfl_sync(0xffffffffu, ent.z, src), __shfl_sync(0xffffffffu, ent.w, src));
+        if (lane < n) L[lane] = out;
         if (lane == 0) sorted[tile] = 1;
         return;
     }
     int size = 64;
     while (size < n) size <<= 1;
     float* key = s_key[warp];
-    int* val = s_val[warp];
+    short* pos = s_pos[warp];
     for (int i = lane; i < size; i += 32) {
-        if (i < n) {
-            const int ri = list[begin + i];
-            key[i] = fminf(boxes[ri].zlo, 3.0e38f);  // real keys stay below the +inf padding
-            val[i] = ri;
-        } else {
-            key[i] = INFINITY;
-            val[i] = -1;
-        }
+        key[i] = i < n ? fminf(__int_as_float(F[i].z), 3.0e38f) : INFINITY;  // real keys stay below the padding
+        pos[i] = (short)i;
     }
     __syncwarp();
     for (int k = 2; k <= size; k <<= 1) {
@@ -331,14 +358,14 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) sort_lists_kernel(int num_t
                     const bool up = (i & k) == 0;
                     if ((a > c) == up && a != c) {
                         key[i] = c; key[l] = a;
-                        const int t = val[i]; val[i] = val[l]; val[l] = t;
+                        const short t = pos[i]; pos[i] = pos[l]; pos[l] = t;
                     }
                 }
             }
             __syncwarp();
         }
     }
-    for (int i = lane; i < n; i += 32) list[begin + i] = val[i];
+    for (int i = lane; i < n; i += 32) L[i] = F[pos[i]];
     if (lane == 0) sorted[tile] = 1;
 }
 
@@ -415,7 +442,7 @@ struct WarpStage {
 // entry (the smallest, when the list is ordered).
 __device__ __forceinline__ int stage_group(const BlockGeom& g, int64_t g0, const TriBox* __restrict__ boxes,
                                            const TriVerts* __restrict__ verts, const TriEdges* __restrict__ edges,
-                                           const int* __restrict__ list, int T, float zcut, WarpStage& st,
+                                           const ListEntry* __restrict__ list, int T, float zcut, WarpStage& st,
                                            float* head_zlo) {
     const int lane = threadIdx.x & 31;
     const int64_t e = g0 + lane;
@@ -425,8 +452,16 @@ __device__ __forceinline__ int stage_group(const BlockGeom& g, int64_t g0, const
     bx.y0 = bx.y1 = bx.x0 = bx.x1 = 0;
     bx.zlo = INFINITY; bx.zhi = INFINITY;
     if (in) {
-        ri = g.exhaustive ? (int)e : __ldg(list + e);
-        bx = boxes[ri];
+        if (g.exhaustive) {
+            ri = (int)e;
+            bx = boxes[ri];
+        } else {
+            const int4 le = __ldg(reinterpret_cast<const int4*>(list + e));
+            ri = le.w;
+            bx.y0 = (short)(le.x & 0xffff); bx.y1 = (short)(le.x >> 16);
+            bx.x0 = (short)(le.y & 0xffff); bx.x1 = (short)(le.y >> 16);
+            bx.zlo = __int_as_float(le.z);
+        }
     }
     *head_zlo = __shfl_sync(0xffffffffu, bx.zlo, 0);
     bool c = in && box_overlaps(bx, g) && bx.zlo <= zcut;
@@ -539,7 +574,7 @@ template <bool REC>
 __global__ void __launch_bounds__(kWarpsPerCta * 32, DSB_RASTER_MIN_CTAS) raster_kernel(
     int B, const ds_view_desc* __restrict__ views, int num_tiles, int T, const TriBox* __restrict__ boxes,
     const TriVerts* __restrict__ verts, const TriEdges* __restrict__ edges, const int64_t* __restrict__ offsets,
-    const int* __restrict__ sorted, const int* __restrict__ list, int64_t capacity, int level, int S,
+    const int* __restrict__ sorted, const ListEntry* __restrict__ list, int64_t capacity, int level, int S,
     const float* __restrict__ alpha_src, int thr_mode, float thr_const, const uint64_t* __restrict__ rng, int* work, float* __restrict__ rast,
     RecordStore rs, int bwl) {
     __shared__ WarpStage s_stage[kWarpsPerCta];
@@ -725,7 +760,7 @@ __global__ void __launch_bounds__(kRecChunk) aux_records_kernel(RecordStore rs, 
 __global__ void __launch_bounds__(kWarpsPerCta * 32) aux_kernel(
     int B, const ds_view_desc* __restrict__ views, int num_tiles, int T, const TriBox* __restrict__ boxes,
     const TriVerts* __restrict__ verts, const TriEdges* __restrict__ edges, const int64_t* __restrict__ offsets,
-    const int* __restrict__ sorted, const int* __restrict__ list, int64_t capacity, int level, int S,
+    const int* __restrict__ sorted, const ListEntry* __restrict__ list, int64_t capacity, int level, int S,
     const float* __restrict__ alpha_src, int C,
     const float* __restrict__ color, const float* __restrict__ target, const float* __restrict__ rast, float scale,
     const int* __restrict__ item_list, const int* __restrict__ item_count, int* work,
@@ -855,11 +890,11 @@ int ds_tiles_bin(int B, const ds_view_desc* views, int num_tiles, int V, const f
     DS_CUDA(cudaMemcpyAsync(w.offsets + num_tiles, total_dev, sizeof(int64_t), cudaMemcpyDeviceToDevice, st));
     if (n > 0)
         bin_fill_kernel<<<blocks_for(n), kThreads, 0, st>>>(B, views, T, w.boxes, w.verts, w.ndc, w.offsets, w.cursor,
-                                                            w.list,
+                                                            w.fill,
                                                             list_capacity, status);
     if (num_tiles > 0)
-        sort_lists_kernel<<<(unsigned)((num_tiles + kWarpsPerCta - 1) / kWarpsPerCta), kWarpsPerCta * 32, 0, st>>>(
-            num_tiles, w.boxes, w.offsets, w.list, list_capacity, w.sorted);
+        sort_lists_kernel<<<(unsigned)((num_tiles + kSortWarps - 1) / kSortWarps), kSortWarps * 32, 0, st>>>(
+            num_tiles, w.offsets, w.fill, w.list, list_capacity, w.sorted);
     return check_launch("tiles_bin");
 }
 
