@@ -39,10 +39,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "fwd+bwd views/s @15K tris 800²: batched BF16 vs plain FP32 on one B200"
-# kernels one training step launches: accumulate+sigmoid x2, project | bin_setup, 3 scan kernels,
-# bin_fill, sort_lists | raster | shade | aux from records, aux of re-enumerated blocks | edge |
-# accumulate+sigmoid backward x2, project backward, finish
-KERNELS_PER_STEP = 18
+# kernels one training step launches (the ncu launch list of the bench shows them): level
+# accumulation + sigmoid (opacity and features in one), project | bin_setup, 3 scan kernels, bin_fill,
+# sort_lists | raster | shade | aux from records, aux of re-enumerated blocks | edge | accumulation
+# adjoint, project backward, finish
+KERNELS_PER_STEP = 16
 WORKLOAD = "config2: 15K-tri sphere-shell soup, 8 views 800x800, levels 0..2 x 8 ch, MLP 11-16-3, stochastic opacity"
 N_INPUT_SETS = 4  # rotating view batches: 4 x 61 MB of targets, larger than the 126 MB L2
 
