@@ -44,6 +44,9 @@ METRIC = "fwd+bwd views/s @15K tris 800²: batched BF16 vs plain FP32 on one B20
 # sort_lists | raster | shade | aux from records, aux of re-enumerated blocks | edge | accumulation
 # adjoint, project backward, finish
 KERNELS_PER_STEP = 16
+# kernels one inference frame launches: project | bin_setup, 3 scan kernels, bin_fill, sort_lists |
+# raster | deferred shade
+RENDER_KERNELS_PER_FRAME = 9
 WORKLOAD = "config2: 15K-tri sphere-shell soup, 8 views 800x800, levels 0..2 x 8 ch, MLP 11-16-3, stochastic opacity"
 N_INPUT_SETS = 4  # rotating view batches: 4 x 61 MB of targets, larger than the 126 MB L2
 
@@ -58,6 +61,8 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-split", dest="split", action="store_false",
                     help="skip timing the split-BF16 precision mode beside the BF16 step")
+    ap.add_argument("--no-render", dest="render", action="store_false",
+                    help="skip timing the inference render (the viewer's frame) beside the training step")
     ap.add_argument("--views", type=int, default=8, help="views per step (8 is the benchmark workload; "
                     "fewer only for small profiling cases)")
     return ap.parse_args()
@@ -383,6 +388,11 @@ def run_ours(args):
     if not args.no_plain and rank == 0:
         plain = run_plain(sc, mlp, sets[0], dev, n_views=16)
 
+    # ---------------- inference render (the viewer's frame) -------------------
+    render = None
+    if rank == 0 and args.render:
+        render = run_render(dev, cpu_sample=not args.no_cpu_baseline)
+
     # ---------------- CPU baseline --------------------------------------------
     cpu_base = None
     if not args.no_cpu_baseline and rank == 0:
@@ -416,6 +426,8 @@ def run_ours(args):
         line["speedup_vs_plain_fp32"] = value / plain["value"]
     if cpu_base is not None:
         line["cpu_baseline"] = cpu_base
+    if render is not None:
+        line["render"] = render
     if rank == 0:
         print(json.dumps(line), flush=True)
     del graphs, egraphs
@@ -498,6 +510,95 @@ def run_plain(sc, mlp, s, dev, n_views: int):
     ms = e0.elapsed_time(e1)
     return {"value": n_views / (ms / 1000.0), "unit": "views/s", "views": n_views,
             "path": "diffsoup_b200 drop-in API, one 800x800 view per call, FP32, eager autograd, torch ColorMLP"}
+
+
+def run_render(dev, cpu_sample: bool = True, frames: int = 200):
+    """The viewer's frame (examples/05_benchmark_fps.py, Viewer::launch_benchmark)
+    on the soup of the training workload: 15K triangles, LUT at level 5, MLP
+    16-16-16-3, 800x800.  Single-view frames as the viewer draws them (one CUDA
+    graph replay each, mean over the 8 cameras), 8 views per call, and the
+    deferred-shading kernel alone on the same G-buffer."""
+    from diffsoup_b200 import _core, scenes, viewer
+
+    vi = scenes.make_viewer_inputs(2, seed=0, level=5)
+    (W1, b1), (W2, b2), (W3, b3) = vi.mlp
+    r = viewer.Renderer(vi.verts, vi.faces, vi.lut0, vi.lut1, W1, b1, W2, b2, W3, b3, level=vi.level, device=dev)
+    H, W, B = vi.height, vi.width, vi.mvps.shape[0]
+    for _ in range(2):
+        r.render(vi.mvps, H, W)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # one view per frame, as the viewer renders
+    f1 = r.frame(vi.mvps[:1], H, W)
+    g1 = f1.capture()
+    per_view = []
+    for b in range(B):
+        f1.set_views(torch.from_numpy(vi.mvps[b:b + 1]))
+        for _ in range(3):
+            g1.replay()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(frames // B):
+            g1.replay()
+        e1.record()
+        e1.synchronize()
+        per_view.append(e0.elapsed_time(e1) / (frames // B))
+    ms1 = sum(per_view) / len(per_view)
+    # all 8 views in one call
+    f8 = r.frame(vi.mvps, H, W)
+    g8 = f8.capture()
+    for _ in range(3):
+        g8.replay()
+    torch.cuda.synchronize()
+    n8 = max(5, frames // B)
+    e0.record()
+    for _ in range(n8):
+        g8.replay()
+    e1.record()
+    e1.synchronize()
+    ms8 = e0.elapsed_time(e1) / n8
+    # the post pass alone on the 8-view G-buffer (inputs: 8 x 640K x 16 B > L2)
+    covered = int((f8.gbuf[:, 3] > 0).sum().item())
+    P = f8.num_pixels
+
+    def post():
+        _core.check(_core.lib.ds_render_deferred(
+            B, _core.ptr(f8.views), P, _core.ptr(f8.gbuf), r.level, _core.ptr(r.lut0), _core.ptr(r.lut1),
+            r.lut0.shape[0], _core.ptr(f8.inv_mvp), _core.ptr(r.mlp), 1.0, 1.0, 1.0, _core.ptr(None),
+            _core.ptr(f8.rgba8), _core.stream()))
+
+    for _ in range(3):
+        post()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(50):
+        post()
+    e1.record()
+    e1.synchronize()
+    post_ms = e0.elapsed_time(e1) / 50
+    alg = 20.0 * P + 24.0 * covered  # G-buffer read + RGBA8 write + 6 texels of 4 B per covered pixel
+    flops = 2.0 * (256 + 256 + 48) * covered
+    out = {"workload": "viewer frame: 15,000 triangles, LUT level 5 (561 texels/face, RGBA8 x 2), "
+                       "MLP 16-16-16-3 with SH2, 800x800, background white",
+           "ms_per_frame": ms1, "fps": 1000.0 / ms1, "ms_per_frame_by_view": [round(t, 4) for t in per_view],
+           "views_per_s_batched": B * 1000.0 / ms8, "views_per_call": B,
+           "post_pass": {"ms_per_8_views": post_ms, "covered_fraction": covered / P,
+                         "achieved_gbs": alg / (post_ms / 1000.0) / 1e9, "fp32_tflops": flops / (post_ms / 1000.0) / 1e12,
+                         "algorithmic_bytes": alg},
+           "gpu_launches_per_frame": RENDER_KERNELS_PER_FRAME}
+    del g1, g8
+    if cpu_sample:
+        from oracle import cpu, viewer as ov
+        t0 = time.perf_counter()
+        pos = cpu.project(vi.verts, vi.mvps[:1])
+        S = r.S
+        alpha = (vi.lut1.reshape(-1, 4)[:, 3].astype(np.float32) / np.float32(255))[:r.T * S].reshape(r.T, S)
+        g, _ = cpu.rasterize_alpha(H, W, pos, vi.faces, vi.level, alpha, False)
+        inv = np.linalg.inv(vi.mvps[:1].astype(np.float64)).astype(np.float32)
+        ov.to_rgba8(ov.post_pass(g, inv, vi.level, vi.lut0, vi.lut1, [a for wb in vi.mlp for a in wb]))
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"fps": 1.0 / dt, "cores": cpu.omp_threads(), "kind": "port",
+                               "sample": "1 frame of view 0: oracle rasterizer (OpenMP) + numpy FP64 post pass"}
+    return out
 
 
 def run_cpu_baseline(sc, mlp, s):

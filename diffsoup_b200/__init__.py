@@ -4,13 +4,15 @@ Drop-in for the rasterize/shade API of kenji-tojo/diffsoup
 (python/diffsoup/__init__.py:11-25): the same public names with the same
 signatures and tensor layouts, backed by hand-written sm_100a kernels in
 libdiffsoup_b200.so.  `step` adds the batched, graph-captured training step,
-`optimize` the fused VectorAdam / Adam updates that follow it.
+`optimize` the fused VectorAdam / Adam updates that follow it, `viewer` the
+headless inference render of the viewer's deferred shading.
 """
 
 from __future__ import annotations
 
 from . import _core
 from . import optimize
+from . import viewer
 from . import visibility
 from ._core import __version__
 from .rasterize import (

@@ -34,6 +34,16 @@ int check_launch(const char* what);
             return ::dsb::set_error(DS_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
     } while (0)
 
+// View of a packed pixel index: the last view whose pix_offset <= p.
+__device__ __forceinline__ int view_of_pixel(const ds_view_desc* __restrict__ views, int B, int64_t p) {
+    int lo = 0, hi = B - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&views[mid].pix_offset) <= p) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
 // ---------------------------------------------------------------------------
 // FP32 arithmetic with the rounding of the reference's default nvcc build.
 //

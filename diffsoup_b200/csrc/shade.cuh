@@ -107,15 +107,6 @@ struct ShadeArgs {
     double* loss_sum;             // [1], accumulates sum of squared errors
 };
 
-__device__ __forceinline__ int view_of_pixel(const ds_view_desc* __restrict__ views, int B, int64_t p) {
-    int lo = 0, hi = B - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (__ldg(&views[mid].pix_offset) <= p) lo = mid; else hi = mid - 1;
-    }
-    return lo;
-}
-
 // bf16 planes of two values: hi = bf16(v), lo = bf16(v - hi).
 __device__ __forceinline__ void split_bf16(float v0, float v1, uint32_t& hi, uint32_t& lo) {
     const __nv_bfloat162 h = __floats2bfloat162_rn(v0, v1);

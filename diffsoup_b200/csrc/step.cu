@@ -618,6 +618,15 @@ int ds_train_step_layout(const ds_step_config* cfg, int num_tiles, int64_t num_p
     return DS_OK;
 }
 
+int ds_project_vertices(int B, int V, const float* verts, const float* mvp, float* pos, ds_stream_t stream) {
+    DS_CHECK_ARG(B >= 0 && V >= 0 && (int64_t)B * V <= 0x7fffffff, "project_vertices: bad sizes");
+    DS_CHECK_ARG((int64_t)B * V == 0 || (verts && mvp && pos), "project_vertices: null pointer");
+    DS_CHECK_ARG(((uintptr_t)pos & 15) == 0, "project_vertices: pos not 16-byte aligned");
+    if ((int64_t)B * V == 0) return DS_OK;
+    project_kernel<<<blocks_for((int64_t)B * V), kThreads, 0, (cudaStream_t)stream>>>(B, V, verts, mvp, pos);
+    return check_launch("project_vertices");
+}
+
 int ds_mlp_param_count(int C, int hidden, int n_layers) {
     const int in = C + 3;
     return hidden * in + hidden + (n_layers - 1) * (hidden * hidden + hidden) + 3 * hidden + 3;

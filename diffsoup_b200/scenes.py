@@ -264,3 +264,48 @@ def mlp_weights(in_dim: int, out_dim: int, hidden: int, n_layers: int, seed: int
             bound = np.sqrt(6.0 / (fi + fo))
         out.append((rng.uniform(-bound, bound, size=(fo, fi)).astype(np.float32), np.zeros(fo, dtype=np.float32)))
     return out
+
+
+@dataclass
+class ViewerInputs:
+    """A soup as the viewer takes it (examples/05_benchmark_fps.py:290-375):
+    vertices, faces, the RGBA8 LUT pair at `level`, MLP 16 -> 16 -> 16 -> 3
+    and row-major MVPs of its views."""
+
+    verts: np.ndarray  # (V,3) float32
+    faces: np.ndarray  # (T,3) int32
+    lut0: np.ndarray  # (tex_h, tex_w, 4) uint8
+    lut1: np.ndarray  # (tex_h, tex_w, 4) uint8
+    mlp: List[Tuple[np.ndarray, np.ndarray]]
+    mvps: np.ndarray  # (B,4,4) float32 row-major
+    height: int
+    width: int
+    level: int
+
+
+def make_viewer_inputs(config: int = 2, seed: int = 0, *, level: int = 5, num_tris: Optional[int] = None,
+                       num_views: Optional[int] = None, resolution: Optional[Tuple[int, int]] = None) -> ViewerInputs:
+    """Synthetic stand-in for a trained checkpoint rendered by the viewer: the
+    soup and cameras of configuration `config`, per-texel features U[0,1]
+    (7 channels) and opacities sigmoid(N(0.5, 2)) at `level`, packed and
+    quantised to RGBA8 as 05_benchmark_fps.py:56-80 and :315-317 do, and a
+    16 -> 16 -> 16 -> 3 ColorMLP with random biases."""
+    sc = make_scene(config, seed, num_tris=num_tris, num_views=num_views, resolution=resolution, with_targets=False)
+    hw = sc.uniform_resolution
+    assert hw is not None, "the viewer renders views of one resolution"
+    rng = np.random.default_rng(np.random.PCG64(seed * 7 + 104729))
+    S = total_feats(level, level)
+    N = sc.T * S
+    feat = rng.uniform(0.0, 1.0, size=(N, 7)).astype(np.float32)
+    alpha = (1.0 / (1.0 + np.exp(-rng.normal(0.5, 2.0, size=(N, 1))))).astype(np.float32)
+    tex_w = min(4096, N)
+    tex_h = -(-N // tex_w)
+    lut = np.zeros((tex_h * tex_w, 8), np.float32)
+    lut[:N, :7] = feat
+    lut[:N, 7:] = alpha
+    lut = lut.reshape(tex_h, tex_w, 8)
+    lut0 = (lut[..., :4] * 255).clip(0, 255).astype(np.uint8)
+    lut1 = (lut[..., 4:] * 255).clip(0, 255).astype(np.uint8)
+    mlp = mlp_weights(16, 3, 16, 2, seed=seed)
+    mlp = [(W, rng.normal(0.0, 0.1, size=b.shape).astype(np.float32)) for W, b in mlp]
+    return ViewerInputs(sc.verts, sc.tri, lut0, lut1, mlp, sc.mvps(), hw[0], hw[1], level)

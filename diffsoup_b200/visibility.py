@@ -18,9 +18,14 @@ from . import tiles as _tiles
 
 
 def project_vertices(V: torch.Tensor, MVPs: torch.Tensor) -> torch.Tensor:
-    """Clip-space positions [B, Nv, 4] (examples/utils.py:412-426)."""
-    vh = torch.cat([V, torch.ones_like(V[:, :1])], dim=-1)
-    return torch.einsum("bij,nj->bni", MVPs, vh).contiguous()
+    """Clip-space positions [B, Nv, 4] = MVPs[b] . (V, 1) (examples/utils.py:
+    412-426), by the projection kernel of the training step."""
+    V = V.float().contiguous()
+    M = MVPs.float().contiguous()
+    out = torch.empty(M.shape[0], V.shape[0], 4, dtype=torch.float32, device=V.device)
+    _core.check(_core.lib.ds_project_vertices(M.shape[0], V.shape[0], _core.ptr(V), _core.ptr(M), _core.ptr(out),
+                                              _core.stream()))
+    return out
 
 
 def count_visible_triangles(resolution: Tuple[int, int], MVPs: torch.Tensor, V: torch.Tensor, F: torch.Tensor,

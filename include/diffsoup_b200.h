@@ -324,6 +324,57 @@ int ds_adam_step(float* param, const float* grad, float* exp_avg, float* exp_avg
 int ds_vector_adam_step(float* param, const float* grad, float* g1, float* g2, int64_t rows, int dim, double lr,
                         double beta1, double beta2, int* step, ds_stream_t stream);
 
+/* Clip-space positions pos [B,V,4] = mvp[b] . (verts[v], 1) with mvp [B,4,4]
+ * row-major (project_vertices, examples/utils.py:412-426; the training step
+ * projects with the same kernel).  pos 16-byte aligned. */
+int ds_project_vertices(int B, int V, const float* verts, const float* mvp, float* pos, ds_stream_t stream);
+
+/* ===================================================================== */
+/*  Inference render: the viewer's deferred shading without a window      */
+/* ===================================================================== */
+
+/* The LUT is the viewer's pair of RGBA8 textures (viewer/src/viewer.cpp:
+ * 549-554, packed by examples/05_benchmark_fps.py:56-80 and :315-317):
+ * texel t = face * S + lattice index at `level` (S = texels per face),
+ * lut0[t] = 255 * (f0, f1, f2, f3), lut1[t] = 255 * (f4, f5, f6, opacity),
+ * num_texels >= T * S (the texture may be padded).  mlp_params packs
+ * W1 [16,16], b1 [16], W2 [16,16], b2 [16], W3 [3,16], b3 [3] (torch Linear
+ * layout [out, in]; 595 floats). */
+
+/* Opacity channel as FP32 for the geometry pass: alpha[t] = lut1[t].a / 255
+ * for t < num_texels (the texture fetch of viewer.cpp:228, UNORM8 decode). */
+int ds_render_lut_opacity(int64_t num_texels, const unsigned char* lut1, float* alpha, ds_stream_t stream);
+
+/* Post pass of viewer.cpp:241-341 over a G-buffer gbuf [num_pixels,4] in the
+ * rasterizer's layout (b0, b1, z/w, triangle id + 1; id 0 = empty): LUT
+ * interpolation at the fragment's lattice cell (viewer.cpp:197-230), view
+ * direction through inv_mvp [B,16] at the pixel centre, SH2 encoding, MLP
+ * 16 -> 16 -> 16 -> 3 and mix(A.rgb, mlp, A.a); empty pixels take the
+ * background.  Writes rgb [num_pixels,3] FP32 and/or rgba8 [num_pixels,4]
+ * (either may be NULL, not both). */
+int ds_render_deferred(int B, const ds_view_desc* views, int64_t num_pixels, const float* gbuf, int level,
+                       const unsigned char* lut0, const unsigned char* lut1, int64_t num_texels,
+                       const float* inv_mvp, const float* mlp_params, float bg_r, float bg_g, float bg_b,
+                       float* rgb, unsigned char* rgba8, ds_stream_t stream);
+
+/* Bytes of workspace for ds_render_frame. */
+size_t ds_render_workspace_size(int B, int V, int T, int num_tiles, int64_t list_capacity);
+
+/* One frame of the viewer (replaces Viewer::launch_benchmark's render_one,
+ * viewer/src/viewer.cpp:861-909, and Viewer::render, :663-720) for B views:
+ * projection of verts [V,3] by mvp [B,4,4] row-major, screen-tile binning,
+ * the geometry pass (nearest fragment whose LUT opacity alpha [T,S] -- from
+ * ds_render_lut_opacity -- is at least 0.5; triangle ID buffer into gbuf)
+ * and the post pass of ds_render_deferred.  Never host-synchronising and
+ * capturable in a CUDA graph; a bin list overflow sets DS_STATUS_LIST_OVERFLOW
+ * in *status and stays exact (ds_tiles_bin). */
+int ds_render_frame(int B, const ds_view_desc* views, int num_tiles, int64_t num_pixels, int V, const float* verts,
+                    int T, const int* faces, const float* mvp, const float* inv_mvp, int level,
+                    const unsigned char* lut0, const unsigned char* lut1, int64_t num_texels, const float* alpha,
+                    const float* mlp_params, float bg_r, float bg_g, float bg_b, float* gbuf, float* rgb,
+                    unsigned char* rgba8, void* workspace, size_t workspace_bytes, int64_t list_capacity,
+                    int* status, ds_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
