@@ -528,7 +528,8 @@ def run_render(dev, cpu_sample: bool = True, frames: int = 200):
         r.render(vi.mvps, H, W)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     # one view per frame, as the viewer renders
-    f1 = r.frame(vi.mvps[:1], H, W)
+    for b in range(B):  # a bin-list capacity that fits every single view
+        f1 = r.frame(vi.mvps[b:b + 1], H, W)
     g1 = f1.capture()
     per_view = []
     for b in range(B):

@@ -147,23 +147,14 @@ class Renderer:
             _core.check(_core.lib.ds_render_lut_opacity(self.lut1.shape[0], _core.ptr(self.lut1),
                                                         _core.ptr(self.alpha), _core.stream()))
         self._frames: Dict[Tuple, "_Frame"] = {}
-        self.capacity = max(1 << 16, 8 * self.T)
-        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
 
     # -- one frame --------------------------------------------------------
     def _frame(self, B: int, H: int, W: int) -> "_Frame":
-        key = (B, H, W, self.capacity)
-        f = self._frames.get(key)
+        f = self._frames.get((B, H, W))
         if f is None:
             f = _Frame(self, B, H, W)
-            self._frames = {k: v for k, v in self._frames.items() if k[:3] != (B, H, W)}
-            self._frames[key] = f
+            self._frames[(B, H, W)] = f
         return f
-
-    def _grow_if_overflowed(self) -> None:
-        if int(self.status.item()) & _tiles.DS_STATUS_LIST_OVERFLOW:
-            self.capacity = min(2 * self.capacity, 0x7FFFFFFF)
-            self.status.zero_()
 
     def render(self, mvps, height: int, width: int, rgb: bool = False, gbuf: bool = False):
         """Frames of views mvps [B,4,4] (row-major, clip = mvp . (v, 1)) at
@@ -173,9 +164,11 @@ class Renderer:
         m = torch.as_tensor(mvps, dtype=torch.float32).reshape(-1, 4, 4)
         f = self._frame(m.shape[0], int(height), int(width))
         f.set_views(m)
+        f.status.zero_()
         f.run(want_rgb=rgb)
         torch.cuda.current_stream(self.device).synchronize()
-        self._grow_if_overflowed()
+        if f.overflowed():
+            f.grow()  # this frame is exact all the same; the next ones bin without overflow
         out = [f.rgba8.view(f.B, f.H, f.W, 4).clone()]
         if rgb:
             out.append(f.rgb.view(f.B, f.H, f.W, 3).clone())
@@ -184,18 +177,25 @@ class Renderer:
         return out[0] if len(out) == 1 else tuple(out)
 
     def frame(self, mvps, height: int, width: int) -> "_Frame":
-        """The resident frame for these views, inputs set, for replaying (its
-        `run()` launches the whole frame; `capture()` returns a CUDA graph of
-        it)."""
+        """The resident frame for these views, inputs set and its bin-list
+        capacity fitted to them, for replaying (its `run()` launches the whole
+        frame; `capture()` returns a CUDA graph of it)."""
         m = torch.as_tensor(mvps, dtype=torch.float32).reshape(-1, 4, 4)
         f = self._frame(m.shape[0], int(height), int(width))
         f.set_views(m)
+        f.fit()
         return f
 
 
 class _Frame:
     """Device buffers of one batch shape: view table, MVPs, G-buffer, outputs
-    and the binning workspace."""
+    and the binning workspace.
+
+    The number of (triangle, tile) bin entries depends on the views.  The
+    workspace holds `capacity` of them (first 8 per triangle and view); a
+    frame whose lists do not fit sets DS_STATUS_LIST_OVERFLOW and is still
+    exact (its overflowing tiles test every triangle, slowly), and `fit()` /
+    `grow()` double the capacity until the lists fit."""
 
     def __init__(self, r: Renderer, B: int, H: int, W: int):
         self.r, self.B, self.H, self.W = r, B, H, W
@@ -207,10 +207,37 @@ class _Frame:
             self.gbuf = torch.empty(self.num_pixels, 4, dtype=torch.float32, device=dev)
             self.rgb = torch.empty(self.num_pixels, 3, dtype=torch.float32, device=dev)
             self.rgba8 = torch.empty(self.num_pixels, 4, dtype=torch.uint8, device=dev)
-            self.capacity = r.capacity
-            nbytes = _core.lib.ds_render_workspace_size(B, r.V, r.T, self.num_tiles, self.capacity)
-            self.workspace = _core.workspace(nbytes, dev)
-        self._want_rgb = False
+            self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.capacity = max(1 << 16, 8 * B * r.T)
+        self._alloc()
+
+    def _alloc(self) -> None:
+        nbytes = _core.lib.ds_render_workspace_size(self.B, self.r.V, self.r.T, self.num_tiles, self.capacity)
+        self.workspace = None
+        self.workspace = _core.workspace(nbytes, self.r.device)
+
+    def overflowed(self) -> bool:
+        return bool(int(self.status.item()) & _tiles.DS_STATUS_LIST_OVERFLOW)
+
+    def grow(self) -> None:
+        """Doubles the bin-list capacity (a new workspace: graphs captured
+        before hold the old one)."""
+        if self.capacity >= 0x7FFFFFFF:
+            raise RuntimeError("render: bin-list capacity exceeds the int32 range")
+        self.capacity = min(2 * self.capacity, 0x7FFFFFFF)
+        self._alloc()
+
+    def fit(self) -> None:
+        """Eager frames of the current views, doubling the capacity until no
+        bin list overflows."""
+        for _ in range(24):
+            self.status.zero_()
+            self.run()
+            torch.cuda.current_stream(self.r.device).synchronize()
+            if not self.overflowed():
+                return
+            self.grow()
+        raise RuntimeError("render: bin-list capacity did not converge")
 
     def set_views(self, mvps: torch.Tensor) -> None:
         """Row-major MVPs [B,4,4] and their inverses (FP64 on the host, then
@@ -228,7 +255,7 @@ class _Frame:
             _core.ptr(r.faces), _core.ptr(self.mvp), _core.ptr(self.inv_mvp), r.level, _core.ptr(r.lut0),
             _core.ptr(r.lut1), r.lut0.shape[0], _core.ptr(r.alpha), _core.ptr(r.mlp), bg[0], bg[1], bg[2],
             _core.ptr(self.gbuf), _core.ptr(self.rgb) if want_rgb else _core.ptr(None), _core.ptr(self.rgba8),
-            _core.ptr(self.workspace), self.workspace.numel(), self.capacity, _core.ptr(r.status), _core.stream()))
+            _core.ptr(self.workspace), self.workspace.numel(), self.capacity, _core.ptr(self.status), _core.stream()))
 
     def capture(self) -> torch.cuda.CUDAGraph:
         """A CUDA graph of one frame (RGBA8 output), reading the MVPs from
@@ -279,12 +306,12 @@ def benchmark(verts, faces, lut0, lut1, W1, b1, W2, b2, W3, b3, mvps, width: int
     m_row = np.ascontiguousarray(np.transpose(m_col, (0, 2, 1)))
     r = Renderer(verts, faces, lut0, lut1, W1, b1, W2, b2, W3, b3, level=level)
     H, W = int(height), int(width)
-    f = r.frame(m_row[:1], H, W)
+    for i in range(m_row.shape[0]):  # bin-list capacity that fits every view
+        f = r.frame(m_row[i:i + 1], H, W)
+    f.set_views(torch.from_numpy(m_row[:1]))
     for _ in range(max(int(warmup), 1)):
         f.run()
     torch.cuda.synchronize()
-    r._grow_if_overflowed()
-    f = r.frame(m_row[:1], H, W)
     graph = f.capture()
     times: List[float] = []
     out_dir = os.path.join(os.path.abspath(output_dir), "")

@@ -114,3 +114,16 @@ def test_benchmark_writes_viewer_outputs(inputs, tmp_path):
     assert shots == ["benchmark_00000.png", "benchmark_00002.png"]
     with open(os.path.join(tmp_path, "screenshots", shots[0]), "rb") as fh:
         assert fh.read(8) == b"\x89PNG\r\n\x1a\n"
+
+
+def test_bin_list_overflow_stays_exact(renderer, inputs):
+    H, W = inputs.height, inputs.width
+    want = renderer.render(inputs.mvps, H, W)
+    f = renderer._frame(inputs.mvps.shape[0], H, W)
+    f.capacity = 4096  # far fewer (triangle, tile) entries than the views need
+    f._alloc()
+    got = renderer.render(inputs.mvps, H, W)
+    assert torch.equal(got, want)
+    assert f.capacity == 8192  # grown after the overflowing frame
+    f.fit()
+    assert not f.overflowed()
