@@ -329,7 +329,7 @@ __global__ void __launch_bounds__(kThreads) project_backward_kernel(int B, int V
 // of equal triangles before one FP64 atomic per vertex component.
 constexpr int kEdgeThreads = DS_TILE * DS_TILE;
 #ifndef DSB_EDGE_MIN_CTAS
-#define DSB_EDGE_MIN_CTAS 3  // resident 8-warp CTAs per SM the register budget is sized for
+#define DSB_EDGE_MIN_CTAS 4  // resident 8-warp CTAs per SM the register budget is sized for (64 registers)
 #endif
 
 __device__ __forceinline__ int tile_view(const ds_view_desc* __restrict__ views, int B, int tile) {

@@ -567,7 +567,7 @@ __device__ __noinline__ void flush_records(const RecordStore& rs, WarpRecs& R, i
 // bound at every point of the walk, so the walk meets and keeps all of them;
 // at the end of the block those behind the final surface are dropped.
 #ifndef DSB_RASTER_MIN_CTAS
-#define DSB_RASTER_MIN_CTAS 4  // resident 8-warp CTAs per SM the register budget is sized for
+#define DSB_RASTER_MIN_CTAS 5  // resident 8-warp CTAs per SM the register budget is sized for (48 registers)
 #endif
 
 template <bool REC>
