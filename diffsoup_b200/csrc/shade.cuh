@@ -263,6 +263,22 @@ __global__ void __launch_bounds__(K::WARPS * 32, K::REG_GRADS ? DSB_SHADE_MIN_CT
             view_direction(pix_ndc(px, vd.W), pix_ndc(py, vd.H), M, d);
             x[K::C + 0] = d[0]; x[K::C + 1] = d[1]; x[K::C + 2] = d[2];
         }
+        if (!__any_sync(0xffffffffu, mask)) {
+            // no covered pixel in the chunk: background colour 1, no MLP and no gradients
+            if (valid) {
+                float l1 = 0.f;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const float diff = 1.f - a.target[p * 3 + c];
+                    loss_acc += diff * diff;
+                    a.color[p * 3 + c] = 1.f;
+                    a.grad_color[p * 3 + c] = 2.f * diff * a.inv_n;
+                    l1 += fabsf(diff);
+                }
+                a.l1[p] = l1;
+            }
+            continue;
+        }
         {
             // 16-byte stores: rows are 16-byte aligned and, at these strides,
             // the 8 lanes of each store phase hit distinct bank groups

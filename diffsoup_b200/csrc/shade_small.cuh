@@ -150,37 +150,41 @@ __global__ void __launch_bounds__(kShadeSmallWarps * 32, DSB_SHADE_SMALL_MIN_CTA
             view_direction(pix_ndc(px, vd.W), pix_ndc(py, vd.H), M, d);
             x[8] = d[0]; x[9] = d[1]; x[10] = d[2];
         }
-        {
-            __nv_bfloat16* xr = ws.X + lane * 24;
-            *reinterpret_cast<uint4*>(xr) =
-                make_uint4(pack_bf16(x[0], x[1]), pack_bf16(x[2], x[3]), pack_bf16(x[4], x[5]), pack_bf16(x[6], x[7]));
-            *reinterpret_cast<uint4*>(xr + 8) = make_uint4(pack_bf16(x[8], x[9]), pack_bf16(x[10], 0.f), 0u, 0u);
-        }
-        __syncwarp();
-
-        // ---------------- MLP forward (activations in registers) ------------------
+        // a chunk without covered pixels has an all-background colour: no MLP, no gradients
+        const bool any = __any_sync(0xffffffffu, mask);
         uint32_t aH[2][4];  // relu(X W0^T + b0) as bf16, A operand of the next products
+        if (any) {
+            {
+                __nv_bfloat16* xr = ws.X + lane * 24;
+                *reinterpret_cast<uint4*>(xr) = make_uint4(pack_bf16(x[0], x[1]), pack_bf16(x[2], x[3]),
+                                                           pack_bf16(x[4], x[5]), pack_bf16(x[6], x[7]));
+                *reinterpret_cast<uint4*>(xr + 8) = make_uint4(pack_bf16(x[8], x[9]), pack_bf16(x[10], 0.f), 0u, 0u);
+            }
+            __syncwarp();
+
+            // ---------------- MLP forward (activations in registers) ------------------
 #pragma unroll
-        for (int mt = 0; mt < 2; ++mt) {
-            uint32_t aX[4];
-            load_a(aX, ws.X, 24, mt * 16, 0);
+            for (int mt = 0; mt < 2; ++mt) {
+                uint32_t aX[4];
+                load_a(aX, ws.X, 24, mt * 16, 0);
 #pragma unroll
-            for (int nt = 0; nt < 2; ++nt) {
+                for (int nt = 0; nt < 2; ++nt) {
+                    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+                    mma_16816(acc, aX, bW0[nt]);
+                    aH[mt][2 * nt] = pack_bf16(fmaxf(acc[0] + bb0[nt][0], 0.f), fmaxf(acc[1] + bb0[nt][1], 0.f));
+                    aH[mt][2 * nt + 1] = pack_bf16(fmaxf(acc[2] + bb0[nt][0], 0.f), fmaxf(acc[3] + bb0[nt][1], 0.f));
+                }
                 float acc[4] = {0.f, 0.f, 0.f, 0.f};
-                mma_16816(acc, aX, bW0[nt]);
-                aH[mt][2 * nt] = pack_bf16(fmaxf(acc[0] + bb0[nt][0], 0.f), fmaxf(acc[1] + bb0[nt][1], 0.f));
-                aH[mt][2 * nt + 1] = pack_bf16(fmaxf(acc[2] + bb0[nt][0], 0.f), fmaxf(acc[3] + bb0[nt][1], 0.f));
+                mma_16816(acc, aH[mt], bWo);
+                if (q < 2) {  // logits of outputs 2q, 2q+1 for rows g, g+8
+                    ws.scr[(mt * 16 + g) * 17 + 2 * q] = acc[0];
+                    ws.scr[(mt * 16 + g) * 17 + 2 * q + 1] = acc[1];
+                    ws.scr[(mt * 16 + g + 8) * 17 + 2 * q] = acc[2];
+                    ws.scr[(mt * 16 + g + 8) * 17 + 2 * q + 1] = acc[3];
+                }
             }
-            float acc[4] = {0.f, 0.f, 0.f, 0.f};
-            mma_16816(acc, aH[mt], bWo);
-            if (q < 2) {  // logits of outputs 2q, 2q+1 for rows g, g+8
-                ws.scr[(mt * 16 + g) * 17 + 2 * q] = acc[0];
-                ws.scr[(mt * 16 + g) * 17 + 2 * q + 1] = acc[1];
-                ws.scr[(mt * 16 + g + 8) * 17 + 2 * q] = acc[2];
-                ws.scr[(mt * 16 + g + 8) * 17 + 2 * q + 1] = acc[3];
-            }
+            __syncwarp();
         }
-        __syncwarp();
 
         // ---------------- blend, loss, dL/dcolour (lane = pixel) ------------------
         float dz[3] = {0.f, 0.f, 0.f};
@@ -191,7 +195,7 @@ __global__ void __launch_bounds__(kShadeSmallWarps * 32, DSB_SHADE_SMALL_MIN_CTA
             float l1 = 0.f;
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                const float s = 1.f / (1.f + expf(-(ws.scr[lane * 17 + c] + bo[c])));
+                const float s = mask ? 1.f / (1.f + expf(-(ws.scr[lane * 17 + c] + bo[c]))) : 0.f;
                 const float col = mask ? (1.f - res) * x[c] + res * s : 1.f;
                 const float diff = col - tgt[c];
                 loss_acc += diff * diff;
@@ -210,6 +214,7 @@ __global__ void __launch_bounds__(kShadeSmallWarps * 32, DSB_SHADE_SMALL_MIN_CTA
 #pragma unroll
         for (int c = 0; c < 3; ++c) gbo[c] += dz[c];
         __syncwarp();  // scr is rewritten below
+        if (!any) continue;
 
         // ---------------- MLP backward --------------------------------------------
         // dZo as an A operand: rows g, g+8 of each m-tile; outputs 2q, 2q+1 (q < 2)

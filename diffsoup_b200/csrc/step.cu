@@ -382,6 +382,7 @@ __global__ void __launch_bounds__(kEdgeThreads, DSB_EDGE_MIN_CTAS) edge_step_ker
     const int it0 = edge_grad_pixel_staged(h, (ly + 1) * kHaloW + lx + 1, y, x, vd.H, vd.W,
                                            tab.verts + (size_t)b * T, acc);
     const int key = (it0 >= 0 && acc.any) ? it0 : -1 - lane;
+    if (__ballot_sync(0xffffffffu, key >= 0) == 0) return;  // no lane of the warp has a contribution
     const int prev = __shfl_up_sync(0xffffffffu, key, 1);
     const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || prev != key);
     const int seg = __popc(heads & ((2u << lane) - 1u));
