@@ -284,9 +284,65 @@ __global__ void __launch_bounds__(kThreads) bin_fill_kernel(int B, const ds_view
     if (over) atomicOr(status, DS_STATUS_LIST_OVERFLOW);
 }
 
+// Bitonic network over the R * 32 (key, position) pairs of a warp, element
+// e = s * 32 + lane in register slot s, ascending.  Partners 32 or more apart
+// sit in the same lane (a compare-exchange between two slots), nearer ones in
+// the same slot of another lane (a shuffle).
+template <int R>
+__device__ __forceinline__ void warp_bitonic(float (&key)[R], int (&pos)[R], int lane) {
+#pragma unroll
+    for (int k = 2; k <= R * 32; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            if (j >= 32) {
+#pragma unroll
+                for (int s = 0; s < R; ++s) {
+                    const int t = s ^ (j >> 5);
+                    if (t > s) {
+                        const bool up = ((s * 32 + lane) & k) == 0;  // the lower element keeps the smaller key
+                        if ((key[s] > key[t]) == up && key[s] != key[t]) {
+                            const float kk = key[s]; key[s] = key[t]; key[t] = kk;
+                            const int pp = pos[s]; pos[s] = pos[t]; pos[t] = pp;
+                        }
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int s = 0; s < R; ++s) {
+                    const float ok = __shfl_xor_sync(0xffffffffu, key[s], j);
+                    const int op = __shfl_xor_sync(0xffffffffu, pos[s], j);
+                    const bool up = ((s * 32 + lane) & k) == 0, lower = (lane & j) == 0;
+                    const bool take = (lower == up) ? (ok < key[s]) : (ok > key[s]);
+                    if (take) { key[s] = ok; pos[s] = op; }
+                }
+            }
+        }
+    }
+}
+
+// Sorts the n <= R * 32 entries of F by zlo into L (register network, one
+// gather per entry).
+template <int R>
+__device__ __forceinline__ void sort_in_registers(const int4* __restrict__ F, int4* __restrict__ L, int n, int lane) {
+    float key[R];
+    int pos[R];
+#pragma unroll
+    for (int s = 0; s < R; ++s) {
+        const int e = s * 32 + lane;
+        key[s] = e < n ? fminf(__int_as_float(F[e].z), 3.0e38f) : INFINITY;  // real keys stay below the padding
+        pos[s] = e;
+    }
+    warp_bitonic<R>(key, pos, lane);
+#pragma unroll
+    for (int s = 0; s < R; ++s) {
+        const int e = s * 32 + lane;
+        if (e < n) L[e] = F[pos[s]];
+    }
+}
+
 // Pass 3: each tile's list ordered by zlo, from the fill pass's lists into
 // the rasterizer's (warp per tile): the (key, position) pairs are sorted by a
-// bitonic network in registers (up to 32 entries) or in shared memory (up to
+// bitonic network in registers (up to 128 entries) or in shared memory (up to
 // kSortMax), and each entry is then gathered once.  Longer lists are copied
 // as they are and marked unsorted; lists cut by the capacity are not used.
 __global__ void __launch_bounds__(kSortWarps * 32) sort_lists_kernel(int num_tiles,
@@ -340,7 +396,13 @@ __global__ void __launch_bounds__(kSortWarps * 32) sort_lists_kernel(int num_til
         if (lane == 0) sorted[tile] = 1;
         return;
     }
-    int size = 64;
+    if (n <= 128) {
+        if (n <= 64) sort_in_registers<2>(F, L, n, lane);
+        else sort_in_registers<4>(F, L, n, lane);
+        if (lane == 0) sorted[tile] = 1;
+        return;
+    }
+    int size = 256;
     while (size < n) size <<= 1;
     float* key = s_key[warp];
     short* pos = s_pos[warp];
