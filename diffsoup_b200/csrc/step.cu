@@ -202,11 +202,16 @@ __global__ void __launch_bounds__(kTabWarps * 32) accum_tab_kernel(int T, int lo
                                                                    const float* __restrict__ feat_src,
                                                                    float* __restrict__ alpha_out,
                                                                    float* __restrict__ feat_out,
-                                                                   __nv_bfloat16* __restrict__ feat_bf16) {
+                                                                   __nv_bfloat16* __restrict__ feat_bf16,
+                                                                   uint4* __restrict__ tab_out) {
     extern __shared__ __align__(16) unsigned char tab_smem[];
     const int NE = (hi - lo + 1) * 3;
     const LatticeTab L = lattice_tab_at(tab_smem, ST * NE, S);
     build_lattice_tab(L, lo, hi, ST, S);
+    if (blockIdx.x == 0) {  // the tables for the adjoint kernel of this step
+        const uint4* src = reinterpret_cast<const uint4*>(tab_smem);
+        for (int i = threadIdx.x; i < (int)(lattice_tab_bytes(ST * NE, S) / 16); i += blockDim.x) tab_out[i] = src[i];
+    }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float* sa = reinterpret_cast<float*>(tab_smem + lattice_tab_bytes(ST * NE, S)) + (size_t)warp * S * (C + 1);
     float* sf = sa + S;
@@ -232,16 +237,22 @@ __global__ void __launch_bounds__(kTabWarps * 32) accum_tab_kernel(int T, int lo
 }
 
 // Adjoint of accum_tab_kernel: grad_src[t][d] = sum over the targets k that
-// read d of w * grad_out[t][k] * s (1 - s); a gather, written once.
+// read d of w * grad_out[t][k] * s (1 - s); a gather, written once.  The
+// tables are the ones the forward kernel of the step built (copied, not
+// rebuilt: this kernel sits on the step's critical path).
 template <int C>
 __global__ void __launch_bounds__(kTabWarps * 32) accum_tab_backward_kernel(
     int T, int lo, int hi, int S, int ST, const float* __restrict__ alpha_sig, const float* __restrict__ alpha_grad,
     const float* __restrict__ feat_sig, const float* __restrict__ feat_grad, float* __restrict__ alpha_src_grad,
-    float* __restrict__ feat_src_grad) {
+    float* __restrict__ feat_src_grad, const uint4* __restrict__ tab_in) {
     extern __shared__ __align__(16) unsigned char tab_smem[];
     const int NE = (hi - lo + 1) * 3;
     const LatticeTab L = lattice_tab_at(tab_smem, ST * NE, S);
-    build_lattice_tab(L, lo, hi, ST, S);
+    {
+        uint4* dst = reinterpret_cast<uint4*>(tab_smem);
+        for (int i = threadIdx.x; i < (int)(lattice_tab_bytes(ST * NE, S) / 16); i += blockDim.x) dst[i] = tab_in[i];
+        __syncthreads();
+    }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float* ga = reinterpret_cast<float*>(tab_smem + lattice_tab_bytes(ST * NE, S)) + (size_t)warp * ST * (C + 1);
     float* gf = ga + ST;
@@ -519,6 +530,7 @@ struct StepWs {
     float* color;
     float* grad_color;
     float* l1;
+    uint4* tab;         // lattice tables of the level accumulation, from its forward kernel
     double* grad_pos;
     float* grad_alpha_acc;
     float* grad_feat_acc;
@@ -552,6 +564,9 @@ static StepWs carve_step(void* ws, const ds_step_config& c, int num_tiles, int64
     w.color = reinterpret_cast<float*>(base + o); o += al((size_t)P * 12);
     w.grad_color = reinterpret_cast<float*>(base + o); o += al((size_t)P * 12);
     w.l1 = reinterpret_cast<float*>(base + o); o += al((size_t)P * 4);
+    w.tab = reinterpret_cast<uint4*>(base + o);
+    o += al(lattice_tab_bytes(ST * (c.max_level - c.min_level + 1) * 3,
+                              (int)total_feats((uint32_t)c.min_level, (uint32_t)c.max_level)));
     // zeroed together each step: grad_pos .. loss_sum
     w.grad_pos = reinterpret_cast<double*>(base + o); o += al((size_t)c.B * c.V * 32);
     w.grad_alpha_acc = reinterpret_cast<float*>(base + o); o += al((size_t)c.T * ST * 4);
@@ -680,13 +695,17 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     const size_t tsm = lattice_tab_smem(c.min_level, c.max_level, S, ST, c.C);
     const int64_t tw = ((int64_t)c.T + kTabWarps - 1) / kTabWarps;
     const unsigned tgrid = (unsigned)(tw < kSMs * 4 ? tw : kSMs * 4);  // persistent: tables built once per CTA
+    // the adjoint copies the tables instead of building them, so more CTAs pay
+    const unsigned tgrid_bwd = (unsigned)(tw < kSMs * 8 ? tw : kSMs * 8);
     if (c.T > 0 && tab) {
         if (k8)
             accum_tab_kernel<8><<<tgrid, kTabWarps * 32, tsm, sst>>>(c.T, c.min_level, c.max_level, S, ST, alpha_src,
-                                                                   feat_src, w.alpha_acc, w.feat_acc, w.feat_bf16);
+                                                                   feat_src, w.alpha_acc, w.feat_acc, w.feat_bf16,
+                                                                   w.tab);
         else
             accum_tab_kernel<16><<<tgrid, kTabWarps * 32, tsm, sst>>>(c.T, c.min_level, c.max_level, S, ST, alpha_src,
-                                                                    feat_src, w.alpha_acc, w.feat_acc, w.feat_bf16);
+                                                                    feat_src, w.alpha_acc, w.feat_acc, w.feat_bf16,
+                                                                   w.tab);
     } else if (c.T > 0) {
         accum_sigmoid_kernel<false><<<tb, kPrepWarps * 32, 0, sst>>>(c.T, c.min_level, c.max_level, c.max_level, S, ST,
                                                                     1, alpha_src, w.alpha_acc, nullptr);
@@ -738,13 +757,13 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     // adjoints of sigmoid + level accumulation, and of the projection
     if (c.T > 0 && tab) {
         if (k8)
-            accum_tab_backward_kernel<8><<<tgrid, kTabWarps * 32, tsm, st>>>(
+            accum_tab_backward_kernel<8><<<tgrid_bwd, kTabWarps * 32, tsm, st>>>(
                 c.T, c.min_level, c.max_level, S, ST, w.alpha_acc, w.grad_alpha_acc, w.feat_acc, w.grad_feat_acc,
-                grad_alpha_src, grad_feat_src);
+                grad_alpha_src, grad_feat_src, w.tab);
         else
-            accum_tab_backward_kernel<16><<<tgrid, kTabWarps * 32, tsm, st>>>(
+            accum_tab_backward_kernel<16><<<tgrid_bwd, kTabWarps * 32, tsm, st>>>(
                 c.T, c.min_level, c.max_level, S, ST, w.alpha_acc, w.grad_alpha_acc, w.feat_acc, w.grad_feat_acc,
-                grad_alpha_src, grad_feat_src);
+                grad_alpha_src, grad_feat_src, w.tab);
     } else if (c.T > 0) {
         accum_sigmoid_backward_kernel<<<tb, kPrepWarps * 32, 0, st>>>(c.T, c.min_level, c.max_level, c.max_level, S,
                                                                       ST, 1, w.alpha_acc, w.grad_alpha_acc,
