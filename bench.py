@@ -393,6 +393,11 @@ def run_ours(args):
     if rank == 0 and args.render:
         render = run_render(dev, cpu_sample=not args.no_cpu_baseline)
 
+    # ---------------- soup subdivision (resampling step) -----------------------
+    remesh_line = None
+    if rank == 0 and args.render:
+        remesh_line = run_remesh(dev, cpu_sample=not args.no_cpu_baseline)
+
     # ---------------- CPU baseline --------------------------------------------
     cpu_base = None
     if not args.no_cpu_baseline and rank == 0:
@@ -428,6 +433,8 @@ def run_ours(args):
         line["cpu_baseline"] = cpu_base
     if render is not None:
         line["render"] = render
+    if remesh_line is not None:
+        line["remesh"] = remesh_line
     if rank == 0:
         print(json.dumps(line), flush=True)
     del graphs, egraphs
@@ -600,6 +607,39 @@ def run_render(dev, cpu_sample: bool = True, frames: int = 200):
         out["cpu_baseline"] = {"fps": 1.0 / dt, "cores": cpu.omp_threads(), "kind": "port",
                                "sample": "1 frame of view 0: oracle rasterizer (OpenMP) + numpy FP64 post pass"}
     return out
+
+
+def run_remesh(dev, cpu_sample: bool = True, reps: int = 5):
+    """The resampling step's subdivision on the benchmark soup: 15,000 faces
+    split in screen space under one 800x800 view until every edge is below
+    0.004 image heights (split_triangle_soup_clip_until), timed end to end
+    through the public call with device tensors (two kernels, one scan and the
+    count read back), beside the reference's own CPU remesher."""
+    from diffsoup_b200 import remesh, scenes
+
+    sc = scenes.make_scene(2, seed=0, num_views=1, with_targets=False)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    args = ((800, 800), t(sc.mvps()[0]), t(sc.verts), t(sc.tri), t(np.ones(sc.T, np.int32)), 0.004)
+    out = remesh.split_triangle_soup_clip_until(*args)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        out = remesh.split_triangle_soup_clip_until(*args)
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) * 1000.0 / reps
+    res = {"workload": "split_triangle_soup_clip_until, 15,000 faces, 800x800 view, tau_ratio 0.004",
+           "faces_out": int(out[1].shape[0]), "splits": int(out[1].shape[0]) - sc.T, "ms": ms,
+           "msplits_per_s": (int(out[1].shape[0]) - sc.T) / ms / 1e3}
+    if cpu_sample:
+        from oracle import remesh as R
+        if R.reference_available():
+            t0 = time.perf_counter()
+            R.reference_split(sc.verts, sc.tri, -1, 0.004, mvp=sc.mvps()[0], valid=np.ones(sc.T, np.int32),
+                              aspect_wh=1.0)
+            res["cpu_baseline"] = {"ms": (time.perf_counter() - t0) * 1000.0, "cores": 1, "kind": "reference",
+                                   "sample": "the same call through the reference's own remesher (src/remesh_clip.cpp,"
+                                             " one host thread, as the reference runs it)"}
+    return res
 
 
 def run_cpu_baseline(sc, mlp, s):

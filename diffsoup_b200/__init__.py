@@ -5,13 +5,15 @@ Drop-in for the rasterize/shade API of kenji-tojo/diffsoup
 signatures and tensor layouts, backed by hand-written sm_100a kernels in
 libdiffsoup_b200.so.  `step` adds the batched, graph-captured training step,
 `optimize` the fused VectorAdam / Adam updates that follow it, `viewer` the
-headless inference render of the viewer's deferred shading.
+headless inference render of the viewer's deferred shading, `remesh` the
+soup subdivision of the resampling step.
 """
 
 from __future__ import annotations
 
 from . import _core
 from . import optimize
+from . import remesh
 from . import viewer
 from . import visibility
 from ._core import __version__
@@ -21,6 +23,13 @@ from .rasterize import (
     encode_view_dir,
     encode_view_dir_sh2,
     opacity_aux_loss,
+)
+from .remesh import (
+    expand_by_index,
+    split_triangle_soup,
+    split_triangle_soup_clip,
+    split_triangle_soup_clip_until,
+    split_triangle_soup_until,
 )
 from .multires import (
     ColorMLP,
@@ -39,8 +48,13 @@ __all__ = [
     "edge_grad",
     "encode_view_dir",
     "encode_view_dir_sh2",
+    "expand_by_index",
     "feats_at_level",
     "multires_triangle_color",
     "opacity_aux_loss",
     "rasterize_multires_triangle_alpha",
+    "split_triangle_soup",
+    "split_triangle_soup_clip",
+    "split_triangle_soup_clip_until",
+    "split_triangle_soup_until",
 ]

@@ -1,0 +1,326 @@
+// diffsoup_b200/csrc/remesh.cu -- adaptive subdivision of the triangle soup
+// (the resampling step of training, examples/utils.py:493-545), on the GPU.
+//
+// The reference splits on the CPU (src/remesh.cpp world-space lengths,
+// src/remesh_clip.cpp screen-space lengths under one MVP) with a global
+// priority queue: pop the longest edge, bisect its triangle, re-enqueue both
+// halves, until the longest edge is below the threshold.  In a soup no two
+// triangles share vertices, so a split only ever touches the descendants of
+// one input face, and every face is split at its longest (considered) edge
+// while that edge is at least the threshold: the queue's global order
+// decides only the numbering of the new vertices and faces, not the geometry.
+// Here each input face is one thread that walks its own split tree depth
+// first, twice: a counting pass (the new faces of every family, scanned into
+// offsets) and an emitting pass that writes the vertices and faces.
+//
+// Layout of the output, as the reference's (src/remesh.cpp:15-64): the N
+// input vertices unchanged, then 3 vertices per split (the two copies of the
+// split point and the copy of the opposite vertex); face slot t keeps the
+// first child of every split of family t, and each split gives its second
+// child a new slot after the M inputs.  New vertices and slots of a family are
+// numbered in the depth-first order of its tree (the reference numbers them
+// in global pop order), so the result equals the reference's up to that
+// renumbering: the same set of triangles per family, bit for bit.
+//
+// Arithmetic follows the reference's host build (IEEE single precision, every
+// product and sum rounded on its own, no FMA contraction).  A face whose
+// longest edge ties with another takes the first in edge order (0,1), (1,2),
+// (2,0); the reference's heap leaves such ties unordered.
+#include "common.cuh"
+#include "scan.cuh"
+
+namespace dsb {
+
+constexpr int kSplitThreads = 128;
+constexpr int kSplitStack = 40;                 // pending second children along one path
+constexpr int64_t kMaxFamilySplits = 1 << 20;   // per input face
+constexpr int64_t kMaxTotalSplits = 1ll << 27;  // per call
+
+struct SplitParams {
+    int mode;      // 0 world (remesh.cpp), 1 clip (remesh_clip.cpp)
+    float m[16];   // MVP, row-major (clip mode)
+    float aspect;  // W / H (clip mode)
+    float tau2;    // squared threshold in the metric's units
+};
+
+struct SplitNode {
+    float p[9];  // positions of the three corners
+    int id[3];   // their vertex indices
+    int slot;    // face slot
+};
+
+// ((m0 x + m1 y) + m2 z) + m3, each operation rounded (remesh_clip.cpp:19-29)
+__device__ __forceinline__ float hom_row(const float* m, int r, const float* v) {
+    return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m[4 * r + 0], v[0]), __fmul_rn(m[4 * r + 1], v[1])),
+                               __fmul_rn(m[4 * r + 2], v[2])),
+                     m[4 * r + 3]);
+}
+
+struct ClipPoint {
+    float c[4];    // clip coordinates
+    float n[3];    // NDC (0 where w <= 0)
+    bool inside;   // w > 0 and inside the NDC cube
+};
+
+__device__ __forceinline__ ClipPoint clip_point(const SplitParams& P, const float* v) {
+    ClipPoint q;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) q.c[r] = hom_row(P.m, r, v);
+    const bool wok = q.c[3] > 0.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) q.n[k] = wok ? __fdiv_rn(q.c[k], q.c[3]) : 0.f;
+    q.inside = wok && q.n[0] >= -1.f && q.n[0] <= 1.f && q.n[1] >= -1.f && q.n[1] <= 1.f && q.n[2] >= -1.f &&
+               q.n[2] <= 1.f;
+    return q;
+}
+
+// Squared length of edge (A, B) in the metric: world (remesh.h:41-48) or
+// image-height units, 0 when an end leaves the NDC cube (remesh_clip.cpp:33-78).
+__device__ __forceinline__ float edge_len2(const SplitParams& P, const float* A, const float* B) {
+    if (P.mode == 0) {
+        const float dx = __fsub_rn(B[0], A[0]), dy = __fsub_rn(B[1], A[1]), dz = __fsub_rn(B[2], A[2]);
+        return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+    }
+    const ClipPoint a = clip_point(P, A), b = clip_point(P, B);
+    if (!a.inside || !b.inside) return 0.f;
+    const float dx = __fmul_rn(__fsub_rn(a.n[0], b.n[0]), P.aspect), dy = __fsub_rn(a.n[1], b.n[1]);
+    return __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+}
+
+// The split point of edge (A, B): the midpoint in world space, or the point
+// whose projection is the NDC midpoint (remesh_clip.cpp:100-145).
+__device__ __forceinline__ void split_point(const SplitParams& P, const float* A, const float* B, float* C) {
+    if (P.mode == 0) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) C[k] = __fmul_rn(0.5f, __fadd_rn(A[k], B[k]));
+        return;
+    }
+    const ClipPoint a = clip_point(P, A), b = clip_point(P, B);
+    const float nx = __fmul_rn(0.5f, __fadd_rn(a.n[0], b.n[0]));
+    const float ny = __fmul_rn(0.5f, __fadd_rn(a.n[1], b.n[1]));
+    const float dx = __fsub_rn(b.c[0], a.c[0]), dy = __fsub_rn(b.c[1], a.c[1]), dw = __fsub_rn(b.c[3], a.c[3]);
+    const float ax = __fsub_rn(a.c[0], __fmul_rn(nx, a.c[3])), ay = __fsub_rn(a.c[1], __fmul_rn(ny, a.c[3]));
+    const float bx = __fsub_rn(dx, __fmul_rn(nx, dw)), by = __fsub_rn(dy, __fmul_rn(ny, dw));
+    const float den = __fadd_rn(__fmul_rn(bx, bx), __fmul_rn(by, by));
+    const float tB = den != 0.f ? __fdiv_rn(-__fadd_rn(__fmul_rn(ax, bx), __fmul_rn(ay, by)), den) : 0.5f;
+    const float tA = __fsub_rn(1.f, tB);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) C[k] = __fadd_rn(__fmul_rn(tA, A[k]), __fmul_rn(tB, B[k]));
+}
+
+// Walks the split tree of face t.  Counting pass (EMIT false): returns the
+// number of splits.  Emitting pass: writes the family's faces, its new
+// vertices from vbase and its new slots from fbase.  Both passes take the
+// same decisions; a family that would exceed max_splits (or the stack) stops
+// splitting and raises DS_STATUS_SPLIT_LIMIT, which the host turns into an
+// error after the counting pass.
+template <bool EMIT>
+__device__ int64_t walk_family(const SplitParams& P, int t, const float* __restrict__ verts,
+                               const int* __restrict__ faces, bool splittable, int64_t max_splits, int64_t vbase,
+                               int64_t fbase, float* __restrict__ out_verts, int* __restrict__ out_faces,
+                               int* __restrict__ status, unsigned long long* __restrict__ total) {
+    SplitNode stack[kSplitStack];
+    int top = 0;
+    SplitNode cur;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        cur.id[k] = faces[(size_t)t * 3 + k];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) cur.p[k * 3 + j] = verts[(size_t)cur.id[k] * 3 + j];
+    }
+    cur.slot = t;
+    int64_t splits = 0;
+    bool stop = !splittable;
+    while (true) {
+        // longest considered edge: e = 0 (0,1), 1 (1,2), 2 (2,0); first of equals
+        int e = -1;
+        float best = 0.f;
+        if (!stop) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float l2 = edge_len2(P, cur.p + k * 3, cur.p + ((k + 1) % 3) * 3);
+                const bool considered = P.mode == 0 || l2 > 0.f;
+                if (considered && (e < 0 || l2 > best)) { e = k; best = l2; }
+            }
+        }
+        const bool split = e >= 0 && best >= P.tau2 && best > 0.f;
+        if (split && (top == kSplitStack || splits >= max_splits)) {
+            atomicOr(status, DS_STATUS_SPLIT_LIMIT);  // the family stops here; the host reports it
+            stop = true;
+            continue;
+        }
+        if (split) {
+            // the call's total, charged every 256 splits of a family
+            if (!EMIT && splits > 0 && (splits & 255) == 0 &&
+                atomicAdd(total, 256ull) > (unsigned long long)kMaxTotalSplits) {
+                atomicOr(status, DS_STATUS_SPLIT_LIMIT);
+                stop = true;
+                continue;
+            }
+            const int ia = e, ib = (e + 1) % 3, ic = (e + 2) % 3;  // edge (a, b), opposite c
+            float C[3];
+            split_point(P, cur.p + ia * 3, cur.p + ib * 3, C);
+            const int64_t k = splits++;
+            const int mA = (int)(vbase + 3 * k), mB = mA + 1, cA = mA + 2;
+            SplitNode second;  // (mB, b, c) in a new slot
+            second.slot = (int)(fbase + k);
+            second.id[0] = mB; second.id[1] = cur.id[ib]; second.id[2] = cur.id[ic];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                second.p[j] = C[j];
+                second.p[3 + j] = cur.p[ib * 3 + j];
+                second.p[6 + j] = cur.p[ic * 3 + j];
+            }
+            if (EMIT) {
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    out_verts[(size_t)mA * 3 + j] = C[j];
+                    out_verts[(size_t)mB * 3 + j] = C[j];
+                    out_verts[(size_t)cA * 3 + j] = cur.p[ic * 3 + j];
+                }
+            }
+            // (a, mA, cA) keeps the slot and is walked next
+            SplitNode first;
+            first.slot = cur.slot;
+            first.id[0] = cur.id[ia]; first.id[1] = mA; first.id[2] = cA;
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                first.p[j] = cur.p[ia * 3 + j];
+                first.p[3 + j] = C[j];
+                first.p[6 + j] = cur.p[ic * 3 + j];
+            }
+            stack[top++] = second;
+            cur = first;
+            continue;
+        }
+        if (EMIT) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) out_faces[(size_t)cur.slot * 3 + k] = cur.id[k];
+        }
+        if (top == 0) break;
+        cur = stack[--top];
+    }
+    return splits;
+}
+
+__global__ void __launch_bounds__(kSplitThreads) split_count_kernel(SplitParams P, int M, const float* __restrict__ verts,
+                                                                    const int* __restrict__ faces,
+                                                                    const int* __restrict__ valid,
+                                                                    int* __restrict__ counts, int* __restrict__ status,
+                                                                    unsigned long long* __restrict__ total) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= M) return;
+    const bool splittable = P.mode == 0 || valid == nullptr || valid[t] > 0;
+    counts[t] = (int)walk_family<false>(P, t, verts, faces, splittable, kMaxFamilySplits, 0, 0, nullptr, nullptr,
+                                        status, total);
+}
+
+__global__ void __launch_bounds__(kSplitThreads) split_emit_kernel(SplitParams P, int N, int M,
+                                                                   const float* __restrict__ verts,
+                                                                   const int* __restrict__ faces,
+                                                                   const int* __restrict__ valid,
+                                                                   const int64_t* __restrict__ offsets,
+                                                                   float* __restrict__ out_verts,
+                                                                   int* __restrict__ out_faces, int* __restrict__ map,
+                                                                   int* __restrict__ flag, int* __restrict__ status) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= M) return;
+    const int64_t o = offsets[t], n = offsets[t + 1] - o;
+    const bool splittable = n > 0;
+    walk_family<true>(P, t, verts, faces, splittable, n, N + 3 * o, M + o, out_verts, out_faces, status, nullptr);
+    // faceMapping / sameAsOriginal of the family's slots (src/remesh.cpp:35-50)
+    map[t] = t;
+    flag[t] = n == 0 ? 1 : 0;
+    for (int64_t k = 0; k < n; ++k) {
+        map[M + o + k] = t;
+        flag[M + o + k] = 0;
+    }
+}
+
+__global__ void copy_floats_kernel(int64_t n, const float* __restrict__ src, float* __restrict__ dst) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
+static int make_params(int mode, const float* mvp_host, float aspect_wh, float tau, SplitParams& P) {
+    DS_CHECK_ARG(mode == 0 || mode == 1, "split_soup: mode %d is neither 0 (world) nor 1 (clip)", mode);
+    DS_CHECK_ARG(mode == 0 || mvp_host != nullptr, "split_soup: clip mode needs the MVP");
+    P.mode = mode;
+    for (int i = 0; i < 16; ++i) P.m[i] = mode == 1 ? mvp_host[i] : 0.f;
+    P.aspect = aspect_wh;
+    // world: tau; clip: tau = 2 * tau_ratio (NDC spans 2 per image height)
+    const float tt = mode == 0 ? tau : 2.0f * tau;
+    P.tau2 = tt * tt;
+    return DS_OK;
+}
+
+static size_t al256(size_t n) { return (n + 255) & ~(size_t)255; }
+
+}  // namespace dsb
+
+using namespace dsb;
+
+extern "C" {
+
+size_t ds_split_soup_workspace_size(int M) {
+    return al256((size_t)(M > 0 ? M : 1) * sizeof(int)) + al256(scan_workspace_bytes(M > 0 ? M : 1)) + 256;
+}
+
+int ds_split_soup_count(int mode, const float* mvp_host, float aspect_wh, float tau, int N, const float* verts, int M,
+                        const int* faces, const int* valid, int64_t* split_offsets, int64_t* total_splits_host,
+                        void* workspace, size_t workspace_bytes, int* status, ds_stream_t stream) {
+    SplitParams P;
+    int rc = make_params(mode, mvp_host, aspect_wh, tau, P);
+    if (rc) return rc;
+    DS_CHECK_ARG(N >= 0 && M >= 0 && total_splits_host && split_offsets && status, "split_soup: bad arguments");
+    DS_CHECK_ARG(M == 0 || (verts && faces), "split_soup: null pointer");
+    DS_CHECK_ARG(workspace && workspace_bytes >= ds_split_soup_workspace_size(M), "split_soup: workspace too small");
+    cudaStream_t st = (cudaStream_t)stream;
+    char* ws = reinterpret_cast<char*>(workspace);
+    int* counts = reinterpret_cast<int*>(ws);
+    void* scan_ws = ws + al256((size_t)(M > 0 ? M : 1) * sizeof(int));
+    unsigned long long* total = reinterpret_cast<unsigned long long*>(
+        ws + al256((size_t)(M > 0 ? M : 1) * sizeof(int)) + al256(scan_workspace_bytes(M > 0 ? M : 1)));
+    DS_CUDA(cudaMemsetAsync(total, 0, sizeof(unsigned long long), st));
+    // threshold mode only: the reference splits nothing unless the threshold is positive
+    const bool active = tau > 0.f && M > 0;
+    if (active)
+        split_count_kernel<<<blocks_for(M, kSplitThreads), kSplitThreads, 0, st>>>(P, M, verts, faces,
+                                                                                    mode == 1 ? valid : nullptr,
+                                                                                    counts, status, total);
+    else if (M > 0)
+        DS_CUDA(cudaMemsetAsync(counts, 0, (size_t)M * sizeof(int), st));
+    int64_t* total_dev = nullptr;
+    if ((rc = device_scan<int, int64_t>(counts, M, split_offsets, false, scan_ws, st, &total_dev))) return rc;
+    DS_CUDA(cudaMemcpyAsync(split_offsets + M, total_dev, sizeof(int64_t), cudaMemcpyDeviceToDevice, st));
+    DS_CUDA(cudaMemcpyAsync(total_splits_host, total_dev, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    DS_CUDA(cudaStreamSynchronize(st));
+    return check_launch("split_soup_count");
+}
+
+int ds_split_soup_emit(int mode, const float* mvp_host, float aspect_wh, float tau, int N, const float* verts, int M,
+                       const int* faces, const int* valid, const int64_t* split_offsets, int64_t total_splits,
+                       float* out_verts, int* out_faces, int* out_map, int* out_flag, int* status,
+                       ds_stream_t stream) {
+    SplitParams P;
+    int rc = make_params(mode, mvp_host, aspect_wh, tau, P);
+    if (rc) return rc;
+    DS_CHECK_ARG(N >= 0 && M >= 0 && total_splits >= 0 && split_offsets && status, "split_soup: bad arguments");
+    DS_CHECK_ARG((int64_t)N + 3 * total_splits <= 0x7fffffff && (int64_t)M + total_splits <= 0x7fffffff,
+                 "split_soup: %lld splits exceed the int32 vertex and face indices", (long long)total_splits);
+    DS_CHECK_ARG(M == 0 || (verts && faces && out_verts && out_faces && out_map && out_flag),
+                 "split_soup: null pointer");
+    (void)valid;  // the counting pass already applied the mask: families with no splits stay as they are
+    cudaStream_t st = (cudaStream_t)stream;
+    if (N > 0) {
+        const unsigned b = blocks_for((int64_t)N * 3);
+        copy_floats_kernel<<<b < (unsigned)kSMs * 8 ? b : (unsigned)kSMs * 8, kThreads, 0, st>>>((int64_t)N * 3,
+                                                                                                   verts, out_verts);
+    }
+    if (M > 0)
+        split_emit_kernel<<<blocks_for(M, kSplitThreads), kSplitThreads, 0, st>>>(
+            P, N, M, verts, faces, valid, split_offsets, out_verts, out_faces, out_map, out_flag, status);
+    return check_launch("split_soup_emit");
+}
+
+}  // extern "C"

@@ -1,0 +1,93 @@
+"""The GPU soup subdivision (csrc/remesh.cu through diffsoup_b200.remesh)
+against its oracle.
+
+* bit for bit the arrays of the restatement (oracle/remesh.py, pinned to the
+  reference's remeshers on CPU), which numbers the output as the GPU does:
+  vertices, faces, face mapping and flags, world and screen-space lengths,
+  masked faces and corners outside the NDC cube;
+* at the benchmark soup's size (15,000 faces, one 800x800 view), the same
+  triangles per input face as the reference's own compiled remesher;
+* the resampling step of training (several views in turn) keeps the face
+  mapping consistent with the faces' geometry.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from diffsoup_b200 import remesh, scenes
+from oracle import remesh as R
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda"
+
+
+def _np(q):
+    return tuple(x.cpu().numpy() for x in q)
+
+
+def _soup(T, seed, spread=0.15):
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(-1, 1, (T, 3))
+    v = (c[:, None, :] + rng.normal(0, spread, (T, 3, 3))).reshape(-1, 3).astype(np.float32)
+    return v, np.arange(3 * T, dtype=np.int32).reshape(T, 3)
+
+
+def _equal(got, want):
+    for g, w in zip(got, want):
+        assert g.shape == w.shape
+        assert np.array_equal(g.view(np.uint32) if g.dtype == np.float32 else g, w.view(np.uint32)
+                              if w.dtype == np.float32 else w)
+
+
+@pytest.mark.parametrize("tau", [0.05, 0.2])
+def test_world_split_equals_oracle(tau):
+    v, f = _soup(200, seed=7)
+    got = _np(remesh.split_triangle_soup_until(torch.from_numpy(v).to(DEV), torch.from_numpy(f).to(DEV), tau))
+    _equal(got, R.restated_split(v, f, tau))
+
+
+def test_clip_split_equals_oracle():
+    sc = scenes.make_scene(2, seed=3, num_tris=300, num_views=1, resolution=(600, 800), with_targets=False)
+    rng = np.random.default_rng(3)
+    valid = (rng.random(sc.T) < 0.7).astype(np.int32)
+    verts = sc.verts.copy()
+    verts[:40] *= 6.0
+    mvp = sc.mvps()[0]
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(DEV)  # noqa: E731
+    got = _np(remesh.split_triangle_soup_clip_until((600, 800), t(mvp), t(verts), t(sc.tri), t(valid), 0.01))
+    want = R.restated_split(verts, sc.tri, 0.01, mvp=mvp, valid=valid, aspect_wh=800 / 600)
+    assert want[1].shape[0] > sc.T
+    _equal(got, want)
+
+
+@pytest.mark.skipif(not R.reference_available(), reason="oracle/_ref/libremesh_ref.so not built")
+def test_benchmark_soup_matches_reference():
+    sc = scenes.make_scene(2, seed=0, num_views=1, with_targets=False)
+    mvp = sc.mvps()[0]
+    valid = np.ones(sc.T, np.int32)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(DEV)  # noqa: E731
+    got = _np(remesh.split_triangle_soup_clip_until((800, 800), t(mvp), t(sc.verts), t(sc.tri), t(valid), 0.004))
+    ref = R.reference_split(sc.verts, sc.tri, -1, 0.004, mvp=mvp, valid=valid, aspect_wh=1.0)
+    assert got[1].shape == ref[1].shape and ref[1].shape[0] > 2 * sc.T
+    assert R.families(*got) == R.families(*ref)
+    print(f"clip split of {sc.T} faces: {ref[1].shape[0] - sc.T} splits, same triangles as the reference")
+
+
+def test_resampling_step_keeps_the_mapping():
+    sc = scenes.make_scene(2, seed=2, num_tris=2000, num_views=4, resolution=(200, 200), with_targets=False)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(DEV)  # noqa: E731
+    torch.manual_seed(0)
+    S = 15  # level 2
+    alpha = torch.full((sc.T, S), 0.9, device=DEV)
+    V, F, fmap = remesh.split_edges_from_training_views((200, 200), t(sc.mvps()), t(sc.verts), t(sc.tri), 2, alpha,
+                                                        tau_ratio=0.02, num_views_cap=3)
+    assert F.shape[0] > sc.T and fmap.shape[0] == F.shape[0]
+    assert int(fmap.min()) >= 0 and int(fmap.max()) < sc.T
+    # every output face lies in the plane of the input face it maps to
+    v0 = t(sc.verts)[t(sc.tri).long()]  # [T,3,3]
+    n = torch.linalg.cross(v0[:, 1] - v0[:, 0], v0[:, 2] - v0[:, 0])
+    n = n / n.norm(dim=1, keepdim=True)
+    pts = V[F.long()]  # [M',3,3]
+    d = ((pts - v0[fmap][:, :1]) * n[fmap][:, None, :]).sum(-1)
+    assert float(d.abs().max()) < 1e-4
