@@ -76,10 +76,9 @@ _sig("ds_tiles_opacity_aux", _i32, _i32, _vp, _i32, _i32, _vp, _i32, _vp, _i32, 
      _vp, _vp, _sz, _i64, _vp)
 _sig("ds_project_vertices", _i32, _i32, _i32, _vp, _vp, _vp, _vp)
 _sig("ds_split_soup_workspace_size", _sz, _i32)
-_sig("ds_split_soup_count", _i32, _i32, _vp, _f32, _f32, _i32, _vp, _i32, _vp, _vp, _vp, C.POINTER(C.c_int64), _vp,
-     _sz, _vp, _vp)
-_sig("ds_split_soup_emit", _i32, _i32, _vp, _f32, _f32, _i32, _vp, _i32, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _vp,
-     _vp, _vp)
+_sig("ds_split_soup_count", _i32, _i32, _vp, _f32, _f32, _i32, _i32, _vp, _i32, _vp, _vp, _vp,
+     C.POINTER(C.c_int64), _vp, _sz, _vp, _vp)
+_sig("ds_split_soup_emit", _i32, _i32, _vp, _f32, _i32, _vp, _i32, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp)
 _sig("ds_render_lut_opacity", _i32, _i64, _vp, _vp, _vp)
 _sig("ds_render_deferred", _i32, _i32, _vp, _i64, _vp, _i32, _vp, _vp, _i64, _vp, _vp, _f32, _f32, _f32, _vp, _vp, _vp)
 _sig("ds_render_workspace_size", _sz, _i32, _i32, _i32, _i32, _i64)

@@ -26,6 +26,8 @@
 // product and sum rounded on its own, no FMA contraction).  A face whose
 // longest edge ties with another takes the first in edge order (0,1), (1,2),
 // (2,0); the reference's heap leaves such ties unordered.
+#include <cstring>
+
 #include "common.cuh"
 #include "scan.cuh"
 
@@ -40,7 +42,12 @@ struct SplitParams {
     int mode;      // 0 world (remesh.cpp), 1 clip (remesh_clip.cpp)
     float m[16];   // MVP, row-major (clip mode)
     float aspect;  // W / H (clip mode)
-    float tau2;    // squared threshold in the metric's units
+};
+
+// Which edges a walk splits: those of squared length >= tau2 and, up to a
+// per-face quota, those of exactly tie2 (a split budget's cut-off, below).
+struct SplitPlan {
+    float tau2, tie2;
 };
 
 struct SplitNode {
@@ -115,7 +122,7 @@ __device__ __forceinline__ void split_point(const SplitParams& P, const float* A
 // splitting and raises DS_STATUS_SPLIT_LIMIT, which the host turns into an
 // error after the counting pass.
 template <bool EMIT>
-__device__ int64_t walk_family(const SplitParams& P, int t, const float* __restrict__ verts,
+__device__ int64_t walk_family(const SplitParams& P, SplitPlan plan, int quota, int t, const float* __restrict__ verts,
                                const int* __restrict__ faces, bool splittable, int64_t max_splits, int64_t vbase,
                                int64_t fbase, float* __restrict__ out_verts, int* __restrict__ out_faces,
                                int* __restrict__ status, unsigned long long* __restrict__ total) {
@@ -143,7 +150,8 @@ __device__ int64_t walk_family(const SplitParams& P, int t, const float* __restr
                 if (considered && (e < 0 || l2 > best)) { e = k; best = l2; }
             }
         }
-        const bool split = e >= 0 && best >= P.tau2 && best > 0.f;
+        const bool tie = quota > 0 && best == plan.tie2;
+        const bool split = e >= 0 && best > 0.f && (best >= plan.tau2 || tie);
         if (split && (top == kSplitStack || splits >= max_splits)) {
             atomicOr(status, DS_STATUS_SPLIT_LIMIT);  // the family stops here; the host reports it
             stop = true;
@@ -160,6 +168,7 @@ __device__ int64_t walk_family(const SplitParams& P, int t, const float* __restr
             const int ia = e, ib = (e + 1) % 3, ic = (e + 2) % 3;  // edge (a, b), opposite c
             float C[3];
             split_point(P, cur.p + ia * 3, cur.p + ib * 3, C);
+            if (tie && !(best >= plan.tau2)) --quota;
             const int64_t k = splits++;
             const int mA = (int)(vbase + 3 * k), mB = mA + 1, cA = mA + 2;
             SplitNode second;  // (mB, b, c) in a new slot
@@ -203,22 +212,24 @@ __device__ int64_t walk_family(const SplitParams& P, int t, const float* __restr
     return splits;
 }
 
-__global__ void __launch_bounds__(kSplitThreads) split_count_kernel(SplitParams P, int M, const float* __restrict__ verts,
+__global__ void __launch_bounds__(kSplitThreads) split_count_kernel(SplitParams P, SplitPlan plan, int M,
+                                                                    const float* __restrict__ verts,
                                                                     const int* __restrict__ faces,
                                                                     const int* __restrict__ valid,
+                                                                    const int* __restrict__ quota,
                                                                     int* __restrict__ counts, int* __restrict__ status,
                                                                     unsigned long long* __restrict__ total) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= M) return;
     const bool splittable = P.mode == 0 || valid == nullptr || valid[t] > 0;
-    counts[t] = (int)walk_family<false>(P, t, verts, faces, splittable, kMaxFamilySplits, 0, 0, nullptr, nullptr,
-                                        status, total);
+    counts[t] = (int)walk_family<false>(P, plan, quota ? quota[t] : 0, t, verts, faces, splittable, kMaxFamilySplits,
+                                        0, 0, nullptr, nullptr, status, total);
 }
 
-__global__ void __launch_bounds__(kSplitThreads) split_emit_kernel(SplitParams P, int N, int M,
-                                                                   const float* __restrict__ verts,
+__global__ void __launch_bounds__(kSplitThreads) split_emit_kernel(SplitParams P, const SplitPlan* __restrict__ plan,
+                                                                   int N, int M, const float* __restrict__ verts,
                                                                    const int* __restrict__ faces,
-                                                                   const int* __restrict__ valid,
+                                                                   const int* __restrict__ quota,
                                                                    const int64_t* __restrict__ offsets,
                                                                    float* __restrict__ out_verts,
                                                                    int* __restrict__ out_faces, int* __restrict__ map,
@@ -226,8 +237,8 @@ __global__ void __launch_bounds__(kSplitThreads) split_emit_kernel(SplitParams P
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= M) return;
     const int64_t o = offsets[t], n = offsets[t + 1] - o;
-    const bool splittable = n > 0;
-    walk_family<true>(P, t, verts, faces, splittable, n, N + 3 * o, M + o, out_verts, out_faces, status, nullptr);
+    walk_family<true>(P, *plan, quota[t], t, verts, faces, n > 0, n, N + 3 * o, M + o, out_verts, out_faces, status,
+                      nullptr);
     // faceMapping / sameAsOriginal of the family's slots (src/remesh.cpp:35-50)
     map[t] = t;
     flag[t] = n == 0 ? 1 : 0;
@@ -237,24 +248,112 @@ __global__ void __launch_bounds__(kSplitThreads) split_emit_kernel(SplitParams P
     }
 }
 
+// Largest considered squared edge length over the faces that may split (as
+// the bits of a non-negative float, which order like the values).
+__global__ void __launch_bounds__(kSplitThreads) split_max_edge_kernel(SplitParams P, int M,
+                                                                       const float* __restrict__ verts,
+                                                                       const int* __restrict__ faces,
+                                                                       const int* __restrict__ valid,
+                                                                       unsigned* __restrict__ max_bits) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= M || !(P.mode == 0 || valid == nullptr || valid[t] > 0)) return;
+    float p[9];
+    for (int k = 0; k < 3; ++k)
+        for (int j = 0; j < 3; ++j) p[k * 3 + j] = verts[(size_t)faces[(size_t)t * 3 + k] * 3 + j];
+    float best = 0.f;
+    for (int k = 0; k < 3; ++k) best = fmaxf(best, edge_len2(P, p + k * 3, p + ((k + 1) % 3) * 3));
+    atomicMax(max_bits, __float_as_uint(best));
+}
+
+// quota[t] = the share of face t in the first `extra` cut-off splits, faces in
+// index order: clamp(extra - before[t], 0, ties[t]).
+__global__ void split_quota_kernel(int M, const int* __restrict__ ties, const int64_t* __restrict__ before,
+                                   int64_t extra, int* __restrict__ quota) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= M) return;
+    const int64_t q = extra - before[t];
+    quota[t] = q <= 0 ? 0 : (q < ties[t] ? (int)q : ties[t]);
+}
+
+__global__ void split_diff_kernel(int M, const int* __restrict__ a, int* __restrict__ b) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < M) b[t] -= a[t];
+}
+
 __global__ void copy_floats_kernel(int64_t n, const float* __restrict__ src, float* __restrict__ dst) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         dst[i] = src[i];
 }
 
-static int make_params(int mode, const float* mvp_host, float aspect_wh, float tau, SplitParams& P) {
+static int make_params(int mode, const float* mvp_host, float aspect_wh, SplitParams& P) {
     DS_CHECK_ARG(mode == 0 || mode == 1, "split_soup: mode %d is neither 0 (world) nor 1 (clip)", mode);
     DS_CHECK_ARG(mode == 0 || mvp_host != nullptr, "split_soup: clip mode needs the MVP");
     P.mode = mode;
     for (int i = 0; i < 16; ++i) P.m[i] = mode == 1 ? mvp_host[i] : 0.f;
     P.aspect = aspect_wh;
-    // world: tau; clip: tau = 2 * tau_ratio (NDC spans 2 per image height)
-    const float tt = mode == 0 ? tau : 2.0f * tau;
-    P.tau2 = tt * tt;
     return DS_OK;
 }
 
 static size_t al256(size_t n) { return (n + 255) & ~(size_t)255; }
+
+// The count call's workspace: per-face counts and quotas, the scan's
+// partials, and a small block of scalars that the emit call reads back.
+struct SplitWs {
+    int* counts;
+    int* quota;
+    void* scan;
+    unsigned long long* total;  // limit accounting of a counting pass
+    int* probe_status;          // status of the current counting pass
+    unsigned* max_bits;         // largest edge (split budget)
+    SplitPlan* plan;            // the plan the emit call follows
+};
+
+static SplitWs carve_split(void* ws, int M, size_t* bytes) {
+    const size_t m = (size_t)(M > 0 ? M : 1);
+    char* p = reinterpret_cast<char*>(ws);
+    size_t o = 0;
+    SplitWs w;
+    w.counts = reinterpret_cast<int*>(p + o); o += al256(m * sizeof(int));
+    w.quota = reinterpret_cast<int*>(p + o); o += al256(m * sizeof(int));
+    w.scan = p + o; o += al256(scan_workspace_bytes((int64_t)m));
+    w.total = reinterpret_cast<unsigned long long*>(p + o);
+    w.probe_status = reinterpret_cast<int*>(p + o + 8);
+    w.max_bits = reinterpret_cast<unsigned*>(p + o + 12);
+    w.plan = reinterpret_cast<SplitPlan*>(p + o + 16);
+    o += 256;
+    if (bytes) *bytes = o;
+    return w;
+}
+
+// One counting pass under `plan` (quotas when given): per-face counts into
+// w.counts, their exclusive scan into offsets [M+1]; returns the total, or -1
+// when a family or the call exceeded the limits.
+static int64_t count_pass(const SplitParams& P, SplitPlan plan, const int* quota, int M, const float* verts,
+                          const int* faces, const int* valid, int64_t* offsets, const SplitWs& w, cudaStream_t st,
+                          int* rc) {
+    *rc = DS_OK;
+    if (cudaMemsetAsync(w.total, 0, 16, st) != cudaSuccess) { *rc = check_launch("split_soup_count"); return -1; }
+    if (M > 0)
+        split_count_kernel<<<blocks_for(M, kSplitThreads), kSplitThreads, 0, st>>>(P, plan, M, verts, faces, valid,
+                                                                                    quota, w.counts, w.probe_status,
+                                                                                    w.total);
+    int64_t* total_dev = nullptr;
+    if ((*rc = device_scan<int, int64_t>(w.counts, M, offsets, false, w.scan, st, &total_dev))) return -1;
+    int64_t total = 0;
+    int pst = 0;
+    if (cudaMemcpyAsync(offsets + M, total_dev, sizeof(int64_t), cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(&total, total_dev, sizeof(int64_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(&pst, w.probe_status, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+        *rc = check_launch("split_soup_count");
+        return -1;
+    }
+    if ((*rc = check_launch("split_soup_count"))) return -1;
+    return (pst & DS_STATUS_SPLIT_LIMIT) ? -1 : total;
+}
+
+static float bits_float(unsigned b) { float f; std::memcpy(&f, &b, 4); return f; }
+static unsigned float_bits(float f) { unsigned b; std::memcpy(&b, &f, 4); return b; }
 
 }  // namespace dsb
 
@@ -263,54 +362,148 @@ using namespace dsb;
 extern "C" {
 
 size_t ds_split_soup_workspace_size(int M) {
-    return al256((size_t)(M > 0 ? M : 1) * sizeof(int)) + al256(scan_workspace_bytes(M > 0 ? M : 1)) + 256;
+    size_t b = 0;
+    carve_split(nullptr, M, &b);
+    return b;
 }
 
-int ds_split_soup_count(int mode, const float* mvp_host, float aspect_wh, float tau, int N, const float* verts, int M,
-                        const int* faces, const int* valid, int64_t* split_offsets, int64_t* total_splits_host,
-                        void* workspace, size_t workspace_bytes, int* status, ds_stream_t stream) {
+int ds_split_soup_count(int mode, const float* mvp_host, float aspect_wh, float tau, int num_splits, int N,
+                        const float* verts, int M, const int* faces, const int* valid, int64_t* split_offsets,
+                        int64_t* total_splits_host, void* workspace, size_t workspace_bytes, int* status,
+                        ds_stream_t stream) {
     SplitParams P;
-    int rc = make_params(mode, mvp_host, aspect_wh, tau, P);
+    int rc = make_params(mode, mvp_host, aspect_wh, P);
     if (rc) return rc;
     DS_CHECK_ARG(N >= 0 && M >= 0 && total_splits_host && split_offsets && status, "split_soup: bad arguments");
     DS_CHECK_ARG(M == 0 || (verts && faces), "split_soup: null pointer");
     DS_CHECK_ARG(workspace && workspace_bytes >= ds_split_soup_workspace_size(M), "split_soup: workspace too small");
     cudaStream_t st = (cudaStream_t)stream;
-    char* ws = reinterpret_cast<char*>(workspace);
-    int* counts = reinterpret_cast<int*>(ws);
-    void* scan_ws = ws + al256((size_t)(M > 0 ? M : 1) * sizeof(int));
-    unsigned long long* total = reinterpret_cast<unsigned long long*>(
-        ws + al256((size_t)(M > 0 ? M : 1) * sizeof(int)) + al256(scan_workspace_bytes(M > 0 ? M : 1)));
-    DS_CUDA(cudaMemsetAsync(total, 0, sizeof(unsigned long long), st));
-    // threshold mode only: the reference splits nothing unless the threshold is positive
-    const bool active = tau > 0.f && M > 0;
-    if (active)
-        split_count_kernel<<<blocks_for(M, kSplitThreads), kSplitThreads, 0, st>>>(P, M, verts, faces,
-                                                                                    mode == 1 ? valid : nullptr,
-                                                                                    counts, status, total);
-    else if (M > 0)
-        DS_CUDA(cudaMemsetAsync(counts, 0, (size_t)M * sizeof(int), st));
-    int64_t* total_dev = nullptr;
-    if ((rc = device_scan<int, int64_t>(counts, M, split_offsets, false, scan_ws, st, &total_dev))) return rc;
-    DS_CUDA(cudaMemcpyAsync(split_offsets + M, total_dev, sizeof(int64_t), cudaMemcpyDeviceToDevice, st));
-    DS_CUDA(cudaMemcpyAsync(total_splits_host, total_dev, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    const SplitWs w = carve_split(workspace, M, nullptr);
+    const int* vmask = mode == 1 ? valid : nullptr;
+    // world: tau; clip: tau = 2 * tau_ratio (NDC spans 2 per image height)
+    const float tt = mode == 0 ? tau : 2.0f * tau;
+    const float tau2 = tt * tt;
+    SplitPlan plan{INFINITY, 0.f};  // splits nothing
+    if (M > 0) DS_CUDA(cudaMemsetAsync(w.quota, 0, (size_t)M * sizeof(int), st));
+    DS_CUDA(cudaMemsetAsync(w.probe_status, 0, sizeof(int), st));
+    int64_t total = 0;
+    if (num_splits < 0 && tau > 0.f) {
+        // threshold mode (the *_until functions): every edge of at least tau
+        plan = SplitPlan{tau2, 0.f};
+        total = count_pass(P, plan, nullptr, M, verts, faces, vmask, split_offsets, w, st, &rc);
+        if (rc) return rc;
+        if (total < 0) DS_CUDA(cudaMemcpyAsync(status, w.probe_status, sizeof(int), cudaMemcpyDeviceToDevice, st));
+    } else if (num_splits > 0 && M > 0) {
+        // split budget K: the reference pops edges longest first until K splits, so it performs the K longest
+        // splits of all the faces' split trees (a child's edges are shorter than the edge its parent split).
+        // Search the squared length lam with count(lam) <= K < count(prev(lam)); the R = K - count(lam) missing
+        // splits are edges of exactly prev(lam), taken in face order (the reference's heap takes such ties in
+        // an unspecified order).
+        const int64_t K = num_splits;
+        if (tau > 0.f) {
+            total = count_pass(P, SplitPlan{tau2, 0.f}, nullptr, M, verts, faces, vmask, split_offsets, w, st, &rc);
+            if (rc) return rc;
+            if (total >= 0 && total <= K) plan = SplitPlan{tau2, 0.f};
+        }
+        if (!(plan.tau2 < INFINITY)) {
+            DS_CUDA(cudaMemsetAsync(w.max_bits, 0, sizeof(unsigned), st));
+            split_max_edge_kernel<<<blocks_for(M, kSplitThreads), kSplitThreads, 0, st>>>(P, M, verts, faces, vmask,
+                                                                                        w.max_bits);
+            unsigned hi_bits = 0;
+            DS_CUDA(cudaMemcpyAsync(&hi_bits, w.max_bits, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+            DS_CUDA(cudaStreamSynchronize(st));
+            const unsigned floor_bits = tau > 0.f ? float_bits(tau2) : 1u;  // lam stays >= tau^2 (> 0)
+            if (hi_bits == 0 || hi_bits < floor_bits) {
+                total = 0;  // nothing reaches the threshold
+            } else {
+                // count(hi) <= K is not certain (equal longest edges): walk down until count > K or the floor
+                unsigned ok = hi_bits + 1, bad = 0;  // count(ok) <= K, count(bad) > K
+                bool have_bad = false;
+                unsigned probe = hi_bits;
+                for (int it = 0; it < 64 && !have_bad; ++it) {
+                    const int64_t c = count_pass(P, SplitPlan{bits_float(probe), 0.f}, nullptr, M, verts, faces,
+                                                 vmask, split_offsets, w, st, &rc);
+                    if (rc) return rc;
+                    if (c < 0 || c > K) { bad = probe; have_bad = true; break; }
+                    ok = probe;
+                    if (probe == floor_bits) break;
+                    // halve the squared length (one exponent step), not below the floor
+                    probe = probe > floor_bits + (1u << 23) ? probe - (1u << 23) : floor_bits;
+                }
+                if (have_bad) {
+                    while (ok - bad > 1) {
+                        const unsigned mid = bad + (ok - bad) / 2;
+                        const int64_t c = count_pass(P, SplitPlan{bits_float(mid), 0.f}, nullptr, M, verts, faces,
+                                                     vmask, split_offsets, w, st, &rc);
+                        if (rc) return rc;
+                        if (c < 0 || c > K) bad = mid; else ok = mid;
+                    }
+                }
+                // lam = the smallest length whose count fits; when even the longest edges exceed the budget,
+                // lam lies above them and only the cut-off ties are split
+                plan = SplitPlan{bits_float(ok), have_bad ? bits_float(ok - 1) : 0.f};
+                total = count_pass(P, SplitPlan{plan.tau2, 0.f}, nullptr, M, verts, faces, vmask, split_offsets, w,
+                                   st, &rc);
+                if (rc) return rc;
+                const int64_t extra = K - total;
+                if (have_bad && total >= 0 && extra > 0) {
+                    // ties[t] = count_t(prev(lam)) - count_t(lam); quota = their first `extra` in face order
+                    DS_CUDA(cudaMemcpyAsync(w.quota, w.counts, (size_t)M * sizeof(int), cudaMemcpyDeviceToDevice,
+                                            st));
+                    const int64_t c2 = count_pass(P, SplitPlan{plan.tie2, 0.f}, nullptr, M, verts, faces, vmask,
+                                                  split_offsets, w, st, &rc);
+                    if (rc) return rc;
+                    if (c2 < 0) {
+                        total = -1;
+                    } else {
+                        split_diff_kernel<<<blocks_for(M, kSplitThreads), kSplitThreads, 0, st>>>(M, w.quota,
+                                                                                                   w.counts);
+                        if ((rc = device_scan<int, int64_t>(w.counts, M, split_offsets, false, w.scan, st))) return rc;
+                        split_quota_kernel<<<blocks_for(M, kSplitThreads), kSplitThreads, 0, st>>>(
+                            M, w.counts, split_offsets, extra, w.quota);
+                        total = count_pass(P, plan, w.quota, M, verts, faces, vmask, split_offsets, w, st, &rc);
+                        if (rc) return rc;
+                    }
+                } else {
+                    plan.tie2 = 0.f;
+                }
+            }
+        }
+        if (total < 0) DS_CUDA(cudaMemcpyAsync(status, w.probe_status, sizeof(int), cudaMemcpyDeviceToDevice, st));
+    }
+    if (total == 0) {
+        // nothing to split: zero offsets
+        plan = SplitPlan{INFINITY, 0.f};
+        if (M > 0) DS_CUDA(cudaMemsetAsync(w.counts, 0, (size_t)M * sizeof(int), st));
+        if ((rc = device_scan<int, int64_t>(w.counts, M, split_offsets, false, w.scan, st))) return rc;
+        DS_CUDA(cudaMemsetAsync(split_offsets + M, 0, sizeof(int64_t), st));
+        total = 0;
+    }
+    if (total < 0) {
+        int one = DS_STATUS_SPLIT_LIMIT;
+        DS_CUDA(cudaMemcpyAsync(status, &one, sizeof(int), cudaMemcpyHostToDevice, st));
+        total = 0;
+    }
+    DS_CUDA(cudaMemcpyAsync(w.plan, &plan, sizeof(SplitPlan), cudaMemcpyHostToDevice, st));
     DS_CUDA(cudaStreamSynchronize(st));
+    *total_splits_host = total;
     return check_launch("split_soup_count");
 }
 
-int ds_split_soup_emit(int mode, const float* mvp_host, float aspect_wh, float tau, int N, const float* verts, int M,
-                       const int* faces, const int* valid, const int64_t* split_offsets, int64_t total_splits,
+int ds_split_soup_emit(int mode, const float* mvp_host, float aspect_wh, int N, const float* verts, int M,
+                       const int* faces, const int64_t* split_offsets, int64_t total_splits, const void* workspace,
                        float* out_verts, int* out_faces, int* out_map, int* out_flag, int* status,
                        ds_stream_t stream) {
     SplitParams P;
-    int rc = make_params(mode, mvp_host, aspect_wh, tau, P);
+    int rc = make_params(mode, mvp_host, aspect_wh, P);
     if (rc) return rc;
-    DS_CHECK_ARG(N >= 0 && M >= 0 && total_splits >= 0 && split_offsets && status, "split_soup: bad arguments");
+    DS_CHECK_ARG(N >= 0 && M >= 0 && total_splits >= 0 && split_offsets && status && workspace,
+                 "split_soup: bad arguments");
     DS_CHECK_ARG((int64_t)N + 3 * total_splits <= 0x7fffffff && (int64_t)M + total_splits <= 0x7fffffff,
                  "split_soup: %lld splits exceed the int32 vertex and face indices", (long long)total_splits);
     DS_CHECK_ARG(M == 0 || (verts && faces && out_verts && out_faces && out_map && out_flag),
                  "split_soup: null pointer");
-    (void)valid;  // the counting pass already applied the mask: families with no splits stay as they are
+    const SplitWs w = carve_split(const_cast<void*>(workspace), M, nullptr);
     cudaStream_t st = (cudaStream_t)stream;
     if (N > 0) {
         const unsigned b = blocks_for((int64_t)N * 3);
@@ -319,7 +512,7 @@ int ds_split_soup_emit(int mode, const float* mvp_host, float aspect_wh, float t
     }
     if (M > 0)
         split_emit_kernel<<<blocks_for(M, kSplitThreads), kSplitThreads, 0, st>>>(
-            P, N, M, verts, faces, valid, split_offsets, out_verts, out_faces, out_map, out_flag, status);
+            P, w.plan, N, M, verts, faces, w.quota, split_offsets, out_verts, out_faces, out_map, out_flag, status);
     return check_launch("split_soup_emit");
 }
 

@@ -6,9 +6,10 @@ The reference splits on the CPU with a global priority queue of edges
 independently, so here each input face walks its own split tree on the GPU:
 the same triangles as the reference, bit for bit, with the new vertices and
 faces numbered per input face (depth first) instead of in the queue's global
-order.  Training uses the threshold mode (`*_until`, num_splits = -1); that is
-the mode computed here.  A positive split budget (num_splits > 0) depends on
-the global order of the queue and is not provided: it raises.
+order.  Training uses the threshold mode (`*_until`, num_splits = -1).  A
+split budget (num_splits > 0) keeps the queue's global choice: the
+num_splits longest splits, found by a search over counting passes; splits of
+exactly equal length at the cut-off are taken in face order.
 """
 
 from __future__ import annotations
@@ -27,15 +28,11 @@ DS_STATUS_SPLIT_LIMIT = 4
 
 def _split(mode: int, verts: torch.Tensor, faces: torch.Tensor, num_splits: int, tau: float,
            mvp: torch.Tensor = None, valid: torch.Tensor = None, aspect_wh: float = 1.0) -> Quad:
-    if num_splits > 0:
-        raise NotImplementedError("split budget (num_splits > 0): only the threshold mode (num_splits = -1, "
-                                  "the *_until functions) runs on the GPU")
     out_dev = verts.device
     dev = out_dev if out_dev.type == "cuda" else torch.device("cuda", torch.cuda.current_device())
     v = verts.detach().to(dev, torch.float32).contiguous()
     f = faces.detach().to(dev, torch.int32).contiguous()
     N, M = v.shape[0], f.shape[0]
-    active = num_splits < 0 and tau > 0.0
     vm = None
     if mode == 1:
         vm = valid.detach().to(dev, torch.int32).contiguous()
@@ -47,7 +44,7 @@ def _split(mode: int, verts: torch.Tensor, faces: torch.Tensor, num_splits: int,
         status = torch.zeros(1, dtype=torch.int32, device=dev)
         ws = _core.workspace(_core.lib.ds_split_soup_workspace_size(M), dev)
         total = C.c_int64(0)
-        _core.check(_core.lib.ds_split_soup_count(mode, m_host, float(aspect_wh), float(tau if active else 0.0), N,
+        _core.check(_core.lib.ds_split_soup_count(mode, m_host, float(aspect_wh), float(tau), int(num_splits), N,
                                                   _core.ptr(v), M, _core.ptr(f), _core.ptr(vm), _core.ptr(offsets),
                                                   C.byref(total), _core.ptr(ws), ws.numel(), _core.ptr(status),
                                                   _core.stream()))
@@ -59,10 +56,10 @@ def _split(mode: int, verts: torch.Tensor, faces: torch.Tensor, num_splits: int,
         out_f = torch.empty(M + S, 3, dtype=torch.int32, device=dev)
         out_map = torch.empty(M + S, dtype=torch.int32, device=dev)
         out_flag = torch.empty(M + S, dtype=torch.int32, device=dev)
-        _core.check(_core.lib.ds_split_soup_emit(mode, m_host, float(aspect_wh), float(tau if active else 0.0), N,
-                                                 _core.ptr(v), M, _core.ptr(f), _core.ptr(vm), _core.ptr(offsets), S,
-                                                 _core.ptr(out_v), _core.ptr(out_f), _core.ptr(out_map),
-                                                 _core.ptr(out_flag), _core.ptr(status), _core.stream()))
+        _core.check(_core.lib.ds_split_soup_emit(mode, m_host, float(aspect_wh), N, _core.ptr(v), M, _core.ptr(f),
+                                                 _core.ptr(offsets), S, _core.ptr(ws), _core.ptr(out_v),
+                                                 _core.ptr(out_f), _core.ptr(out_map), _core.ptr(out_flag),
+                                                 _core.ptr(status), _core.stream()))
     return (out_v.to(out_dev), out_f.to(out_dev), out_map.to(out_dev), out_flag.to(out_dev))
 
 

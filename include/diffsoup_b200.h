@@ -336,34 +336,42 @@ int ds_project_vertices(int B, int V, const float* verts, const float* mvp, floa
 
 /* replaces _core.split_triangle_soup (src/main.cpp:308-340, src/remesh.cpp)
  * with mode 0 and _core.split_triangle_soup_clip (src/main.cpp:342-388,
- * src/remesh_clip.cpp) with mode 1, in threshold mode (num_splits = -1, the
- * reference's `*_until` functions that training calls, examples/utils.py:540):
- * every face is bisected at its longest edge while that edge's squared length
- * is at least tau^2 (mode 0: world units) or (2 tau)^2 (mode 1: tau is the
- * reference's tau_ratio in image heights; lengths in NDC with x scaled by
- * aspect_wh = W/H, edges with an end outside the NDC cube ignored, faces with
- * valid[t] <= 0 left as they are).  mvp_host: row-major 4x4 in host memory
- * (mode 1; NULL in mode 0).  tau <= 0 splits nothing, as in the reference.
+ * src/remesh_clip.cpp) with mode 1.  A face is bisected at its longest edge
+ * (squared length in world units, mode 0; in mode 1 in NDC with x scaled by
+ * aspect_wh = W/H, edges with an end outside the NDC cube ignored, faces
+ * with valid[t] <= 0 never split); both halves continue.  num_splits < 0
+ * (the reference's `*_until` functions, which training calls,
+ * examples/utils.py:540): split while the longest edge is at least tau
+ * (mode 0) or 2 tau (mode 1: tau is the reference's tau_ratio in image
+ * heights); tau <= 0 splits nothing.  num_splits > 0: the num_splits longest
+ * splits of all faces, as the reference's queue pops them, stopping early at
+ * the threshold when tau > 0; splits of exactly equal length at the cut-off
+ * are taken in face order (the reference's heap takes them in an unspecified
+ * order).  num_splits == 0: nothing.  mvp_host: row-major 4x4 in host memory
+ * (mode 1; NULL in mode 0).
  *
- * Two calls.  ds_split_soup_count writes split_offsets [M+1] (int64, device):
- * the exclusive offsets of each face's splits and their total, which it also
- * returns in *total_splits_host; host-synchronising, like the reference's
+ * Two calls on one workspace.  ds_split_soup_count writes split_offsets [M+1]
+ * (int64, device): the exclusive offsets of each face's splits and their
+ * total, which it also returns in *total_splits_host; host-synchronising (a
+ * split budget runs a search of counting passes), like the reference's
  * binding returning its arrays.  A face whose split tree would exceed 2^20
- * splits or a depth of 40, or a call above 2^27 splits, sets
- * DS_STATUS_SPLIT_LIMIT in *status (device int) and must not be emitted.
- * ds_split_soup_emit then writes, for S = total splits: out_verts [N+3S,3]
- * (the inputs, then per split the two copies of the split point and the copy
- * of the opposite vertex), out_faces [M+S,3], out_map [M+S] (input face of
- * each output face) and out_flag [M+S] (1 for faces never split), the
- * reference's four outputs.  The same triangles as the reference, bit for bit;
- * new vertices and faces are numbered per input face in depth-first order
- * (the reference's follow its global queue order). */
+ * splits or a depth of 40, or a pass above 2^27 splits, sets
+ * DS_STATUS_SPLIT_LIMIT in *status (device int); do not emit then.
+ * ds_split_soup_emit follows the plan the count call left in the workspace
+ * and writes, for S = total splits: out_verts [N+3S,3] (the inputs, then per
+ * split the two copies of the split point and the copy of the opposite
+ * vertex), out_faces [M+S,3], out_map [M+S] (input face of each output face)
+ * and out_flag [M+S] (1 for faces never split), the reference's four outputs.
+ * The same triangles as the reference, bit for bit; new vertices and faces
+ * are numbered per input face in depth-first order (the reference's follow its
+ * global queue order). */
 size_t ds_split_soup_workspace_size(int M);
-int ds_split_soup_count(int mode, const float* mvp_host, float aspect_wh, float tau, int N, const float* verts, int M,
-                        const int* faces, const int* valid, int64_t* split_offsets, int64_t* total_splits_host,
-                        void* workspace, size_t workspace_bytes, int* status, ds_stream_t stream);
-int ds_split_soup_emit(int mode, const float* mvp_host, float aspect_wh, float tau, int N, const float* verts, int M,
-                       const int* faces, const int* valid, const int64_t* split_offsets, int64_t total_splits,
+int ds_split_soup_count(int mode, const float* mvp_host, float aspect_wh, float tau, int num_splits, int N,
+                        const float* verts, int M, const int* faces, const int* valid, int64_t* split_offsets,
+                        int64_t* total_splits_host, void* workspace, size_t workspace_bytes, int* status,
+                        ds_stream_t stream);
+int ds_split_soup_emit(int mode, const float* mvp_host, float aspect_wh, int N, const float* verts, int M,
+                       const int* faces, const int64_t* split_offsets, int64_t total_splits, const void* workspace,
                        float* out_verts, int* out_faces, int* out_map, int* out_flag, int* status,
                        ds_stream_t stream);
 

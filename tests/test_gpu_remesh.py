@@ -91,3 +91,43 @@ def test_resampling_step_keeps_the_mapping():
     pts = V[F.long()]  # [M',3,3]
     d = ((pts - v0[fmap][:, :1]) * n[fmap][:, None, :]).sum(-1)
     assert float(d.abs().max()) < 1e-4
+
+
+@pytest.mark.skipif(not R.reference_available(), reason="oracle/_ref/libremesh_ref.so not built")
+@pytest.mark.parametrize("mode,K,tau", [("world", 500, 0.0), ("world", 300, 0.1), ("world", 10 ** 6, 0.2),
+                                        ("clip", 1000, 0.005), ("clip", 40, 0.0)])
+def test_split_budget_matches_reference(mode, K, tau):
+    """num_splits > 0: the K longest splits over all faces, as the reference's
+    queue pops them (stopping early at the threshold when tau > 0)."""
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(DEV)  # noqa: E731
+    if mode == "world":
+        v, f = _soup(200, seed=11)
+        got = _np(remesh.split_triangle_soup(t(v), t(f), K, tau=tau))
+        ref = R.reference_split(v, f, K, tau)
+    else:
+        sc = scenes.make_scene(2, seed=5, num_tris=300, num_views=1, resolution=(600, 800), with_targets=False)
+        valid = (np.random.default_rng(5).random(sc.T) < 0.8).astype(np.int32)
+        mvp = sc.mvps()[0]
+        got = _np(remesh.split_triangle_soup_clip((600, 800), t(mvp), t(sc.verts), t(sc.tri), t(valid), K,
+                                                  tau_ratio=tau))
+        ref = R.reference_split(sc.verts, sc.tri, K, tau, mvp=mvp, valid=valid, aspect_wh=800 / 600)
+    assert got[1].shape == ref[1].shape and got[0].shape == ref[0].shape
+    assert R.families(*got) == R.families(*ref)
+
+
+def test_split_budget_with_equal_edges():
+    """Congruent faces tie at every length: the budget is met exactly and the
+    ties go to the lower faces first."""
+    base = np.array([[0, 0, 0], [1, 0, 0], [0, 0.7, 0]], np.float32)
+    v = np.concatenate([base + np.float32(2 * i) for i in range(10)]).astype(np.float32)
+    f = np.arange(30, dtype=np.int32).reshape(10, 3)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(DEV)  # noqa: E731
+    got = _np(remesh.split_triangle_soup(t(v), t(f), 15, tau=0.0))
+    assert got[1].shape[0] == 10 + 15 and got[0].shape[0] == 30 + 3 * 15
+    if R.reference_available():
+        ref = R.reference_split(v, f, 15, 0.0)
+        assert ref[1].shape == got[1].shape
+    # every face splits its hypotenuse (10 splits), then the next longest edges (one leg per face, all
+    # equal) take the remaining 5 in face order: faces 0..4 end with 3 triangles, faces 5..9 with 2
+    per_face = np.bincount(got[2], minlength=10)
+    assert per_face.tolist() == [3] * 5 + [2] * 5

@@ -68,8 +68,6 @@ def test_thresholds_that_split_nothing():
 
 def test_product_argument_checks():
     v, f = _soup(4, seed=4)
-    with pytest.raises(NotImplementedError):
-        remesh.split_triangle_soup(torch.from_numpy(v), torch.from_numpy(f), 10, tau=0.1)
     src = torch.arange(5.0)
     assert torch.equal(remesh.expand_by_index(src, torch.tensor([4, 0, 0])), torch.tensor([4.0, 0.0, 0.0]))
     with pytest.raises(ValueError):
