@@ -83,12 +83,14 @@ __device__ __forceinline__ ClipPoint clip_point(const SplitParams& P, const floa
 
 // Squared length of edge (A, B) in the metric: world (remesh.h:41-48) or
 // image-height units, 0 when an end leaves the NDC cube (remesh_clip.cpp:33-78).
-__device__ __forceinline__ float edge_len2(const SplitParams& P, const float* A, const float* B) {
+// a, b: the ends' clip points (clip mode; a pure function of the world point,
+// so computing them once per vertex gives the reference's values).
+__device__ __forceinline__ float edge_len2(const SplitParams& P, const float* A, const float* B, const ClipPoint& a,
+                                           const ClipPoint& b) {
     if (P.mode == 0) {
         const float dx = __fsub_rn(B[0], A[0]), dy = __fsub_rn(B[1], A[1]), dz = __fsub_rn(B[2], A[2]);
         return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
     }
-    const ClipPoint a = clip_point(P, A), b = clip_point(P, B);
     if (!a.inside || !b.inside) return 0.f;
     const float dx = __fmul_rn(__fsub_rn(a.n[0], b.n[0]), P.aspect), dy = __fsub_rn(a.n[1], b.n[1]);
     return __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
@@ -96,13 +98,13 @@ __device__ __forceinline__ float edge_len2(const SplitParams& P, const float* A,
 
 // The split point of edge (A, B): the midpoint in world space, or the point
 // whose projection is the NDC midpoint (remesh_clip.cpp:100-145).
-__device__ __forceinline__ void split_point(const SplitParams& P, const float* A, const float* B, float* C) {
+__device__ __forceinline__ void split_point(const SplitParams& P, const float* A, const float* B, const ClipPoint& a,
+                                            const ClipPoint& b, float* C) {
     if (P.mode == 0) {
 #pragma unroll
         for (int k = 0; k < 3; ++k) C[k] = __fmul_rn(0.5f, __fadd_rn(A[k], B[k]));
         return;
     }
-    const ClipPoint a = clip_point(P, A), b = clip_point(P, B);
     const float nx = __fmul_rn(0.5f, __fadd_rn(a.n[0], b.n[0]));
     const float ny = __fmul_rn(0.5f, __fadd_rn(a.n[1], b.n[1]));
     const float dx = __fsub_rn(b.c[0], a.c[0]), dy = __fsub_rn(b.c[1], a.c[1]), dw = __fsub_rn(b.c[3], a.c[3]);
@@ -136,6 +138,11 @@ __device__ int64_t walk_family(const SplitParams& P, SplitPlan plan, int quota, 
         for (int j = 0; j < 3; ++j) cur.p[k * 3 + j] = verts[(size_t)cur.id[k] * 3 + j];
     }
     cur.slot = t;
+    ClipPoint q[3];  // clip points of cur's corners (clip mode)
+    if (P.mode == 1) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) q[k] = clip_point(P, cur.p + k * 3);
+    }
     int64_t splits = 0;
     bool stop = !splittable;
     while (true) {
@@ -145,7 +152,7 @@ __device__ int64_t walk_family(const SplitParams& P, SplitPlan plan, int quota, 
         if (!stop) {
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                const float l2 = edge_len2(P, cur.p + k * 3, cur.p + ((k + 1) % 3) * 3);
+                const float l2 = edge_len2(P, cur.p + k * 3, cur.p + ((k + 1) % 3) * 3, q[k], q[(k + 1) % 3]);
                 const bool considered = P.mode == 0 || l2 > 0.f;
                 if (considered && (e < 0 || l2 > best)) { e = k; best = l2; }
             }
@@ -167,7 +174,7 @@ __device__ int64_t walk_family(const SplitParams& P, SplitPlan plan, int quota, 
             }
             const int ia = e, ib = (e + 1) % 3, ic = (e + 2) % 3;  // edge (a, b), opposite c
             float C[3];
-            split_point(P, cur.p + ia * 3, cur.p + ib * 3, C);
+            split_point(P, cur.p + ia * 3, cur.p + ib * 3, q[ia], q[ib], C);
             if (tie && !(best >= plan.tau2)) --quota;
             const int64_t k = splits++;
             const int mA = (int)(vbase + 3 * k), mB = mA + 1, cA = mA + 2;
@@ -200,6 +207,12 @@ __device__ int64_t walk_family(const SplitParams& P, SplitPlan plan, int quota, 
             }
             stack[top++] = second;
             cur = first;
+            if (P.mode == 1) {  // corners (a, C, c)
+                const ClipPoint qa = q[ia], qc = q[ic];
+                q[0] = qa;
+                q[1] = clip_point(P, C);
+                q[2] = qc;
+            }
             continue;
         }
         if (EMIT) {
@@ -208,6 +221,10 @@ __device__ int64_t walk_family(const SplitParams& P, SplitPlan plan, int quota, 
         }
         if (top == 0) break;
         cur = stack[--top];
+        if (P.mode == 1) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) q[k] = clip_point(P, cur.p + k * 3);
+        }
     }
     return splits;
 }
@@ -260,8 +277,10 @@ __global__ void __launch_bounds__(kSplitThreads) split_max_edge_kernel(SplitPara
     float p[9];
     for (int k = 0; k < 3; ++k)
         for (int j = 0; j < 3; ++j) p[k * 3 + j] = verts[(size_t)faces[(size_t)t * 3 + k] * 3 + j];
+    ClipPoint q[3];
+    for (int k = 0; k < 3; ++k) q[k] = P.mode == 1 ? clip_point(P, p + k * 3) : ClipPoint{};
     float best = 0.f;
-    for (int k = 0; k < 3; ++k) best = fmaxf(best, edge_len2(P, p + k * 3, p + ((k + 1) % 3) * 3));
+    for (int k = 0; k < 3; ++k) best = fmaxf(best, edge_len2(P, p + k * 3, p + ((k + 1) % 3) * 3, q[k], q[(k + 1) % 3]));
     atomicMax(max_bits, __float_as_uint(best));
 }
 
