@@ -131,3 +131,24 @@ def test_split_budget_with_equal_edges():
     # equal) take the remaining 5 in face order: faces 0..4 end with 3 triangles, faces 5..9 with 2
     per_face = np.bincount(got[2], minlength=10)
     assert per_face.tolist() == [3] * 5 + [2] * 5
+
+
+def test_degenerate_and_empty_soups():
+    v, f = _soup(40, seed=9)
+    v[0:3] = v[0]
+    v[3:6] = [[0, 0, 0], [1, 0.001, 0.0003], [2.7, 0.002, 0.0001]]
+    f[10] = f[9]
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(DEV)  # noqa: E731
+    for tau in (0.05, 0.3):
+        _equal(_np(remesh.split_triangle_soup_until(t(v), t(f), tau)), R.restated_split(v, f, tau))
+    got = _np(remesh.split_triangle_soup_until(t(np.zeros((0, 3), np.float32)), t(np.zeros((0, 3), np.int32)), 0.1))
+    assert got[0].shape == (0, 3) and got[1].shape == (0, 3)
+    # no face valid: nothing splits, everything is flagged as original
+    sc = scenes.make_scene(1, seed=9, num_tris=30, num_views=1, resolution=(64, 64), with_targets=False)
+    got = _np(remesh.split_triangle_soup_clip_until((64, 64), t(sc.mvps()[0]), t(sc.verts), t(sc.tri),
+                                                    t(np.zeros(sc.T, np.int32)), 0.01))
+    assert got[1].shape == sc.tri.shape and (got[3] == 1).all() and np.array_equal(got[1], sc.tri)
+    # CPU tensors in, CPU tensors out (computed on the GPU)
+    cpu = remesh.split_triangle_soup_until(torch.from_numpy(v), torch.from_numpy(f), 0.3)
+    assert cpu[0].device.type == "cpu"
+    _equal(tuple(x.numpy() for x in cpu), R.restated_split(v, f, 0.3))

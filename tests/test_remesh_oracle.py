@@ -74,3 +74,28 @@ def test_product_argument_checks():
         remesh.expand_by_index(src, torch.tensor([5]))
     with pytest.raises(TypeError):
         remesh.expand_by_index(src, [1])
+
+
+def test_degenerate_faces_match_reference():
+    """A point face (every edge of length 0), a sliver, two faces on the same
+    vertices and an empty soup, in both metrics.  (A face with two edges of
+    equal float length, such as one with a vanishing edge, is split at either
+    in the reference, by its heap's order; such faces are left out.)"""
+    rng = np.random.default_rng(9)
+    v, f = _soup(40, seed=9)
+    v[0:3] = v[0]                        # a point face
+    v[3:6] = [[0, 0, 0], [1, 0.001, 0.0003], [2.7, 0.002, 0.0001]]  # a sliver (exactly collinear corners give exact ties, unordered in the reference)
+    f[10] = f[9]                          # two faces on the same vertices
+    for tau in (0.05, 0.3):
+        _same(R.reference_split(v, f, -1, tau), R.restated_split(v, f, tau), v.shape[0])
+    sc = scenes.make_scene(1, seed=9, num_tris=30, num_views=1, resolution=(64, 64), with_targets=False)
+    valid = np.ones(sc.T, np.int32)
+    verts = sc.verts.copy()
+    verts[0:3] = verts[0]
+    ref = R.reference_split(verts, sc.tri, -1, 0.05, mvp=sc.mvps()[0], valid=valid, aspect_wh=1.0)
+    res = R.restated_split(verts, sc.tri, 0.05, mvp=sc.mvps()[0], valid=valid, aspect_wh=1.0)
+    _same(ref, res, verts.shape[0])
+    empty = (np.zeros((0, 3), np.float32), np.zeros((0, 3), np.int32))
+    e_ref = R.reference_split(*empty, -1, 0.1)
+    e_res = R.restated_split(*empty, 0.1)
+    assert e_ref[1].shape == e_res[1].shape == (0, 3)
