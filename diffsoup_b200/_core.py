@@ -238,3 +238,25 @@ def accumulate_to_level_backward(min_level: int, max_level: int, target_level: i
     T, S, Cd = grad_feat_all.shape
     check(_lib.ds_accumulate_to_level_backward(T, min_level, max_level, target_level, S, grad_feat_max.shape[1], Cd,
                                                ptr(grad_feat_all), ptr(grad_feat_max), stream()))
+
+
+def split_triangle_soup(verts, faces, numSplits: int, tau: float):
+    """_core.split_triangle_soup (src/main.cpp:308-340): numpy verts [N,3] f32,
+    faces [M,3] i32 -> numpy (verts, faces, face_mapping, face_flags), split
+    on the GPU (csrc/remesh.cu)."""
+    import numpy as np
+    from . import remesh
+    out = remesh._split(0, torch.from_numpy(np.ascontiguousarray(verts, np.float32)),
+                        torch.from_numpy(np.ascontiguousarray(faces, np.int32)), int(numSplits), float(tau))
+    return tuple(x.numpy() for x in out)
+
+
+def split_triangle_soup_clip(mvp, verts, faces, valid_faces, numSplits: int, tau_ratio: float, aspectWH: float):
+    """_core.split_triangle_soup_clip (src/main.cpp:342-388): numpy arguments
+    and results as the reference's binding, split on the GPU."""
+    import numpy as np
+    from . import remesh
+    t = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a, dt))  # noqa: E731
+    out = remesh._split(1, t(verts, np.float32), t(faces, np.int32), int(numSplits), float(tau_ratio),
+                        mvp=t(mvp, np.float32), valid=t(valid_faces, np.int32), aspect_wh=float(aspectWH))
+    return tuple(x.numpy() for x in out)

@@ -152,3 +152,17 @@ def test_degenerate_and_empty_soups():
     cpu = remesh.split_triangle_soup_until(torch.from_numpy(v), torch.from_numpy(f), 0.3)
     assert cpu[0].device.type == "cpu"
     _equal(tuple(x.numpy() for x in cpu), R.restated_split(v, f, 0.3))
+
+
+def test_core_bindings_take_numpy():
+    """ds._core.split_triangle_soup(_clip): the reference binding's numpy
+    arguments and results (src/main.cpp:308-388)."""
+    from diffsoup_b200 import _core
+    v, f = _soup(50, seed=12)
+    got = _core.split_triangle_soup(v, f, -1, 0.1)
+    assert all(isinstance(x, np.ndarray) for x in got)
+    _equal(got, R.restated_split(v, f, 0.1))
+    sc = scenes.make_scene(2, seed=12, num_tris=100, num_views=1, resolution=(300, 400), with_targets=False)
+    valid = np.ones(sc.T, np.int32)
+    got = _core.split_triangle_soup_clip(sc.mvps()[0], sc.verts, sc.tri, valid, -1, 0.02, 400 / 300)
+    _equal(got, R.restated_split(sc.verts, sc.tri, 0.02, mvp=sc.mvps()[0], valid=valid, aspect_wh=400 / 300))
