@@ -106,3 +106,32 @@ def test_renderer_is_gpu_only(golden):
         viewer.Renderer(verts, faces, lut0, lut1, *W, level=2, device="cpu")
     with pytest.raises(RuntimeError, match="headless"):
         viewer.launch_viewer()
+
+
+def test_png_writer_round_trip(tmp_path):
+    """viewer._write_png (the screenshots of benchmark()) as a standard PNG:
+    signature, IHDR, CRCs, and the pixel rows back through zlib."""
+    import struct
+    import zlib
+
+    rng = np.random.default_rng(0)
+    img = rng.integers(0, 256, (5, 7, 4), dtype=np.uint8)
+    path = tmp_path / "x.png"
+    viewer._write_png(str(path), img)
+    data = path.read_bytes()
+    assert data[:8] == b"\x89PNG\r\n\x1a\n"
+    pos, chunks = 8, {}
+    while pos < len(data):
+        n = struct.unpack(">I", data[pos:pos + 4])[0]
+        tag, body = data[pos + 4:pos + 8], data[pos + 8:pos + 8 + n]
+        crc = struct.unpack(">I", data[pos + 8 + n:pos + 12 + n])[0]
+        assert crc == zlib.crc32(tag + body) & 0xFFFFFFFF
+        chunks[tag] = body
+        pos += 12 + n
+    w, h, depth, ctype = struct.unpack(">IIBB", chunks[b"IHDR"][:10])
+    assert (w, h, depth, ctype) == (7, 5, 8, 6)
+    raw = zlib.decompress(chunks[b"IDAT"])
+    rows = np.frombuffer(raw, np.uint8).reshape(5, 1 + 7 * 4)
+    assert (rows[:, 0] == 0).all()
+    assert np.array_equal(rows[:, 1:].reshape(5, 7, 4), img)
+    assert b"IEND" in chunks
