@@ -24,6 +24,11 @@ from .rasterize import (
     encode_view_dir_sh2,
     opacity_aux_loss,
 )
+from .point3d import (
+    nn_spacing,
+    remove_unreferenced_vertices_from_soup,
+    triangle_soup_from_points,
+)
 from .remesh import (
     expand_by_index,
     split_triangle_soup,
@@ -51,10 +56,13 @@ __all__ = [
     "expand_by_index",
     "feats_at_level",
     "multires_triangle_color",
+    "nn_spacing",
     "opacity_aux_loss",
     "rasterize_multires_triangle_alpha",
+    "remove_unreferenced_vertices_from_soup",
     "split_triangle_soup",
     "split_triangle_soup_clip",
     "split_triangle_soup_clip_until",
     "split_triangle_soup_until",
+    "triangle_soup_from_points",
 ]
