@@ -80,3 +80,43 @@ def test_train_step_binding_argument_errors():
     assert rc == 1 and b"unsupported MLP" in _core.lib.ds_last_error()
     assert S.mlp_param_count(8, 16, 1) == 16 * 11 + 16 + 3 * 16 + 3
     assert S.mlp_param_count(16, 64, 2) == 64 * 19 + 64 + 64 * 64 + 64 + 3 * 64 + 3
+
+
+def declared_prototypes():
+    """name -> list of parameter declarations of every ds_* prototype."""
+    src = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    protos = {}
+    for m in re.finditer(r"\b(ds_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", src, flags=re.S):
+        params = [p.strip() for p in m.group(2).replace("\n", " ").split(",") if p.strip()]
+        protos[m.group(1)] = [] if params == ["void"] else params
+    return protos
+
+
+def test_ctypes_signatures_match_the_header():
+    """Every binding in diffsoup_b200/_core.py passes as many arguments as
+    the header declares, with 64-bit, floating and pointer slots where the
+    header has them (an ABI drift between the two would misread arguments)."""
+    from diffsoup_b200 import _core
+
+    protos = declared_prototypes()
+    checked = 0
+    for name, params in protos.items():
+        fn = getattr(_core.lib, name)
+        if fn.argtypes is None:
+            continue
+        assert len(fn.argtypes) == len(params), (name, len(fn.argtypes), len(params))
+        for arg, decl in zip(fn.argtypes, params):
+            if "*" in decl:
+                assert arg in (C.c_void_p, C.c_char_p) or issubclass(arg, C._Pointer), (name, decl, arg)
+            elif decl.startswith(("int64_t", "size_t")):
+                assert arg in (C.c_int64, C.c_size_t), (name, decl, arg)
+            elif decl.startswith("double"):
+                assert arg is C.c_double, (name, decl, arg)
+            elif decl.startswith("float"):
+                assert arg is C.c_float, (name, decl, arg)
+            elif decl.startswith(("int ", "int32_t")):
+                assert arg is C.c_int, (name, decl, arg)
+            elif decl.startswith("ds_stream_t"):
+                assert arg is C.c_void_p, (name, decl, arg)
+        checked += 1
+    assert checked >= 30, checked
