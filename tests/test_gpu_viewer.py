@@ -127,3 +127,31 @@ def test_bin_list_overflow_stays_exact(renderer, inputs):
     assert f.capacity == 8192  # grown after the overflowing frame
     f.fit()
     assert not f.overflowed()
+
+
+def test_batched_frames_equal_single_view_frames(renderer, inputs):
+    """Views rendered in one call equal the same views rendered one by one
+    (view table offsets, per-view inverse MVPs)."""
+    H, W = inputs.height, inputs.width
+    batch = renderer.render(inputs.mvps, H, W)
+    for b in range(inputs.mvps.shape[0]):
+        assert torch.equal(batch[b], renderer.render(inputs.mvps[b:b + 1], H, W)[0]), b
+
+
+def test_post_pass_entry_point_equals_the_frame(renderer, inputs):
+    """ds_render_deferred on a frame's G-buffer gives that frame's image."""
+    from diffsoup_b200 import _core
+
+    H, W = inputs.height, inputs.width
+    f = renderer.frame(inputs.mvps, H, W)
+    f.run(want_rgb=True)
+    torch.cuda.synchronize()
+    rgb = torch.empty_like(f.rgb)
+    rgba = torch.empty_like(f.rgba8)
+    bg = renderer.background
+    _core.check(_core.lib.ds_render_deferred(f.B, _core.ptr(f.views), f.num_pixels, _core.ptr(f.gbuf), renderer.level,
+                                             _core.ptr(renderer.lut0), _core.ptr(renderer.lut1),
+                                             renderer.lut0.shape[0], _core.ptr(f.inv_mvp), _core.ptr(renderer.mlp),
+                                             bg[0], bg[1], bg[2], _core.ptr(rgb), _core.ptr(rgba), _core.stream()))
+    torch.cuda.synchronize()
+    assert torch.equal(rgb, f.rgb) and torch.equal(rgba, f.rgba8)
