@@ -216,6 +216,14 @@ def algorithmic_bytes(phase: str, P_: int, B: int, T: int, V: int, ST: int, C_: 
     return 0.0
 
 
+def step_algorithmic_bytes(B: int, T: int, V: int, S: int, C_: int, P_: int) -> float:
+    """Minimal DRAM bytes of a whole training step: 12 B per triangle, features and opacities read and
+    their gradients written (8 B per lattice sample and channel, C + 1 channels), and per view the clip
+    positions read and their gradients written (32 B per vertex) plus, per pixel, the ID buffer written
+    (16 B), the colour written (12 B), the target read (12 B) and dL/dcolour read (12 B)."""
+    return 12.0 * T + 8.0 * T * S * (C_ + 1) + B * 32.0 * V + P_ * (16.0 + 12.0 + 12.0 + 12.0)
+
+
 def run_ours(args):
     from diffsoup_b200 import scenes, _core, replicas
     from diffsoup_b200.step import TrainStep
@@ -357,6 +365,7 @@ def run_ours(args):
     peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
     achieved = alg / (phase_ms[dom] / 1000.0) / 1e9
+    step_bytes = step_algorithmic_bytes(B, T, V, _core.total_feats(sc.min_level, sc.max_level), sc.feat_dim, P_)
     traffic = read_traffic(dom)
 
     # ---------------- split-BF16 precision mode (same workload) ---------------
@@ -420,6 +429,8 @@ def run_ours(args):
         "gpu_launches": KERNELS_PER_STEP * args.steps,
         "clocks": clocks,
         "phase_ms": {k: round(v, 4) for k, v in phase_ms.items()},
+        "step_roofline": {"algorithmic_bytes": step_bytes, "achieved_gbs": step_bytes / (ms / args.steps / 1000.0)
+                          / 1e9, "frac": step_bytes / (ms / args.steps / 1000.0) / 1e9 / peak, "unit": "GB/s"},
         "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                      "algorithmic_bytes": alg},
