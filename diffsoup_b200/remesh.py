@@ -17,7 +17,6 @@ from __future__ import annotations
 import ctypes as C
 from typing import Tuple
 
-import numpy as np
 import torch
 
 from . import _core
