@@ -17,6 +17,18 @@ int set_error(int code, const char* fmt, ...) {
     return code;
 }
 
+int sm_count() {
+    constexpr int kMaxDevices = 64;
+    static int cache[kMaxDevices] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return 1;
+    if (dev < kMaxDevices && cache[dev] > 0) return cache[dev];
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) n = 1;
+    if (dev < kMaxDevices) cache[dev] = n;
+    return n;
+}
+
 int check_launch(const char* what) {
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return set_error(DS_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));

@@ -10,7 +10,15 @@
 namespace dsb {
 
 constexpr int kThreads = 256;
-constexpr int kSMs = 148;  // B200: 2 dies x 74 SMs
+
+// Streaming multiprocessors of the current device (cudaDevAttrMultiProcessorCount,
+// queried once per device and cached; 148 on a B200).  Grids of persistent and
+// grid-stride kernels are sized from it.
+int sm_count();
+
+// Upper bound on the resident warps of a grid of 256-thread CTAs on the
+// current device: 2048 threads per SM.
+inline int64_t max_resident_warps() { return (int64_t)sm_count() * 64; }
 
 inline unsigned blocks_for(int64_t n, int threads = kThreads) {
     return (unsigned)((n + threads - 1) / threads);

@@ -38,7 +38,7 @@ int ds_count_triangle_ids(int64_t num_pixels, const float* rast, int num_tris, i
     DS_CHECK_ARG(((uintptr_t)rast & 15) == 0, "count_triangle_ids: rast not 16-byte aligned");
     if (num_pixels == 0) return DS_OK;
     const int64_t blocks = (num_pixels + kThreads - 1) / kThreads;
-    const unsigned grid = (unsigned)(blocks < (int64_t)kSMs * 16 ? blocks : (int64_t)kSMs * 16);
+    const unsigned grid = (unsigned)(blocks < (int64_t)sm_count() * 16 ? blocks : (int64_t)sm_count() * 16);
     count_ids_kernel<<<grid, kThreads, 0, (cudaStream_t)stream>>>(
         num_pixels, reinterpret_cast<const float4*>(rast), num_tris, reinterpret_cast<unsigned long long*>(counts),
         status);

@@ -211,7 +211,7 @@ int ds_depth_test(int B, int H, int W, int num_frags, const int* frag_pix, const
         return set_error(DS_ERR_WORKSPACE, "depth_test: workspace too small");
     cudaStream_t st = (cudaStream_t)stream;
     unsigned long long* zbuf = reinterpret_cast<unsigned long long*>(workspace);
-    fill_u64_kernel<<<kSMs * 4, kThreads, 0, st>>>(zbuf, npix, ~0ull);
+    fill_u64_kernel<<<sm_count() * 4, kThreads, 0, st>>>(zbuf, npix, ~0ull);
     depth_test_kernel<<<blocks_for(num_frags), kThreads, 0, st>>>(H, W, num_frags, frag_pix, frag_attrs, frag_alpha,
                                                                   alpha_thresh, zbuf);
     depth_gather_kernel<<<blocks_for(npix), kThreads, 0, st>>>(npix, zbuf, frag_attrs, rast);

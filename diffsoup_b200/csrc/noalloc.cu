@@ -21,7 +21,13 @@
 //   * host code cannot use the array's name as a device address, so the
 //     first call on each device looks the address up with
 //     cudaGetSymbolAddress (with that device current) and caches it.  Make
-//     that first call before any stream capture.
+//     that first call before any stream capture.  The cached address belongs
+//     to the device's current (primary) context: do not call this entry point
+//     again after cudaDeviceReset or after that context was destroyed and
+//     re-created, where the library's module may be loaded at another address;
+//   * fragments whose (batch, row, column) lies outside [0,B) x [0,H) x [0,W)
+//     are skipped, so a bad fragment cannot write into the shared buffer
+//     beyond its own batch (the workspace version leaves that to the caller).
 #include <mutex>
 
 #include "geometry.cuh"
@@ -65,7 +71,7 @@ __global__ void noalloc_clear_kernel(unsigned long long* keys, int64_t n) {
 }
 
 // Same test as the workspace version (rasterize.cu:319-345).
-__global__ void __launch_bounds__(kThreads) noalloc_depth_kernel(int H, int W, int num_frags,
+__global__ void __launch_bounds__(kThreads) noalloc_depth_kernel(int B, int H, int W, int num_frags,
                                                                  const int* __restrict__ frag_pix,
                                                                  const float* __restrict__ frag_attrs,
                                                                  const float* __restrict__ frag_alpha,
@@ -74,8 +80,10 @@ __global__ void __launch_bounds__(kThreads) noalloc_depth_kernel(int H, int W, i
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= num_frags) return;
     const int b = frag_pix[(size_t)i * 3];
-    if (b < 0) return;
-    const int64_t p = (int64_t)b * H * W + (int64_t)frag_pix[(size_t)i * 3 + 1] * W + frag_pix[(size_t)i * 3 + 2];
+    const int y = frag_pix[(size_t)i * 3 + 1], x = frag_pix[(size_t)i * 3 + 2];
+    // b < 0 marks a rejected fragment; anything else outside the batch is skipped too
+    if (b < 0 || b >= B || y < 0 || y >= H || x < 0 || x >= W) return;
+    const int64_t p = ((int64_t)b * H + y) * W + x;
     if (frag_alpha[i] < thresh[i]) return;
     const float z = frag_attrs[(size_t)i * 4 + 2];
     if (z <= -1.f || !isfinite(z)) return;
@@ -115,8 +123,8 @@ extern "C" int ds_depth_test_noalloc(int B, int H, int W, int num_frags, const i
     const int rc = depth_keys_address(&keys);
     if (rc) return rc;
     cudaStream_t st = (cudaStream_t)stream;
-    noalloc_clear_kernel<<<kSMs * 4, kThreads, 0, st>>>(keys, npix);
-    noalloc_depth_kernel<<<blocks_for(num_frags), kThreads, 0, st>>>(H, W, num_frags, frag_pix, frag_attrs,
+    noalloc_clear_kernel<<<sm_count() * 4, kThreads, 0, st>>>(keys, npix);
+    noalloc_depth_kernel<<<blocks_for(num_frags), kThreads, 0, st>>>(B, H, W, num_frags, frag_pix, frag_attrs,
                                                                      frag_alpha, alpha_thresh, keys);
     noalloc_gather_kernel<<<blocks_for(npix), kThreads, 0, st>>>(npix, keys, frag_attrs, rast);
     return check_launch("depth_test_noalloc");

@@ -108,7 +108,7 @@ __global__ void advance_step_kernel(int* step) {
 
 static unsigned grid_for(int64_t n) {
     const int64_t b = (n + kThreads - 1) / kThreads;
-    const int64_t cap = (int64_t)kSMs * 8;
+    const int64_t cap = (int64_t)sm_count() * 8;
     return (unsigned)(b < 1 ? 1 : (b < cap ? b : cap));
 }
 

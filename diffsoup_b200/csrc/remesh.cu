@@ -525,8 +525,8 @@ int ds_split_soup_emit(int mode, const float* mvp_host, float aspect_wh, int N, 
     const SplitWs w = carve_split(const_cast<void*>(workspace), M, nullptr);
     cudaStream_t st = (cudaStream_t)stream;
     if (N > 0) {
-        const unsigned b = blocks_for((int64_t)N * 3);
-        copy_floats_kernel<<<b < (unsigned)kSMs * 8 ? b : (unsigned)kSMs * 8, kThreads, 0, st>>>((int64_t)N * 3,
+        const unsigned b = blocks_for((int64_t)N * 3), cap = (unsigned)sm_count() * 8;
+        copy_floats_kernel<<<b < cap ? b : cap, kThreads, 0, st>>>((int64_t)N * 3,
                                                                                                    verts, out_verts);
     }
     if (M > 0)

@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(kThreads) lut_opacity_kernel(int64_t n, const 
 
 static unsigned pixel_grid(int64_t n) {
     const int64_t b = (n + kThreads - 1) / kThreads;
-    const int64_t cap = (int64_t)kSMs * 8;
+    const int64_t cap = (int64_t)sm_count() * 8;
     return (unsigned)(b < 1 ? 1 : (b < cap ? b : cap));
 }
 

@@ -975,7 +975,7 @@ static unsigned block_grid(int num_tiles, const void* kernel, int& per_sm) {
     }
     const int64_t warps = (int64_t)num_tiles * kBlocksPerTile;
     const int64_t ctas = (warps + kWarpsPerCta - 1) / kWarpsPerCta;
-    const int64_t cap = (int64_t)kSMs * per_sm;
+    const int64_t cap = (int64_t)sm_count() * per_sm;
     return (unsigned)(ctas < 1 ? 1 : (ctas < cap ? ctas : cap));
 }
 
@@ -1027,7 +1027,7 @@ int tiles_aux_impl(int B, const ds_view_desc* views, int num_tiles, int T, int l
     if (rs == nullptr)
         return aux_launch(B, views, num_tiles, T, level, S, alpha_src, 1, l1, nullptr, rast, scale, grad_alpha_src,
                           workspace, list_capacity, nullptr, nullptr, st, bwl);
-    aux_records_kernel<<<kSMs * 8, kRecChunk, 0, st>>>(*rs, level, S, alpha_src, l1, scale, grad_alpha_src);
+    aux_records_kernel<<<sm_count() * 8, kRecChunk, 0, st>>>(*rs, level, S, alpha_src, l1, scale, grad_alpha_src);
     const int rc = check_launch("tiles_opacity_aux records");
     if (rc) return rc;
     return aux_launch(B, views, num_tiles, T, level, S, alpha_src, 1, l1, nullptr, rast, scale, grad_alpha_src,

@@ -76,8 +76,5 @@ int tiles_aux_impl(int B, const ds_view_desc* views, int num_tiles, int T, int l
                    const float* l1, const float* rast, float scale, float* grad_alpha_src, void* workspace,
                    int64_t list_capacity, const RecordStore* rs, cudaStream_t st, int bwl);
 
-// Upper bound on the warps of a tiled-kernel grid (148 SMs x 8 CTAs x 8
-// warps): the record counter ends at most one chunk per warp past capacity.
-constexpr int64_t kMaxTileWarps = 148 * 8 * 8;
 
 }  // namespace dsb

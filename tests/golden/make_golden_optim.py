@@ -19,6 +19,13 @@ import torch
 STEPS = 5
 
 
+def reference_dir() -> str:
+    """The reference checkout: $DIFFSOUP_REFERENCE, else a `reference`
+    directory beside this repository."""
+    root = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    return os.environ.get("DIFFSOUP_REFERENCE") or os.path.join(os.path.dirname(root), "reference")
+
+
 def main(ref_root: str) -> None:
     spec = importlib.util.spec_from_file_location("ref_optimize", os.path.join(ref_root, "python", "diffsoup",
                                                                                "optimize.py"))
@@ -54,4 +61,4 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else reference_dir())

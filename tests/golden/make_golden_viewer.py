@@ -34,6 +34,13 @@ def load_reference_functions(ref_root: str) -> dict:
     return ns
 
 
+def reference_dir() -> str:
+    """The reference checkout: $DIFFSOUP_REFERENCE, else a `reference`
+    directory beside this repository."""
+    root = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    return os.environ.get("DIFFSOUP_REFERENCE") or os.path.join(os.path.dirname(root), "reference")
+
+
 def main(ref_root: str) -> None:
     ns = load_reference_functions(ref_root)
     rng = np.random.default_rng(77)
@@ -63,4 +70,4 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else reference_dir())

@@ -65,6 +65,58 @@ def test_noalloc_depth_test_matches_workspace_version_twice():
         assert torch.equal(got.view(torch.int32), want.view(torch.int32))
 
 
+def test_noalloc_same_shape_again_and_untouched_pixels():
+    """Three calls in a row, the third with the first call's shape but other
+    fragments: each equals the workspace version, and pixels that no fragment
+    wins keep the value the caller put there."""
+    f = _entry()
+    p = _core.ptr
+    for config, seed, views, res in ((2, 3, 2, (512, 640)), (1, 8, 3, (300, 400)), (2, 11, 2, (512, 640))):
+        fp, fa, alpha, thresh, B, H, W = _fragments(config, seed, views, res)
+        want = torch.full((B, H, W, 4), 7.0, device=DEV)
+        _core.depth_test(fp, fa, alpha, thresh, want)
+        got = torch.full((B, H, W, 4), 7.0, device=DEV)
+        _core.check(f(B, H, W, fp.shape[0], p(fp), p(fa), p(alpha), p(thresh), p(got), _core.stream()))
+        torch.cuda.synchronize()
+        empty = want[..., 3] == 7.0
+        assert int(empty.sum()) > 1000
+        assert bool((got[empty] == 7.0).all())
+        assert torch.equal(got.view(torch.int32), want.view(torch.int32))
+
+
+def test_noalloc_skips_fragments_outside_the_batch():
+    """Fragments whose batch index or pixel lies outside the call's B x H x W
+    are skipped: the result equals the workspace version on the valid
+    fragments alone, and the next call is unaffected."""
+    f = _entry()
+    p = _core.ptr
+    fp, fa, alpha, thresh, B, H, W = _fragments(1, 5, 2, (200, 240))
+    n = fp.shape[0]
+    assert (B + 1) * H * W < (1 << 21)
+    # a winning fragment (in front of everything, opacity above its threshold) at
+    # batch B, and one at column W of row 0 (which would alias pixel (1, 0))
+    bad_pix = torch.tensor([[B, 3, 4], [0, 0, W]], dtype=torch.int32, device=DEV)
+    bad_attr = torch.tensor([[0.3, 0.3, -0.99, 1.0], [0.3, 0.3, -0.99, 1.0]], device=DEV)
+    fp2 = torch.cat([fp, bad_pix]).contiguous()
+    fa2 = torch.cat([fa, bad_attr]).contiguous()
+    al2 = torch.cat([alpha, torch.ones(2, device=DEV)]).contiguous()
+    th2 = torch.cat([thresh, torch.zeros(2, device=DEV)]).contiguous()
+    want = torch.zeros(B, H, W, 4, device=DEV)
+    _core.depth_test(fp, fa, alpha, thresh, want)  # the valid fragments only
+    got = torch.zeros(B, H, W, 4, device=DEV)
+    _core.check(f(B, H, W, n + 2, p(fp2), p(fa2), p(al2), p(th2), p(got), _core.stream()))
+    torch.cuda.synchronize()
+    assert torch.equal(got.view(torch.int32), want.view(torch.int32))
+    # the next call, one batch larger, sees nothing of the skipped fragments
+    fp3, fa3, alpha3, thresh3, B3, H3, W3 = _fragments(1, 6, 3, (200, 240))
+    want3 = torch.zeros(B3, H3, W3, 4, device=DEV)
+    _core.depth_test(fp3, fa3, alpha3, thresh3, want3)
+    got3 = torch.zeros(B3, H3, W3, 4, device=DEV)
+    _core.check(f(B3, H3, W3, fp3.shape[0], p(fp3), p(fa3), p(alpha3), p(thresh3), p(got3), _core.stream()))
+    torch.cuda.synchronize()
+    assert torch.equal(got3.view(torch.int32), want3.view(torch.int32))
+
+
 def test_noalloc_rejects_batches_beyond_its_buffer():
     f = _entry()
     null = C.c_void_p(0)
