@@ -10,11 +10,17 @@ gradients).  Synthetic, seeded inputs stand in for the reference's datasets.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Prints one JSON line (rank 0).  `value` is views/s of the batched BF16 step
-(diffsoup_b200.step.TrainStep, one CUDA graph per step) with inputs resident
-in HBM; `e2e` is the same step through the public API with each step's
-camera matrices and target images copied from pinned host memory and the loss
-read back.  N > 1 runs one independent replica per GPU (views are
+Prints one JSON line (rank 0).  `value` is views/s of the batched step
+(diffsoup_b200.step.TrainStep, one CUDA graph per step) in split-BF16
+precision (every shading-MLP operand as two BF16 planes on the tensor cores;
+image and gradients within 1e-3 of the FP64 oracle; --precision bf16 for
+plain BF16 operands) with inputs resident in HBM; `e2e` is the same step
+through the public API with each step's camera matrices and target images
+copied from pinned host memory and the loss read back.  `side` holds the same
+workload in the other precision, the reference's own shading model (7
+features + SH2 -> 16 -> 16 -> 3) on the same soup, and the other benchmark
+configurations (1, 3, 4, 5), each with its dominant kernel's roofline fraction
+and a CPU sample.  N > 1 runs one independent replica per GPU (views are
 independent; the reference has no multi-GPU exchange), timed as the max over
 ranks.  --impl reference times the CPU restatement of the reference's step
 (oracle/pipeline.py, FP32, all host threads) on a bounded sample.
@@ -48,6 +54,12 @@ KERNELS_PER_STEP = 16
 # raster | deferred shade
 RENDER_KERNELS_PER_FRAME = 9
 WORKLOAD = "config2: 15K-tri sphere-shell soup, 8 views 800x800, levels 0..2 x 8 ch, MLP 11-16-3, stochastic opacity"
+PRECISION_TEXT = {
+    "split": "split bf16: every MLP operand as bf16 hi + lo on the BF16 tensor cores (hi*hi + hi*lo + lo*hi, FP32 "
+             "accumulation), FP32 features; image and every gradient group within 1e-3 of the FP64 oracle",
+    "bf16": "bf16: BF16 features and MLP operands on the tensor cores, FP32 accumulation; feature and MLP gradients "
+            "up to ~1.6e-2 / ~5e-3 from the FP64 oracle (the rounding of the BF16 inputs)",
+}
 N_INPUT_SETS = 4  # rotating view batches: 4 x 61 MB of targets, larger than the 126 MB L2
 
 
@@ -59,8 +71,12 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
-    ap.add_argument("--no-split", dest="split", action="store_false",
-                    help="skip timing the split-BF16 precision mode beside the BF16 step")
+    ap.add_argument("--precision", choices=["split", "bf16"], default="split",
+                    help="shading precision of the headline step: split (every MLP operand as two BF16 planes on "
+                         "the tensor cores; image and gradients within 1e-3 of FP64) or bf16 (BF16 operands)")
+    ap.add_argument("--no-side", dest="side", action="store_false",
+                    help="skip the side entries (the other precision, the reference's own shading model and the "
+                         "other benchmark configurations)")
     ap.add_argument("--no-render", dest="render", action="store_false",
                     help="skip timing the inference render (the viewer's frame) beside the training step")
     ap.add_argument("--views", type=int, default=8, help="views per step (8 is the benchmark workload; "
@@ -126,8 +142,33 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # workload
 # ---------------------------------------------------------------------------
-def make_inputs(rank: int, nviews: int = 8):
-    from diffsoup_b200 import scenes
+def load_scenes():
+    """diffsoup_b200/scenes.py (numpy only: the seeded synthetic soups and
+    cameras) loaded from its file, so that a caller can build the workload
+    without importing the package, which loads libdiffsoup_b200.so."""
+    import importlib.util
+
+    name = "_bench_scenes"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, os.path.join(ROOT, "diffsoup_b200", "scenes.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def bench_config(world: int, nviews: int = 8) -> dict:
+    """The workload both arms report (`config`)."""
+    return {"workload": WORKLOAD if nviews == 8 else WORKLOAD.replace("8 views", f"{nviews} views"),
+            "views_per_step": nviews, "triangles": 15000, "resolution": "800x800",
+            "parallelism": f"replicas x{world}",
+            "l2": f"{N_INPUT_SETS} rotating input sets (4 x 61 MB targets) larger than L2"}
+
+
+def make_inputs(rank: int, nviews: int = 8, scenes=None):
+    if scenes is None:
+        from diffsoup_b200 import scenes
 
     sc = scenes.make_scene(2, seed=0, with_targets=False)
     mlp = scenes.mlp_weights(sc.mlp_input_dim, 3, sc.hidden_dim, sc.n_layers, seed=0)
@@ -153,13 +194,16 @@ def mlp_flat(mlp):
 
 # ---------------------------------------------------------------------------
 def run_reference(args):
-    """CPU restatement of the reference's step (the oracle port), rank 0 only."""
+    """The reference's step on the host cores, rank 0 only: the oracle port of
+    its kernels (oracle/, FP32, OpenMP over all host threads; the reference has
+    no CPU implementation of the path and its own CUDA build is the parity
+    checker, not a baseline), one 800x800 view of the workload per step.
+    Neither this arm nor its inputs load libdiffsoup_b200.so."""
     if int(os.environ.get("RANK", "0")) != 0:
         return
     from oracle import cpu, pipeline as P
-    from diffsoup_b200 import scenes
 
-    sc, mlp, sets = make_inputs(0)
+    sc, mlp, sets = make_inputs(0, scenes=load_scenes())
     cores = cpu.omp_threads()
     torch.set_num_threads(max(1, os.cpu_count() or 1))
 
@@ -172,36 +216,34 @@ def run_reference(args):
                            max_level=sc.max_level, stochastic=True, seed=7, iteration=i)
         P.train_step(inp, "f32")
 
-    for i in range(min(args.warmup, 2)):
+    for i in range(args.warmup):
         one_view(i)
-    budget = 120.0
     t0 = time.perf_counter()
-    n = 0
     for i in range(args.steps):
-        one_view(i)
-        n += 1
-        if time.perf_counter() - t0 > budget:
-            break
+        one_view(args.warmup + i)
     dt = time.perf_counter() - t0
+    n = args.steps
     v = n / dt
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "views/s", "n_gpus": args.gpus,
-        "steps": n, "warmup": min(args.warmup, 2), "ms_per_step": 1000 * dt / n, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD, "step_unit": "one 800x800 view per step (bounded sample)"},
+        "steps": n, "warmup": args.warmup, "ms_per_step": 1000 * dt / n, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; stands in for the reference datasets)",
+        "config": bench_config(args.gpus),
+        "step_unit": "one 800x800 view of the workload per step (a bounded sample of the 8-view step)",
         "cpu_baseline": {"value": v, "unit": "views/s", "cores": cores, "kind": "port",
-                         "sample": f"{n} views of config 2 (800x800, 15K tris), FP32 oracle port, {cores} threads"},
+                         "sample": f"{n} views of the workload (800x800, 15K tris), FP32 oracle port, {cores} threads"},
         "e2e": {"value": v, "unit": "views/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
 # ---------------------------------------------------------------------------
-def algorithmic_bytes(phase: str, P_: int, B: int, T: int, V: int, ST: int, C_: int) -> float:
+def algorithmic_bytes(phase: str, P_: int, B: int, T: int, V: int, ST: int, C_: int, feat_bytes: int = 2) -> float:
     """Minimal DRAM bytes of one launch of each step kernel: what the kernel must read and write
-    once (per-pixel buffers, per-(view, triangle) records, lattice samples), no re-reads."""
-    if phase == "shade":  # rast 16 R, target 12 R, colour 12 W, dL/dcolour 12 W, |c-t| 4 W; bf16 features + fp32 grads
-        return P_ * 56.0 + T * ST * C_ * (2 + 8)
+    once (per-pixel buffers, per-(view, triangle) records, lattice samples), no re-reads.  feat_bytes:
+    2 when the shading kernel gathers BF16 features, 4 for FP32 (split precision)."""
+    if phase == "shade":  # rast 16 R, target 12 R, colour 12 W, dL/dcolour 12 W, |c-t| 4 W; features + fp32 grads
+        return P_ * 56.0 + T * ST * C_ * (feat_bytes + 8)
     # fragment records: 16 B each, about one per pixel on this workload (fragments in front of the surface)
     if phase == "raster":  # rast 16 W + records 16 W per pixel; triangle records 64 B per (view, tri); opacities
         return P_ * 32.0 + B * T * 64.0 + T * ST * 4.0
@@ -241,7 +283,7 @@ def run_ours(args):
     params = t(mlp_flat(mlp))
     dsets = [(t(m), t(i), t(g)) for m, i, g in sets]
     step = TrainStep(T, V, hw, sc.feat_dim, sc.min_level, sc.max_level, sc.hidden_dim, sc.n_layers,
-                     stochastic=True, seed=1234 + rank, device=dev)
+                     stochastic=True, seed=1234 + rank, device=dev, precision=args.precision)
 
     def kw(s):
         return dict(verts=verts, tri=tri, mvp=s[0], inv_mvp=s[1], feat_src=feat_src, alpha_src=alpha_src,
@@ -287,6 +329,15 @@ def run_ours(args):
     ms = replicas.max_over_ranks(rep, e0.elapsed_time(e1))
     overflow = step.overflowed()
     value = replicas.job_throughput(rep, B * args.steps, ms)
+    # steadiness: four more back-to-back windows of the same K steps (not part of `value`)
+    windows = []
+    for _ in range(4):
+        e0.record()
+        for i in range(args.steps):
+            graphs[i % N_INPUT_SETS].replay()
+        e1.record()
+        torch.cuda.synchronize()
+        windows.append(replicas.max_over_ranks(rep, e0.elapsed_time(e1)) / args.steps)
 
     # ---------------- end to end through the public API -----------------------
     # pinned host inputs; each step copies its cameras and targets H2D on a copy
@@ -356,7 +407,7 @@ def run_ours(args):
     dom = max(["raster", "shade", "aux", "edge"], key=lambda n: phase_ms[n])
     ST = _core.feats_at_level(sc.max_level)
     P_ = step.num_pixels
-    alg = algorithmic_bytes(dom, P_, B, T, V, ST, sc.feat_dim)
+    alg = algorithmic_bytes(dom, P_, B, T, V, ST, sc.feat_dim, 4 if args.precision == "split" else 2)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -368,29 +419,32 @@ def run_ours(args):
     step_bytes = step_algorithmic_bytes(B, T, V, _core.total_feats(sc.min_level, sc.max_level), sc.feat_dim, P_)
     traffic = read_traffic(dom)
 
-    # ---------------- split-BF16 precision mode (same workload) ---------------
-    split = None
-    if rank == 0 and args.split:
-        sstep = TrainStep(T, V, hw, sc.feat_dim, sc.min_level, sc.max_level, sc.hidden_dim, sc.n_layers,
-                          stochastic=True, seed=1234 + rank, device=dev, precision="split")
-        sstep.capacity = step.capacity
-        sstep.cfg.frag_records = step.cfg.frag_records
-        sstep.cfg.block_shape = step.cfg.block_shape
-        sstep._alloc()
-        sg = [sstep.capture(**kw(s)) for s in dsets]
-        for i in range(3):
-            sg[i % N_INPUT_SETS].replay()
+    # ---------------- the headline workload in the other precision -------------
+    side = None
+    if rank == 0 and args.side:
+        other = "bf16" if args.precision == "split" else "split"
+        ostep = TrainStep(T, V, hw, sc.feat_dim, sc.min_level, sc.max_level, sc.hidden_dim, sc.n_layers,
+                          stochastic=True, seed=1234 + rank, device=dev, precision=other)
+        ostep.capacity = step.capacity
+        ostep.cfg.frag_records = step.cfg.frag_records
+        ostep.cfg.block_shape = step.cfg.block_shape
+        ostep._alloc()
+        og = [ostep.capture(**kw(s)) for s in dsets]
+        for i in range(args.warmup):
+            og[i % N_INPUT_SETS].replay()
         torch.cuda.synchronize()
-        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        nsplit = max(10, args.steps // 4)
-        s0.record()
-        for i in range(nsplit):
-            sg[i % N_INPUT_SETS].replay()
-        s1.record()
+        e0.record()
+        for i in range(args.steps):
+            og[i % N_INPUT_SETS].replay()
+        e1.record()
         torch.cuda.synchronize()
-        split = {"value": B * nsplit / (s0.elapsed_time(s1) / 1000.0), "unit": "views/s", "steps": nsplit,
-                 "precision": "split bf16 (every MLP operand as bf16 hi + lo; gradients within 3e-5 of FP64)"}
-        del sg, sstep
+        oms = e0.elapsed_time(e1)
+        side = {f"config2_{other}": {"workload": WORKLOAD, "precision": PRECISION_TEXT[other],
+                                      "value": B * args.steps / (oms / 1000.0), "unit": "views/s",
+                                      "ms_per_step": oms / args.steps, "steps": args.steps, "warmup": args.warmup}}
+        del og, ostep
+        # the reference's own shading model and the other benchmark configurations
+        side.update(run_side_entries(args, dev, peak))
 
     # ---------------- plain FP32 single-view path (denominator) ---------------
     plain = None
@@ -414,15 +468,18 @@ def run_ours(args):
 
     line = {
         "metric": METRIC, "value": value, "unit": "views/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "repeat_windows": {"ms_per_step": [round(w, 5) for w in windows],
+                           "median_ms_per_step": round(statistics.median(windows), 5),
+                           "steps_each": args.steps},
+        "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "bf16", "data": "synthetic (seeded; stands in for the reference datasets)",
-        "config": {"workload": WORKLOAD if B == 8 else WORKLOAD.replace("8 views", f"{B} views"), "views_per_step": B, "triangles": T, "resolution": "800x800",
-                   "parallelism": f"replicas x{world}", "graph": "one CUDA graph per step",
-                   "l2": f"{N_INPUT_SETS} rotating input sets (4 x 61 MB targets) larger than L2",
-                   "list_overflow": overflow,
-                   "autotuned": {"block": tuned["block"], "frag_records_per_px": round(tuned["frag_records"], 3),
-                                 "list_capacity": tuned["list_capacity"],
-                                 "ms_per_step_by_block": {k: round(v, 4) for k, v in tuned["ms_per_step"].items()}}},
+        "precision": PRECISION_TEXT[args.precision],
+        "config": bench_config(world, B),
+        "graph": "one CUDA graph per step", "list_overflow": overflow,
+        "autotuned": {"block": tuned["block"], "frag_records_per_px": round(tuned["frag_records"], 3),
+                      "list_capacity": tuned["list_capacity"],
+                      "ms_per_step_by_block": {k: round(v, 4) for k, v in tuned["ms_per_step"].items()}},
         "e2e": {"value": e2e, "unit": "views/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 4},
         "mfragments_per_s": nfrag * args.steps * world / (ms / 1000.0) / 1e6,
         "fragments_per_step": int(nfrag),
@@ -435,8 +492,8 @@ def run_ours(args):
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                      "algorithmic_bytes": alg},
     }
-    if split is not None:
-        line["split_precision"] = split
+    if side is not None:
+        line["side"] = side
     if plain is not None:
         line["plain_fp32"] = plain
         line["speedup_vs_plain_fp32"] = value / plain["value"]
@@ -450,6 +507,153 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
     del graphs, egraphs
     replicas.shutdown(rep)
+
+
+def count_fragments(hw, pos, tri) -> int:
+    """Covered fragments (every (pixel, triangle) pair passing the coverage test, before the depth test)
+    of every view, counted by the library's fragment operators one view at a time."""
+    import diffsoup_b200 as ds
+
+    n = 0
+    for b, (H, W) in enumerate(hw):
+        fp, _ = ds.rasterize._compute_fragments((H, W), pos[b:b + 1].contiguous(), tri)
+        n += int(fp.shape[0])
+        del fp
+    return n
+
+
+# Side workloads: (entry, benchmark configuration, shading model, precision, fragment records per pixel;
+# None = the autotuner sizes the record store, 0 = tile-wise recomputation of the fragments)
+SIDE_WORKLOADS = [
+    ("config2_reference_model_split", 2, "reference", "split", None),
+    ("config2_reference_model_bf16", 2, "reference", "bf16", None),
+    ("config1", 1, "config", "split", None),
+    ("config3", 3, "config", "split", None),
+    ("config4_bf16", 4, "config", "bf16", None),
+    ("config4_split", 4, "config", "split", None),
+    ("config5_records", 5, "config", "bf16", None),
+    ("config5_recompute", 5, "config", "bf16", 0.0),
+]
+SIDE_TEXT = {
+    1: "config1: 5K-tri soup in U[-1,1]^3, 1 view 256x256, levels 0..2 x 8 ch, MLP 11-16-3",
+    2: "config2: 15K-tri sphere-shell soup, 8 views 800x800, levels 0..2",
+    3: "config3: 50K tris in 20 clusters + 10K on a shell of radius 10, 64 views of uneven size (widths 400..1200, "
+       "aspects 4:3/16:9/1:1), levels 0..2 x 8 ch, MLP 11-16-3, one CUDA graph",
+    4: "config4: 5K-tri soup, 1 view 256x256, levels 0..3 x 16 ch, MLP 19-64-64-3",
+    5: "config5: 200K tris (shell + clusters), 16 views 1920x1080, levels 0..3 x 16 ch, MLP 19-64-64-3",
+}
+
+
+def measure_workload(dev, sc, mlp, precision: str, steps: int, warmup: int, peak: float,
+                     frag_records=None, cpu_sample: bool = True) -> dict:
+    """One side workload: autotuned, captured in one CUDA graph, `warmup` untimed replays, then `steps`
+    replays each timed with CUDA events and each preceded by an L2 flush (a 256 MB write, outside the
+    timed pair).  Also the per-phase kernel times (the step's profiling events over eager steps), the
+    dominant kernel's roofline fraction, covered fragments per second, the device memory the step holds
+    and a CPU sample (view 0 through the FP32 oracle port)."""
+    from diffsoup_b200 import _core
+    from diffsoup_b200.step import TrainStep
+
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    hw = [(v.height, v.width) for v in sc.views]
+    B, T, V = len(hw), sc.T, sc.verts.shape[0]
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    torch.cuda.reset_peak_memory_stats(dev)
+    base_mem = torch.cuda.memory_allocated(dev)
+    kw = dict(verts=t(sc.verts), tri=t(sc.tri), mvp=t(sc.mvps()), inv_mvp=t(sc.inv_mvps()), feat_src=t(sc.feat_src),
+              alpha_src=t(sc.alpha_src[..., 0]), mlp_params=t(mlp_flat(mlp)),
+              target=t(np.concatenate([x.reshape(-1, 3) for x in sc.targets])))
+    step = TrainStep(T, V, hw, sc.feat_dim, sc.min_level, sc.max_level, sc.hidden_dim, sc.n_layers, stochastic=True,
+                     seed=99, device=dev, precision=precision, view_enc=sc.view_enc,
+                     frag_records=2.0 if frag_records is None else frag_records)
+    tuned = step.autotune(**kw, steps=3)
+    g = step.capture(**kw)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for _ in range(warmup):
+        g.replay()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for a, b in ev:
+        flush.zero_()
+        a.record()
+        g.replay()
+        b.record()
+    torch.cuda.synchronize()
+    ms = statistics.mean(a.elapsed_time(b) for a, b in ev)
+    mem = torch.cuda.max_memory_allocated(dev) - base_mem - flush.numel()
+    overflow = step.overflowed()
+    del g, flush
+    # per-phase kernel time
+    names = ["prep", "bin", "raster", "shade", "aux", "edge", "finish"]
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(8)]
+    for e in evs:
+        e.record()
+    torch.cuda.synchronize()
+    _core.check(_core.lib.ds_train_step_set_events(ctypes_void_p_array(evs), 8))
+    acc = {n: 0.0 for n in names}
+    M = 5
+    for _ in range(M):
+        step.run(**kw)
+        torch.cuda.synchronize()
+        for k, n in enumerate(names):
+            acc[n] += evs[k].elapsed_time(evs[k + 1])
+    _core.check(_core.lib.ds_train_step_set_events(None, 0))
+    phase_ms = {n: acc[n] / M for n in names}
+    dom = max(["raster", "shade", "aux", "edge"], key=lambda n: phase_ms[n])
+    ST = _core.feats_at_level(sc.max_level)
+    alg = algorithmic_bytes(dom, step.num_pixels, B, T, V, ST, sc.feat_dim, 4 if precision == "split" else 2)
+    achieved = alg / (phase_ms[dom] / 1000.0) / 1e9
+    try:
+        nfrag = count_fragments(hw, step.intermediate("pos").clone(), kw["tri"])
+    except RuntimeError:
+        nfrag = None
+    out = {"precision": PRECISION_TEXT[precision], "views_per_step": B, "triangles": T, "pixels_per_step": step.num_pixels,
+           "value": B / (ms / 1000.0), "unit": "views/s", "ms_per_step": ms, "steps": steps, "warmup": warmup,
+           "l2": "flushed (256 MB write) before every timed step",
+           "mfragments_per_s": None if nfrag is None else nfrag / (ms / 1000.0) / 1e6, "fragments_per_step": nfrag,
+           "phase_ms": {k: round(v, 4) for k, v in phase_ms.items()},
+           "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "algorithmic_bytes": alg},
+           "device_memory_bytes": int(mem), "workspace_bytes": int(step.workspace.numel()),
+           "fragment_records": "tile-wise recomputation" if step.record_capacity == 0 else
+                               f"stored ({step.cfg.frag_records:.3f} per pixel)",
+           "autotuned": {"block": tuned["block"], "list_capacity": tuned["list_capacity"]},
+           "list_overflow": overflow}
+    del step, kw
+    if cpu_sample:
+        from oracle import cpu, pipeline as P
+
+        v0 = sc.views[0]
+        inp = P.StepInputs(verts=sc.verts, tri=sc.tri, mvps=sc.mvps()[:1], inv_mvps=sc.inv_mvps()[:1],
+                           hw=[(v0.height, v0.width)], feat_src=sc.feat_src, alpha_src=sc.alpha_src[..., 0], mlp=mlp,
+                           targets=sc.targets[:1], min_level=sc.min_level, max_level=sc.max_level, stochastic=True,
+                           seed=99, iteration=0, view_enc=sc.view_enc)
+        t0 = time.perf_counter()
+        P.train_step(inp, "f32")
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": 1.0 / dt, "unit": "views/s", "cores": cpu.omp_threads(), "kind": "port",
+                               "sample": f"view 0 ({v0.width}x{v0.height}) through the FP32 oracle port"}
+    return out
+
+
+def run_side_entries(args, dev, peak: float) -> dict:
+    """The reference's own shading model on the benchmark soup and the other benchmark configurations
+    (seeded synthetic scenes of their shapes), with the same --steps / --warmup."""
+    from diffsoup_b200 import scenes
+
+    out = {}
+    for name, config, shading, precision, records in SIDE_WORKLOADS:
+        sc = scenes.make_scene(config, seed=0, shading=shading)
+        mlp = scenes.mlp_weights(sc.mlp_input_dim, 3, sc.hidden_dim, sc.n_layers, seed=0)
+        r = measure_workload(dev, sc, mlp, precision, args.steps, args.warmup, peak, records,
+                             cpu_sample=not args.no_cpu_baseline and not name.endswith(("_bf16", "_recompute")))
+        text = SIDE_TEXT[config]
+        if shading == "reference":
+            text += ", the reference's own shading model: 7 features + SH2 -> 16 -> 16 -> 3"
+        r["workload"] = text
+        out[name] = r
+        del sc
+    return out
 
 
 def ctypes_void_p_array(events):

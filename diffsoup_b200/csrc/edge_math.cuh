@@ -395,12 +395,14 @@ __device__ __forceinline__ EdgePair edge_pair(const EdgeHalo& h, const EdgeFrame
 // geometric-edge pairs and pairs that may be triangle intersections are
 // only marked there and evaluated in two further passes, where pass k takes
 // each lane's k-th marked pair, so that lanes run the rarer cases together.
+// `active` false: the lane has no pixel (it takes part in the warp-wide steps only).
 __device__ __forceinline__ int edge_grad_pixel_staged(const EdgeHalo& h, int hidx, int y0, int x0, int H, int W,
-                                                      const TriVerts* __restrict__ tverts, EdgeAccum& acc) {
+                                                      const TriVerts* __restrict__ tverts, EdgeAccum& acc,
+                                                      bool active = true) {
 #pragma unroll
     for (int k = 0; k < 12; ++k) acc.g[k] = 0.f;
     acc.any = false;
-    const int it0 = h.it[hidx];
+    const int it0 = active ? h.it[hidx] : -1;
     unsigned geo = 0u, isect = 0u;  // pairs (bit e) of the second and third passes
     EdgeFrame f;
     // pixel-centre NDC with one reciprocal per axis (this path is compared to

@@ -16,7 +16,7 @@
 
 #include "edge_math.cuh"
 #include "shade.cuh"
-#include "shade_small.cuh"
+#include "shade_reg.cuh"
 #include "tiled.cuh"
 
 namespace dsb {
@@ -29,9 +29,11 @@ namespace dsb {
 constexpr int kPrepWarps = 4;
 constexpr int kMaxSrc = 2048;  // floats of one triangle's samples per warp (S*C)
 
+// Outputs have a channel stride of CP >= C (padding channels written as zero).
 template <bool BF16OUT>
 __global__ void __launch_bounds__(kPrepWarps * 32) accum_sigmoid_kernel(int T, int lo, int hi, int target, int S,
-                                                                       int ST, int C, const float* __restrict__ src,
+                                                                       int ST, int C, int CP,
+                                                                       const float* __restrict__ src,
                                                                        float* __restrict__ out_f32,
                                                                        __nv_bfloat16* __restrict__ out_bf16) {
     __shared__ float s_src[kPrepWarps][kMaxSrc];
@@ -43,8 +45,13 @@ __global__ void __launch_bounds__(kPrepWarps * 32) accum_sigmoid_kernel(int T, i
     for (int i = lane; i < n; i += 32) s_src[warp][i] = ts[i];
     __syncwarp();
     const float R = (float)(1u << target);
-    for (int e = lane; e < ST * C; e += 32) {
-        const int k = e / C, c = e % C;
+    for (int e = lane; e < ST * CP; e += 32) {
+        const int k = e / CP, c = e % CP;
+        if (c >= C) {
+            out_f32[(size_t)t * ST * CP + e] = 0.f;
+            if (BF16OUT) out_bf16[(size_t)t * ST * CP + e] = __float2bfloat16_rn(0.f);
+            continue;
+        }
         uint32_t x, y;
         index_to_xy((uint32_t)k, x, y);
         const float b0 = __fdiv_rn((float)x, R), b1 = __fdiv_rn((float)y, R);
@@ -58,15 +65,16 @@ __global__ void __launch_bounds__(kPrepWarps * 32) accum_sigmoid_kernel(int T, i
             off += feats_at_level((uint32_t)l);
         }
         const float s = 1.f / (1.f + expf(-acc));
-        out_f32[(size_t)t * ST * C + e] = s;
-        if (BF16OUT) out_bf16[(size_t)t * ST * C + e] = __float2bfloat16_rn(s);
+        out_f32[(size_t)t * ST * CP + e] = s;
+        if (BF16OUT) out_bf16[(size_t)t * ST * CP + e] = __float2bfloat16_rn(s);
     }
 }
 
 // Adjoint of accum_sigmoid: grad_src[t] = sum_k lattice^T (grad_out * s (1-s)).
 // Accumulated per warp in shared memory, written once (no global atomics).
+// sig and grad_out have the channel stride CP, grad_src the stride C.
 __global__ void __launch_bounds__(kPrepWarps * 32) accum_sigmoid_backward_kernel(
-    int T, int lo, int hi, int target, int S, int ST, int C, const float* __restrict__ sig,
+    int T, int lo, int hi, int target, int S, int ST, int C, int CP, const float* __restrict__ sig,
     const float* __restrict__ grad_out, float* __restrict__ grad_src) {
     __shared__ float s_acc[kPrepWarps][kMaxSrc];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -78,8 +86,9 @@ __global__ void __launch_bounds__(kPrepWarps * 32) accum_sigmoid_backward_kernel
     const float R = (float)(1u << target);
     for (int e = lane; e < ST * C; e += 32) {
         const int k = e / C, c = e % C;
-        const float s = sig[(size_t)t * ST * C + e];
-        const float gz = grad_out[(size_t)t * ST * C + e] * s * (1.f - s);
+        const size_t o = ((size_t)t * ST + k) * CP + c;
+        const float s = sig[o];
+        const float gz = grad_out[o] * s * (1.f - s);
         if (gz == 0.f) continue;
         uint32_t x, y;
         index_to_xy((uint32_t)k, x, y);
@@ -195,8 +204,9 @@ __device__ void build_lattice_tab(const LatticeTab& L, int lo, int hi, int ST, i
 }
 
 // alpha_out[t] = sigmoid(accumulate(alpha_src[t])), feat_out[t] likewise
-// per channel (+ a bf16 copy); warp per triangle.
-template <int C>
+// per channel (+ a bf16 copy; both with the channel stride CP >= C, padding
+// channels zero); warp per triangle.
+template <int C, int CP>
 __global__ void __launch_bounds__(kTabWarps * 32) accum_tab_kernel(int T, int lo, int hi, int S, int ST,
                                                                    const float* __restrict__ alpha_src,
                                                                    const float* __restrict__ feat_src,
@@ -224,13 +234,16 @@ __global__ void __launch_bounds__(kTabWarps * 32) accum_tab_kernel(int T, int lo
             for (int n = 0; n < NE; ++n) acc = madd(acc, L.fw[k * NE + n], sa[L.fidx[k * NE + n]]);
             alpha_out[(size_t)t * ST + k] = 1.f / (1.f + expf(-acc));
         }
-        for (int e = lane; e < ST * C; e += 32) {
-            const int k = e / C, c = e % C;
-            float acc = 0.f;
-            for (int n = 0; n < NE; ++n) acc = madd(acc, L.fw[k * NE + n], sf[L.fidx[k * NE + n] * C + c]);
-            const float v = 1.f / (1.f + expf(-acc));
-            feat_out[(size_t)t * ST * C + e] = v;
-            feat_bf16[(size_t)t * ST * C + e] = __float2bfloat16_rn(v);
+        for (int e = lane; e < ST * CP; e += 32) {
+            const int k = e / CP, c = e % CP;
+            float v = 0.f;
+            if (c < C) {
+                float acc = 0.f;
+                for (int n = 0; n < NE; ++n) acc = madd(acc, L.fw[k * NE + n], sf[L.fidx[k * NE + n] * C + c]);
+                v = 1.f / (1.f + expf(-acc));
+            }
+            feat_out[(size_t)t * ST * CP + e] = v;
+            feat_bf16[(size_t)t * ST * CP + e] = __float2bfloat16_rn(v);
         }
         __syncwarp();
     }
@@ -239,8 +252,9 @@ __global__ void __launch_bounds__(kTabWarps * 32) accum_tab_kernel(int T, int lo
 // Adjoint of accum_tab_kernel: grad_src[t][d] = sum over the targets k that
 // read d of w * grad_out[t][k] * s (1 - s); a gather, written once.  The
 // tables are the ones the forward kernel of the step built (copied, not
-// rebuilt: this kernel sits on the step's critical path).
-template <int C>
+// rebuilt: this kernel sits on the step's critical path).  feat_sig and
+// feat_grad have the channel stride CP, feat_src_grad the stride C.
+template <int C, int CP>
 __global__ void __launch_bounds__(kTabWarps * 32) accum_tab_backward_kernel(
     int T, int lo, int hi, int S, int ST, const float* __restrict__ alpha_sig, const float* __restrict__ alpha_grad,
     const float* __restrict__ feat_sig, const float* __restrict__ feat_grad, float* __restrict__ alpha_src_grad,
@@ -262,8 +276,9 @@ __global__ void __launch_bounds__(kTabWarps * 32) accum_tab_backward_kernel(
             ga[i] = alpha_grad[(size_t)t * ST + i] * s * (1.f - s);
         }
         for (int i = lane; i < ST * C; i += 32) {
-            const float s = feat_sig[(size_t)t * ST * C + i];
-            gf[i] = feat_grad[(size_t)t * ST * C + i] * s * (1.f - s);
+            const size_t o = ((size_t)t * ST + i / C) * CP + i % C;
+            const float s = feat_sig[o];
+            gf[i] = feat_grad[o] * s * (1.f - s);
         }
         __syncwarp();
         for (int d = lane; d < S; d += 32) {
@@ -337,7 +352,10 @@ __global__ void __launch_bounds__(kThreads) project_backward_kernel(int B, int V
 // dL/dcolour and the triangle's far depth bound), so the four neighbours of
 // every pixel are shared-memory reads.  Pixels of a warp (two rows of 16)
 // mostly share a triangle along a row: a segmented warp reduction sums runs
-// of equal triangles before one FP64 atomic per vertex component.
+// of equal triangles before one FP64 atomic per vertex component.  Only
+// covered pixels have a contribution, so after staging the tile's covered
+// pixels are compacted (row-major order kept) onto the CTA's first threads:
+// warps run full of covered pixels and the warps left without one exit.
 constexpr int kEdgeThreads = DS_TILE * DS_TILE;
 #ifndef DSB_EDGE_MIN_CTAS
 #define DSB_EDGE_MIN_CTAS 4  // resident 8-warp CTAs per SM the register budget is sized for (64 registers)
@@ -384,14 +402,35 @@ __global__ void __launch_bounds__(kEdgeThreads, DSB_EDGE_MIN_CTAS) edge_step_ker
         for (int k = 0; k < 3; ++k) { h.c[k][i] = cc[k]; h.g[k][i] = gg[k]; }
     }
     __syncthreads();
-    const int lane = threadIdx.x & 31;
-    const int ly = threadIdx.x / DS_TILE, lx = threadIdx.x % DS_TILE;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __shared__ short s_pix[kEdgeThreads];
+    __shared__ int s_warp_n[kEdgeThreads / 32];
+    int n = 0;
+    {
+        const int cy = threadIdx.x / DS_TILE, cx = threadIdx.x % DS_TILE;
+        const bool cov = h.it[(cy + 1) * kHaloW + cx + 1] >= 0;  // a triangle (not background, not outside)
+        const unsigned m = __ballot_sync(0xffffffffu, cov);
+        if (lane == 0) s_warp_n[warp] = __popc(m);
+        __syncthreads();
+        int off = 0;
+#pragma unroll
+        for (int w = 0; w < kEdgeThreads / 32; ++w) {
+            off += w < warp ? s_warp_n[w] : 0;
+            n += s_warp_n[w];
+        }
+        if (cov) s_pix[off + __popc(m & ((1u << lane) - 1u))] = (short)threadIdx.x;
+        __syncthreads();
+    }
+    if (warp * 32 >= n) return;  // warp-uniform: no covered pixel left for this warp
+    const bool active = (int)threadIdx.x < n;
+    const int src = active ? s_pix[threadIdx.x] : 0;
+    const int ly = src / DS_TILE, lx = src % DS_TILE;
     const int y = ty0 + ly, x = tx0 + lx;
     EdgeAccum acc;
-    // every lane takes part (warp-wide reductions inside); pixels beyond the view are staged as
-    // kOutside and contribute nothing
+    // every lane of the warp takes part (warp-wide reductions inside); lanes past the covered
+    // pixels contribute nothing
     const int it0 = edge_grad_pixel_staged(h, (ly + 1) * kHaloW + lx + 1, y, x, vd.H, vd.W,
-                                           tab.verts + (size_t)b * T, acc);
+                                           tab.verts + (size_t)b * T, acc, active);
     const int key = (it0 >= 0 && acc.any) ? it0 : -1 - lane;
     if (__ballot_sync(0xffffffffu, key >= 0) == 0) return;  // no lane of the warp has a contribution
     const int prev = __shfl_up_sync(0xffffffffu, key, 1);
@@ -444,25 +483,28 @@ static int launch_shade(const ShadeArgs& a, cudaStream_t st) {
     }
     const int64_t chunks = (a.num_pixels + 31) / 32;
     const int64_t want = (chunks + K::WARPS - 1) / K::WARPS;
-    const int64_t cap = (int64_t)kSMs * (per_sm > 0 ? per_sm : 1);
+    const int64_t cap = (int64_t)sm_count() * (per_sm > 0 ? per_sm : 1);
     const unsigned grid = (unsigned)(want < 1 ? 1 : (want < cap ? want : cap));
     shade_step_kernel<K><<<grid, K::WARPS * 32, smem, st>>>(a);
     return check_launch("shade_step");
 }
 
-// The register-resident kernel of the 8-16-3 MLP.
-static int launch_shade_small(const ShadeArgs& a, cudaStream_t st) {
+// The register-resident kernels of the width-16 MLPs.
+template <class K>
+static int launch_shade_reg(const ShadeArgs& a, cudaStream_t st) {
+    const size_t smem = sizeof(RegSmem<K>);
     static int per_sm = 0;  // set on the first (eager) call, before any graph capture
     if (per_sm == 0) {
-        DS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, shade_small_kernel, kShadeSmallWarps * 32, 0));
-        if (per_sm <= 0) return set_error(DS_ERR_CUDA, "shade_small: kernel does not fit on an SM");
+        DS_CUDA(cudaFuncSetAttribute(shade_reg_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        DS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, shade_reg_kernel<K>, kShadeRegWarps * 32, smem));
+        if (per_sm <= 0) return set_error(DS_ERR_CUDA, "shade_reg: kernel does not fit on an SM");
     }
     const int64_t chunks = (a.num_pixels + 31) / 32;
-    const int64_t want = (chunks + kShadeSmallWarps - 1) / kShadeSmallWarps;
-    const int64_t cap = (int64_t)kSMs * per_sm;
+    const int64_t want = (chunks + kShadeRegWarps - 1) / kShadeRegWarps;
+    const int64_t cap = (int64_t)sm_count() * per_sm;
     const unsigned grid = (unsigned)(want < 1 ? 1 : (want < cap ? want : cap));
-    shade_small_kernel<<<grid, kShadeSmallWarps * 32, 0, st>>>(a);
-    return check_launch("shade_small");
+    shade_reg_kernel<K><<<grid, kShadeRegWarps * 32, smem, st>>>(a);
+    return check_launch("shade_reg");
 }
 
 static inline size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -548,8 +590,14 @@ static int64_t record_capacity(const ds_step_config& c, int num_tiles, int64_t P
     if (!(c.frag_records > 0.f)) return 0;
     const double n = std::ceil((double)P * (double)c.frag_records / kRecChunk);
     const int64_t items = (int64_t)num_tiles * 8;
-    return ((int64_t)n + (items < kMaxTileWarps ? items : kMaxTileWarps)) * kRecChunk;
+    const int64_t warps = max_resident_warps();
+    return ((int64_t)n + (items < warps ? items : warps)) * kRecChunk;
 }
+
+// Channel stride of the step's accumulated feature tables (and their
+// gradients): C rounded up to a multiple of 8, so that a lattice sample is
+// one or more 16-byte (bf16) / 32-byte (fp32) vectors.
+static int feat_stride(const ds_step_config& c) { return (c.C + 7) & ~7; }
 
 static StepWs carve_step(void* ws, const ds_step_config& c, int num_tiles, int64_t P, int64_t cap, size_t* total) {
     char* base = reinterpret_cast<char*>(ws);
@@ -558,8 +606,9 @@ static StepWs carve_step(void* ws, const ds_step_config& c, int num_tiles, int64
     StepWs w;
     w.pos = reinterpret_cast<float*>(base + o); o += al((size_t)c.B * c.V * 16);
     w.alpha_acc = reinterpret_cast<float*>(base + o); o += al((size_t)c.T * ST * 4);
-    w.feat_acc = reinterpret_cast<float*>(base + o); o += al((size_t)c.T * ST * c.C * 4);
-    w.feat_bf16 = reinterpret_cast<__nv_bfloat16*>(base + o); o += al((size_t)c.T * ST * c.C * 2);
+    const int CP = feat_stride(c);
+    w.feat_acc = reinterpret_cast<float*>(base + o); o += al((size_t)c.T * ST * CP * 4);
+    w.feat_bf16 = reinterpret_cast<__nv_bfloat16*>(base + o); o += al((size_t)c.T * ST * CP * 2);
     w.rast = reinterpret_cast<float*>(base + o); o += al((size_t)P * 16);
     w.color = reinterpret_cast<float*>(base + o); o += al((size_t)P * 12);
     w.grad_color = reinterpret_cast<float*>(base + o); o += al((size_t)P * 12);
@@ -570,7 +619,7 @@ static StepWs carve_step(void* ws, const ds_step_config& c, int num_tiles, int64
     // zeroed together each step: grad_pos .. loss_sum
     w.grad_pos = reinterpret_cast<double*>(base + o); o += al((size_t)c.B * c.V * 32);
     w.grad_alpha_acc = reinterpret_cast<float*>(base + o); o += al((size_t)c.T * ST * 4);
-    w.grad_feat_acc = reinterpret_cast<float*>(base + o); o += al((size_t)c.T * ST * c.C * 4);
+    w.grad_feat_acc = reinterpret_cast<float*>(base + o); o += al((size_t)c.T * ST * CP * 4);
     w.loss_sum = reinterpret_cast<double*>(base + o);
     w.rec_counters = reinterpret_cast<int*>(base + o + 64);
     o += 256;
@@ -592,18 +641,30 @@ static int block_shape_log2(const ds_step_config& c) {
     return c.block_shape == 1 ? 4 : (c.block_shape == 2 ? 2 : kDefaultBlockShape);
 }
 
-template <class K>
-static int shade_dispatch_check(const ds_step_config& c) {
-    return (c.C == K::C && c.hidden == K::HID && c.n_layers == K::NL) ? 1 : 0;
+// The fused shading kernels a step can run, by MLP shape.
+enum ShadeShape {
+    kShadeUnsupported = 0,
+    kShadeC8Dir16 = 1,     // 8 features + view direction -> 16 -> 3 (the benchmark configurations 1-3)
+    kShadeC7Sh2_16x2 = 2,  // 7 features + SH2 -> 16 -> 16 -> 3 (the reference's own model)
+    kShadeC16Dir64x2 = 3,  // 16 features + view direction -> 64 -> 64 -> 3 (configurations 4-5)
+};
+
+static int shade_shape(const ds_step_config& c) {
+    if (c.hidden == 16 && c.n_layers == 1 && c.C == 8 && c.view_enc == 0) return kShadeC8Dir16;
+    if (c.hidden == 16 && c.n_layers == 2 && c.C == 7 && c.view_enc == 1) return kShadeC7Sh2_16x2;
+    if (c.hidden == 64 && c.n_layers == 2 && c.C == 16 && c.view_enc == 0) return kShadeC16Dir64x2;
+    return kShadeUnsupported;
 }
 
 }  // namespace dsb
 
 using namespace dsb;
 
-using ShadeC8H16 = ShadeCfg<8, 16, 16, 1>;    // configs 1-3: 8 features + 3 view dir -> 16 -> 3
-using ShadeC16H64 = ShadeCfg<16, 32, 64, 2>;  // configs 4-5: 16 + 3 -> 64 -> 64 -> 3
-using ShadeC8H16Split = ShadeCfg<8, 16, 16, 1, true>;    // the same MLPs in split BF16
+using ShadeC8Dir16 = RegCfg<8, 3, 1, false>;        // 8 features + 3 view dir -> 16 -> 3
+using ShadeC8Dir16Split = RegCfg<8, 3, 1, true>;
+using ShadeC7Sh2_16x2 = RegCfg<7, 9, 2, false>;     // 7 features + 9 SH2 -> 16 -> 16 -> 3
+using ShadeC7Sh2_16x2Split = RegCfg<7, 9, 2, true>;
+using ShadeC16H64 = ShadeCfg<16, 32, 64, 2>;        // 16 + 3 -> 64 -> 64 -> 3
 using ShadeC16H64Split = ShadeCfg<16, 32, 64, 2, true>;
 
 extern "C" {
@@ -648,6 +709,12 @@ int ds_mlp_param_count(int C, int hidden, int n_layers) {
     return hidden * in + hidden + (n_layers - 1) * (hidden * hidden + hidden) + 3 * hidden + 3;
 }
 
+int ds_step_mlp_param_count(const ds_step_config* cfg) {
+    if (cfg == nullptr) return set_error(DS_ERR_ARG, "step_mlp_param_count: null config"), -1;
+    // C + 9 inputs with SH2: the count for C + 6 features and a 3-D direction
+    return ds_mlp_param_count(cfg->C + (cfg->view_enc ? 6 : 0), cfg->hidden, cfg->n_layers);
+}
+
 int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_tiles, int64_t num_pixels,
                   const float* verts, const int* tri, const float* mvp, const float* inv_mvp, const float* feat_src,
                   const float* alpha_src, const float* mlp_params, const float* target, uint64_t* rng,
@@ -661,14 +728,17 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     DS_CHECK_ARG(c.stochastic == 0 || rng != nullptr, "train_step: stochastic opacity needs the rng state");
     DS_CHECK_ARG(c.precision == 0 || c.precision == 1, "train_step: precision must be 0 (bf16) or 1 (split bf16)");
     DS_CHECK_ARG(c.block_shape >= 0 && c.block_shape <= 2, "train_step: block_shape must be 0 (8x4), 1 (16x2) or 2 (4x8)");
-    const bool k8 = shade_dispatch_check<ShadeC8H16>(c), k16 = shade_dispatch_check<ShadeC16H64>(c);
-    DS_CHECK_ARG(k8 || k16, "train_step: unsupported MLP (C=%d hidden=%d layers=%d); built: 8/16/1, 16/64/2", c.C,
-                 c.hidden, c.n_layers);
+    DS_CHECK_ARG(c.view_enc == 0 || c.view_enc == 1, "train_step: view_enc must be 0 (direction) or 1 (SH2)");
+    const int shape = shade_shape(c);
+    DS_CHECK_ARG(shape != kShadeUnsupported,
+                 "train_step: unsupported MLP (C=%d, %s, hidden=%d, layers=%d); built: 8+dir->16->3, "
+                 "7+SH2->16->16->3, 16+dir->64->64->3", c.C, c.view_enc ? "SH2" : "dir", c.hidden, c.n_layers);
+    const int CP = feat_stride(c);
     const int S = (int)total_feats((uint32_t)c.min_level, (uint32_t)c.max_level);
     const int ST = (int)feats_at_level((uint32_t)c.max_level);
     DS_CHECK_ARG(S * c.C <= kMaxSrc, "train_step: %d samples x %d channels exceed the per-triangle limit", S, c.C);
     DS_CHECK_ARG(num_pixels <= 0xffffffffLL, "train_step: more than 2^32 pixels");
-    DS_CHECK_ARG(c.frag_records >= 0.f && record_capacity(c, num_tiles, num_pixels) <= 0x7fffffffLL - kMaxTileWarps * kRecChunk,
+    DS_CHECK_ARG(c.frag_records >= 0.f && record_capacity(c, num_tiles, num_pixels) <= 0x7fffffffLL - max_resident_warps() * kRecChunk,
                  "train_step: frag_records %g gives too many records", (double)c.frag_records);
     size_t need = 0;
     StepWs w = carve_step(workspace, c, num_tiles, num_pixels, list_capacity, &need);
@@ -681,7 +751,7 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     // zero the accumulators of this step
     DS_CUDA(cudaMemsetAsync(w.grad_pos, 0,
                             reinterpret_cast<char*>(w.rec_counters + 2) - reinterpret_cast<char*>(w.grad_pos), st));
-    DS_CUDA(cudaMemsetAsync(grad_mlp_params, 0, sizeof(float) * ds_mlp_param_count(c.C, c.hidden, c.n_layers), st));
+    DS_CUDA(cudaMemsetAsync(grad_mlp_params, 0, sizeof(float) * ds_step_mlp_param_count(&c), st));
 
     // Side stream for independent parts; the phase events (profiling) time
     // the phases one after another on st instead.
@@ -694,23 +764,24 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     const bool tab = lattice_tab_fits(c.min_level, c.max_level, S, ST, c.C);
     const size_t tsm = lattice_tab_smem(c.min_level, c.max_level, S, ST, c.C);
     const int64_t tw = ((int64_t)c.T + kTabWarps - 1) / kTabWarps;
-    const unsigned tgrid = (unsigned)(tw < kSMs * 4 ? tw : kSMs * 4);  // persistent: tables built once per CTA
+    const int64_t nsm = sm_count();
+    const unsigned tgrid = (unsigned)(tw < nsm * 4 ? tw : nsm * 4);  // persistent: tables built once per CTA
     // the adjoint copies the tables instead of building them, so more CTAs pay
-    const unsigned tgrid_bwd = (unsigned)(tw < kSMs * 8 ? tw : kSMs * 8);
+    const unsigned tgrid_bwd = (unsigned)(tw < nsm * 8 ? tw : nsm * 8);
     if (c.T > 0 && tab) {
-        if (k8)
-            accum_tab_kernel<8><<<tgrid, kTabWarps * 32, tsm, sst>>>(c.T, c.min_level, c.max_level, S, ST, alpha_src,
-                                                                   feat_src, w.alpha_acc, w.feat_acc, w.feat_bf16,
-                                                                   w.tab);
-        else
-            accum_tab_kernel<16><<<tgrid, kTabWarps * 32, tsm, sst>>>(c.T, c.min_level, c.max_level, S, ST, alpha_src,
-                                                                    feat_src, w.alpha_acc, w.feat_acc, w.feat_bf16,
-                                                                   w.tab);
+#define DSB_ACCUM_TAB(CC, CPP)                                                                                     \
+    accum_tab_kernel<CC, CPP><<<tgrid, kTabWarps * 32, tsm, sst>>>(c.T, c.min_level, c.max_level, S, ST, alpha_src, \
+                                                                   feat_src, w.alpha_acc, w.feat_acc, w.feat_bf16, \
+                                                                   w.tab)
+        if (c.C == 8) DSB_ACCUM_TAB(8, 8);
+        else if (c.C == 7) DSB_ACCUM_TAB(7, 8);
+        else DSB_ACCUM_TAB(16, 16);
+#undef DSB_ACCUM_TAB
     } else if (c.T > 0) {
         accum_sigmoid_kernel<false><<<tb, kPrepWarps * 32, 0, sst>>>(c.T, c.min_level, c.max_level, c.max_level, S, ST,
-                                                                    1, alpha_src, w.alpha_acc, nullptr);
+                                                                    1, 1, alpha_src, w.alpha_acc, nullptr);
         accum_sigmoid_kernel<true><<<tb, kPrepWarps * 32, 0, sst>>>(c.T, c.min_level, c.max_level, c.max_level, S, ST,
-                                                                   c.C, feat_src, w.feat_acc, w.feat_bf16);
+                                                                   c.C, CP, feat_src, w.feat_acc, w.feat_bf16);
     }
     if ((int64_t)c.B * c.V > 0)
         project_kernel<<<blocks_for((int64_t)c.B * c.V), kThreads, 0, st>>>(c.B, c.V, verts, mvp, w.pos);
@@ -735,10 +806,17 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     a.inv_n = (float)(1.0 / ((double)num_pixels * 3.0));
     a.color = color_out ? color_out : w.color; a.grad_color = w.grad_color; a.l1 = w.l1;
     a.grad_feat = w.grad_feat_acc; a.grad_params = grad_mlp_params; a.loss_sum = w.loss_sum;
-    if (c.precision == 1)
-        rc = k8 ? launch_shade<ShadeC8H16Split>(a, st) : launch_shade<ShadeC16H64Split>(a, st);
-    else
-        rc = k8 ? launch_shade_small(a, st) : launch_shade<ShadeC16H64>(a, st);
+    const bool split = c.precision == 1;
+    switch (shape) {
+        case kShadeC8Dir16:
+            rc = split ? launch_shade_reg<ShadeC8Dir16Split>(a, st) : launch_shade_reg<ShadeC8Dir16>(a, st);
+            break;
+        case kShadeC7Sh2_16x2:
+            rc = split ? launch_shade_reg<ShadeC7Sh2_16x2Split>(a, st) : launch_shade_reg<ShadeC7Sh2_16x2>(a, st);
+            break;
+        default:
+            rc = split ? launch_shade<ShadeC16H64Split>(a, st) : launch_shade<ShadeC16H64>(a, st);
+    }
     if (rc || (rc = mark(4, st))) return rc;
 
     // opacity auxiliary gradient (scaled by 1/numel(colour), rasterize.py:183-195), on the side
@@ -756,20 +834,20 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     if (side && (rc = join_from(side, 1, st))) return rc;  // the adjoints read the opacity gradients
     // adjoints of sigmoid + level accumulation, and of the projection
     if (c.T > 0 && tab) {
-        if (k8)
-            accum_tab_backward_kernel<8><<<tgrid_bwd, kTabWarps * 32, tsm, st>>>(
-                c.T, c.min_level, c.max_level, S, ST, w.alpha_acc, w.grad_alpha_acc, w.feat_acc, w.grad_feat_acc,
-                grad_alpha_src, grad_feat_src, w.tab);
-        else
-            accum_tab_backward_kernel<16><<<tgrid_bwd, kTabWarps * 32, tsm, st>>>(
-                c.T, c.min_level, c.max_level, S, ST, w.alpha_acc, w.grad_alpha_acc, w.feat_acc, w.grad_feat_acc,
-                grad_alpha_src, grad_feat_src, w.tab);
+#define DSB_ACCUM_TAB_BWD(CC, CPP)                                                                                 \
+    accum_tab_backward_kernel<CC, CPP><<<tgrid_bwd, kTabWarps * 32, tsm, st>>>(                                    \
+        c.T, c.min_level, c.max_level, S, ST, w.alpha_acc, w.grad_alpha_acc, w.feat_acc, w.grad_feat_acc,          \
+        grad_alpha_src, grad_feat_src, w.tab)
+        if (c.C == 8) DSB_ACCUM_TAB_BWD(8, 8);
+        else if (c.C == 7) DSB_ACCUM_TAB_BWD(7, 8);
+        else DSB_ACCUM_TAB_BWD(16, 16);
+#undef DSB_ACCUM_TAB_BWD
     } else if (c.T > 0) {
         accum_sigmoid_backward_kernel<<<tb, kPrepWarps * 32, 0, st>>>(c.T, c.min_level, c.max_level, c.max_level, S,
-                                                                      ST, 1, w.alpha_acc, w.grad_alpha_acc,
+                                                                      ST, 1, 1, w.alpha_acc, w.grad_alpha_acc,
                                                                       grad_alpha_src);
         accum_sigmoid_backward_kernel<<<tb, kPrepWarps * 32, 0, st>>>(c.T, c.min_level, c.max_level, c.max_level, S,
-                                                                      ST, c.C, w.feat_acc, w.grad_feat_acc,
+                                                                      ST, c.C, CP, w.feat_acc, w.grad_feat_acc,
                                                                       grad_feat_src);
     }
     if (c.V > 0) project_backward_kernel<<<blocks_for(c.V), kThreads, 0, st>>>(c.B, c.V, mvp, w.grad_pos, grad_verts);

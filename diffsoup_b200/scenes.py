@@ -162,12 +162,18 @@ def _ring_views(n: int, radius: float, width: int, height: int, elevation: float
 
 
 def make_scene(config: int, seed: int = 0, *, num_tris: Optional[int] = None, num_views: Optional[int] = None,
-               resolution: Optional[Tuple[int, int]] = None, with_targets: bool = True) -> Scene:
+               resolution: Optional[Tuple[int, int]] = None, with_targets: bool = True,
+               shading: str = "config") -> Scene:
     """Build benchmark configuration `config` (1-5) with `seed`.
 
     num_tris / num_views / resolution shrink a configuration for fast parity
-    tests while keeping its distributions.
+    tests while keeping its distributions.  shading="reference" keeps the
+    configuration's soup, views and levels but shades it with the reference's
+    own model (examples/02_synthetic.py:289-306, 364): 7 features, the SH2
+    view encoding and ColorMLP(16, hidden 16, n_layers 2).
     """
+    if shading not in ("config", "reference"):
+        raise ValueError(f"shading must be 'config' or 'reference', not {shading!r}")
     rng = np.random.default_rng(np.random.PCG64(seed * 1000003 + config))
     if config in (1, 4):
         T = num_tris or 5000
@@ -221,6 +227,9 @@ def make_scene(config: int, seed: int = 0, *, num_tris: Optional[int] = None, nu
         lo, hi, C, hid, nl, prec = 0, 3, 16, 64, 2, "bf16"
     else:
         raise ValueError(f"unknown config {config}")
+    enc = "dir3"
+    if shading == "reference":
+        C, hid, nl, enc = 7, 16, 2, "sh2"
 
     T = verts.shape[0] // 3
     tri = np.arange(3 * T, dtype=np.int32).reshape(T, 3)
@@ -231,7 +240,7 @@ def make_scene(config: int, seed: int = 0, *, num_tris: Optional[int] = None, nu
     if with_targets:
         targets = [rng.uniform(0.0, 1.0, size=(v.height, v.width, 3)).astype(np.float32) for v in views]
     return Scene(
-        name=f"config{config}",
+        name=f"config{config}" + ("-refmodel" if shading == "reference" else ""),
         verts=verts.astype(np.float32),
         tri=tri,
         views=views,
@@ -242,7 +251,7 @@ def make_scene(config: int, seed: int = 0, *, num_tris: Optional[int] = None, nu
         alpha_src=alpha_src,
         hidden_dim=hid,
         n_layers=nl,
-        view_enc="dir3",
+        view_enc=enc,
         precision=prec,
         seed=seed,
         targets=targets,

@@ -9,14 +9,19 @@ examples/02_synthetic.py:354-385 computes with an MSE photometric loss:
     feat  = sigmoid(accumulate_to_level(lo, hi, feat_src))
     pos   = project_vertices(verts, mvp)
     rast  = rasterize_multires_triangle_alpha((H, W), pos, tri, hi, alpha)
-    x     = cat(multires_triangle_color(rast, hi, feat), view_dir(rast))
+    x     = cat(multires_triangle_color(rast, hi, feat), enc(rast))
+            enc = view direction (3) or encode_view_dir_sh2 (9)
     color = mask * ColorMLP(x, mask) + (1 - mask)
     loss  = opacity_aux_loss(...) + mse(edge_grad(color, ...), target)
 
 and the gradients of loss with respect to verts, feat_src, alpha_src and the
-MLP parameters.  The shading MLP runs in BF16 on the tensor cores with FP32
-accumulation, features are gathered in BF16; coverage, depth and the
-triangle-ID buffer are exact FP32 as in the reference.
+MLP parameters.  The shading MLP runs on the BF16 tensor cores with FP32
+accumulation, with BF16 operands (precision="bf16") or every operand split
+into two BF16 planes (precision="split", gradients within ~1e-5 of FP64);
+coverage, depth and the triangle-ID buffer are exact FP32 as in the
+reference.  Shading MLPs with fused kernels: the reference's own model
+(7 features + SH2 -> 16 -> 16 -> 3, examples/02_synthetic.py:289-306),
+8 features + direction -> 16 -> 3 and 16 features + direction -> 64 -> 64 -> 3.
 """
 
 from __future__ import annotations
@@ -35,12 +40,14 @@ class StepConfig(C.Structure):
     _fields_ = [("B", C.c_int32), ("T", C.c_int32), ("V", C.c_int32), ("C", C.c_int32), ("min_level", C.c_int32),
                 ("max_level", C.c_int32), ("hidden", C.c_int32), ("n_layers", C.c_int32),
                 ("stochastic", C.c_int32), ("thr_const", C.c_float), ("frag_records", C.c_float),
-                ("precision", C.c_int32), ("block_shape", C.c_int32)]
+                ("precision", C.c_int32), ("block_shape", C.c_int32), ("view_enc", C.c_int32)]
 
 
 _L = _core.lib
 _L.ds_mlp_param_count.restype = C.c_int
 _L.ds_mlp_param_count.argtypes = [C.c_int, C.c_int, C.c_int]
+_L.ds_step_mlp_param_count.restype = C.c_int
+_L.ds_step_mlp_param_count.argtypes = [C.POINTER(StepConfig)]
 _L.ds_train_step_workspace_size.restype = C.c_size_t
 _L.ds_train_step_workspace_size.argtypes = [C.POINTER(StepConfig), C.c_int, C.c_int64, C.c_int64]
 _L.ds_train_step_layout.restype = C.c_int
@@ -89,7 +96,7 @@ class TrainStep:
     def __init__(self, T: int, V: int, hw: Sequence[Tuple[int, int]], C_: int, min_level: int, max_level: int,
                  hidden: int, n_layers: int, stochastic: bool = True, seed: int = 0,
                  device: Optional[torch.device] = None, list_capacity: Optional[int] = None,
-                 frag_records: float = 2.0, precision: str = "bf16"):
+                 frag_records: float = 2.0, precision: str = "bf16", view_enc: str = "dir3"):
         self.device = torch.device(device or "cuda")
         self.hw = [(int(h), int(w)) for h, w in hw]
         self.B = len(self.hw)
@@ -97,13 +104,17 @@ class TrainStep:
         # opacity auxiliary gradient (0: that pass re-enumerates the tiles)
         # precision: "bf16" (BF16 operands) or "split" (every MLP operand as bf16 hi + lo, three
         # tensor-core products each; gradients within ~1e-5 of FP64)
+        # view_enc: "dir3" (the 3-D view direction) or "sh2" (encode_view_dir_sh2, 9 inputs)
         if precision not in ("bf16", "split"):
             raise ValueError(f"precision must be 'bf16' or 'split', not {precision!r}")
+        if view_enc not in ("dir3", "sh2"):
+            raise ValueError(f"view_enc must be 'dir3' or 'sh2', not {view_enc!r}")
         self.cfg = StepConfig(self.B, T, V, C_, min_level, max_level, hidden, n_layers, int(stochastic), 0.5,
-                              float(frag_records), 1 if precision == "split" else 0, 0)
+                              float(frag_records), 1 if precision == "split" else 0, 0, 1 if view_enc == "sh2" else 0)
         self.views, self.num_tiles, self.num_pixels, self.pix_offsets = _tiles.view_table(self.hw, self.device)
         self.S = sum(_core.feats_at_level(l) for l in range(min_level, max_level + 1))
-        self.nparam = mlp_param_count(C_, hidden, n_layers)
+        self.nparam = int(_L.ds_step_mlp_param_count(C.byref(self.cfg)))
+        self.CP = (C_ + 7) // 8 * 8  # channel stride of the step's accumulated feature tables
         self.rng = torch.tensor([seed, 0], dtype=torch.int64, device=self.device)
         self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
         self.loss = torch.zeros(1, dtype=torch.float32, device=self.device)
@@ -129,11 +140,11 @@ class TrainStep:
         ST = _core.feats_at_level(c.max_level)
         shapes: Dict[str, Tuple[torch.dtype, Tuple[int, ...]]] = {
             "pos": (torch.float32, (c.B, c.V, 4)), "alpha_acc": (torch.float32, (c.T, ST)),
-            "feat_acc": (torch.float32, (c.T, ST, c.C)), "feat_bf16": (torch.bfloat16, (c.T, ST, c.C)),
+            "feat_acc": (torch.float32, (c.T, ST, self.CP)), "feat_bf16": (torch.bfloat16, (c.T, ST, self.CP)),
             "rast": (torch.float32, (self.num_pixels, 4)), "color": (torch.float32, (self.num_pixels, 3)),
             "grad_color": (torch.float32, (self.num_pixels, 3)), "l1": (torch.float32, (self.num_pixels,)),
             "grad_pos": (torch.float64, (c.B, c.V, 4)), "grad_alpha_acc": (torch.float32, (c.T, ST)),
-            "grad_feat_acc": (torch.float32, (c.T, ST, c.C)),
+            "grad_feat_acc": (torch.float32, (c.T, ST, self.CP)),
             "records": (torch.int32, (self.record_capacity, 4)),
             "chunk_fill": (torch.int32, (self.record_capacity // 256,)),
             "record_counters": (torch.int32, (2,)), "fallback_blocks": (torch.int32, (self.num_tiles * 8 if self.record_capacity else 0,)),
@@ -200,7 +211,7 @@ class TrainStep:
         device and workload (`autotune_cache`).  Returns them."""
         key = (torch.cuda.get_device_name(self.device), self.B, tuple(self.hw), self.cfg.T, self.cfg.V, self.cfg.C,
                self.cfg.min_level, self.cfg.max_level, self.cfg.hidden, self.cfg.n_layers, self.cfg.precision,
-               self.cfg.stochastic)
+               self.cfg.stochastic, self.cfg.view_enc)
         it0 = self.rng[1].clone()
         hit = autotune_cache.get(key)
         if hit is not None:

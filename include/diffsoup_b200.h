@@ -90,7 +90,9 @@ int ds_depth_test(int B, int H, int W, int num_frags, const int* frag_pix, const
  * to 2^21 pixels (larger batches return DS_ERR_ARG).  All calls on a device
  * share that buffer (each clears what it uses); calls whose GPU work overlaps
  * race on it.  The first call on each device looks up the buffer's address
- * (cudaGetSymbolAddress); make it before any stream capture. */
+ * (cudaGetSymbolAddress); make it before any stream capture.  That address is
+ * cached for the device's context: do not use this entry point across a
+ * cudaDeviceReset.  Fragments outside the batch are skipped. */
 int ds_depth_test_noalloc(int B, int H, int W, int num_frags, const int* frag_pix, const float* frag_attrs,
                           const float* frag_alpha, const float* alpha_thresh, float* rast, ds_stream_t stream);
 
@@ -211,12 +213,17 @@ int ds_tiles_opacity_aux(int B, const ds_view_desc* views, int num_tiles, int V,
  *   feat  = sigmoid(accumulate_to_level(min..max -> max, feat_src))
  *   pos   = project(verts, mvp)                                (utils.py:412-426)
  *   rast  = rasterize_multires_triangle_alpha(pos, tri, max, alpha, stochastic)
- *   x     = [multires_triangle_color(rast, feat), view_dir(rast, inv_mvp)]
+ *   x     = [multires_triangle_color(rast, feat), enc(rast, inv_mvp)]
+ *           enc = the 3-D view direction, or encode_view_dir_sh2 (9
+ *           coefficients, examples/02_synthetic.py:364) with view_enc = 1
  *   color = mask ? ColorMLP(x) : 1;  loss = mean((color - target)^2)
  *           + opacity_aux_loss(...) + edge_grad(...)   (zero-valued hooks)
  * and the gradients of loss with respect to verts, feat_src, alpha_src and
- * the MLP parameters (overwritten, not accumulated).  The MLP runs in BF16 on
- * the tensor cores with FP32 accumulation; features are gathered as BF16.
+ * the MLP parameters (overwritten, not accumulated).  The MLP runs on the
+ * BF16 tensor cores with FP32 accumulation (see `precision`).  Built shading
+ * MLPs (features + encoding -> hidden layers -> 3): the reference's own model
+ * 7 + SH2 -> 16 -> 16 -> 3 (examples/02_synthetic.py:289-306), 8 + direction
+ * -> 16 -> 3 and 16 + direction -> 64 -> 64 -> 3; others return DS_ERR_ARG.
  * Never host-synchronising; capturable in a CUDA graph.  With stochastic
  * opacity, rng = device uint64[2] {seed, iteration} and the iteration is
  * incremented on the device at the end of the step. */
@@ -224,7 +231,7 @@ typedef struct {
     int32_t B, T, V;         /* views, triangles, vertices */
     int32_t C;               /* feature channels */
     int32_t min_level, max_level;
-    int32_t hidden, n_layers;/* shading MLP: (C+3) -> hidden x n_layers -> 3 */
+    int32_t hidden, n_layers;/* shading MLP: (C+enc) -> hidden x n_layers -> 3 */
     int32_t stochastic;      /* 1: Philox threshold per (view, pixel, triangle); 0: thr_const */
     float thr_const;
     /* Fragment records per pixel reserved in the workspace (plus one chunk
@@ -244,12 +251,18 @@ typedef struct {
      * 1 = 16x2, 2 = 4x8.  Same results; the fastest depends on the scene
      * (diffsoup_b200.step.TrainStep.autotune times them). */
     int32_t block_shape;
+    /* View encoding appended to the features: 0 = the 3-D view direction
+     * (3 inputs), 1 = its SH2 coefficients (9 inputs, encoding.cu:56-118). */
+    int32_t view_enc;
 } ds_step_config;
 
 /* Packed MLP parameter layout (fp32): W0[hidden][C+3] b0[hidden]
  * (Wl[hidden][hidden] bl[hidden]) x (n_layers-1) Wout[3][hidden] bout[3],
  * i.e. torch.nn.Linear weights in ColorMLP order. */
 int ds_mlp_param_count(int C, int hidden, int n_layers);
+
+/* The same count for a step's MLP: W0 has C+3 or C+9 columns (view_enc). */
+int ds_step_mlp_param_count(const ds_step_config* cfg);
 
 size_t ds_train_step_workspace_size(const ds_step_config* cfg, int num_tiles, int64_t num_pixels,
                                     int64_t list_capacity);
@@ -261,9 +274,10 @@ int ds_train_step_set_events(void* const* events, int n);
 
 /* Byte offsets inside the train-step workspace of its intermediates, for
  * inspection after a step: [0] pos [B,V,4] f32, [1] opacity [T,S_max] f32,
- * [2] features [T,S_max,C] f32, [3] features bf16, [4] rast [pixels,4],
+ * [2] features [T,S_max,Cp] f32 (Cp = C rounded up to a multiple of 8,
+ * padding channels zero), [3] features bf16 [T,S_max,Cp], [4] rast [pixels,4],
  * [5] colour [pixels,3], [6] dL/dcolour [pixels,3], [7] |c - target| summed
- * [pixels], [8] dL/dpos [B,V,4] f64, [9] dL/dopacity, [10] dL/dfeatures,
+ * [pixels], [8] dL/dpos [B,V,4] f64, [9] dL/dopacity, [10] dL/dfeatures [T,S_max,Cp],
  * [11] fragment records int32 [capacity,4] {pixel, triangle | visible << 31,
  * b0 bits, b1 bits}, [12] record count of each 256-record chunk int32,
  * [13] int32 {records reserved, blocks re-enumerated}, [14] ids of the

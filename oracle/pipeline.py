@@ -14,6 +14,16 @@ implementation is torch itself (python/diffsoup/multires.py:109-207):
                    the FP32 rasterization, exactly as in the reference.
   precision="f32": the reference's own FP32 arithmetic, multi-threaded (the
                    CPU baseline).
+
+  mlp_rounding="bf16" (with "f64"): the shading MLP with the BF16 operand
+                   rounding of the fused step's BF16 mode and FP64 arithmetic
+                   otherwise -- features gathered from the BF16-rounded
+                   feature table, MLP inputs, weights, hidden activations and
+                   the back-propagated pre-activation gradients rounded to
+                   BF16 where the kernel feeds them to the tensor cores, biases
+                   and their gradients unrounded (csrc/shade_reg.cuh,
+                   csrc/shade.cuh).  It separates the kernel's own arithmetic
+                   from the rounding of its BF16 operands.
 """
 
 from __future__ import annotations
@@ -43,6 +53,7 @@ class StepInputs:
     stochastic: bool = True
     seed: int = 0
     iteration: int = 0
+    view_enc: str = "dir3"       # "dir3": 3-D view direction; "sh2": encode_view_dir_sh2 (9)
 
 
 @dataclass
@@ -65,12 +76,56 @@ def _mlp_forward(x: torch.Tensor, mlp: List[Tuple[torch.Tensor, torch.Tensor]]) 
     return h
 
 
+def bf16(a) -> np.ndarray:
+    """Round to BF16 (nearest even, through FP32) and widen to float64."""
+    t = torch.from_numpy(np.ascontiguousarray(np.asarray(a, np.float64)))
+    return t.float().bfloat16().double().numpy()
+
+
+def _mlp_bf16(feat: np.ndarray, enc: np.ndarray, mlp, tgt: np.ndarray, N: float):
+    """Forward and backward of the blended ColorMLP over the covered pixels
+    (rows of feat [n,C] and enc [n,E]) with the BF16 operand rounding of the
+    fused step.  Returns colour [n,3], dL/dfeat [n,C], [(dW, db)] and the
+    summed squared error."""
+    C = feat.shape[1]
+    xm = bf16(np.concatenate([feat, enc], axis=1))
+    Wr = [bf16(W) for W, _ in mlp]
+    acts = [xm]
+    a = xm
+    for (W, b), Wq in zip(mlp[:-1], Wr[:-1]):
+        a = bf16(np.maximum(a @ Wq.T + b.astype(np.float64), 0.0))
+        acts.append(a)
+    logit = a @ Wr[-1].T + mlp[-1][1].astype(np.float64)
+    s = 1.0 / (1.0 + np.exp(-logit))
+    res = feat[:, 3:4]
+    col = (1.0 - res) * feat[:, :3] + res * s
+    diff = col - tgt
+    gc = 2.0 * diff / N
+    dfeat = np.zeros_like(feat)
+    dfeat[:, :3] = (1.0 - res) * gc
+    dfeat[:, 3] = ((s - feat[:, :3]) * gc).sum(axis=1)
+    dz = res * gc * s * (1.0 - s)
+    grads = [None] * len(mlp)
+    grads[-1] = (bf16(dz).T @ acts[-1], dz.sum(axis=0))
+    d = (bf16(dz) @ Wr[-1]) * (acts[-1] > 0)
+    for l in range(len(mlp) - 2, -1, -1):
+        dr = bf16(d)
+        grads[l] = (dr.T @ acts[l], d.sum(axis=0))
+        if l > 0:
+            d = (dr @ Wr[l]) * (acts[l] > 0)
+        else:
+            dfeat += (dr @ Wr[0])[:, :C]
+    return col, dfeat, grads, float((diff ** 2).sum())
+
+
 def train_step(inp: StepInputs, precision: str = "f64", rast_in: Optional[List[np.ndarray]] = None,
-               pos32: Optional[np.ndarray] = None, alpha32: Optional[np.ndarray] = None) -> StepResult:
+               pos32: Optional[np.ndarray] = None, alpha32: Optional[np.ndarray] = None,
+               mlp_rounding: str = "none") -> StepResult:
     """One forward+backward.  rast_in / pos32 / alpha32 let a caller supply the
     FP32 rasterization inputs of the device under test (they are recomputed
     here otherwise)."""
     f64 = precision == "f64"
+    assert mlp_rounding in ("none", "bf16") and (mlp_rounding == "none" or f64)
     npdt = np.float64 if f64 else np.float32
     tdt = torch.float64 if f64 else torch.float32
     lo, hi = inp.min_level, inp.max_level
@@ -109,8 +164,29 @@ def train_step(inp: StepInputs, precision: str = "f64", rast_in: Optional[List[n
                                            inp.iteration, view0=b)
             nfrag += nf
         rasts.append(rast)
+        vdir = cpu.encode_view(rast, inp.inv_mvps[b:b + 1], sh=inp.view_enc == "sh2",
+                               precision="f64" if f64 else "f32")
+        if mlp_rounding == "bf16":
+            feat = cpu.multires_color(rast, hi, hi, bf16(f_acc), "f64")
+            m = rast[0, ..., 3] > 0
+            tg = inp.targets[b].astype(np.float64)
+            col = np.ones((H, W, 3))
+            dfeat = np.zeros((H, W, feat.shape[-1]))
+            cm, dfm, gm, sq = _mlp_bf16(feat[0][m], vdir[0][m], inp.mlp, tg[m], N)
+            col[m] = cm
+            dfeat[m] = dfm
+            loss += (sq + float(((1.0 - tg[~m]) ** 2).sum())) / N
+            for (W, bb), (gW, gb) in zip(mlp_t, gm):
+                W.grad = (W.grad if W.grad is not None else 0) + torch.from_numpy(gW)
+                bb.grad = (bb.grad if bb.grad is not None else 0) + torch.from_numpy(gb)
+            colors.append(col)
+            gcol = (2.0 * (col - tg) / N)[None]
+            grad_f_acc += cpu.multires_color_backward(rast, hi, hi, T, dfeat[None])
+            grad_pos[b:b + 1] += cpu.edge_grad(col[None], gcol, rast, pos[b:b + 1], inp.tri, precision="f64")
+            grad_a_acc += cpu.opacity_aux(col[None], tg[None], rast, pos32[b:b + 1], inp.tri, hi, a_acc,
+                                          precision="f64") / N
+            continue
         feat = cpu.multires_color(rast, hi, hi, f_acc, "f64" if f64 else "f32")
-        vdir = cpu.encode_view(rast, inp.inv_mvps[b:b + 1], sh=False, precision="f64" if f64 else "f32")
         xf = torch.tensor(feat, dtype=tdt, requires_grad=True)
         x = torch.cat([xf, torch.tensor(vdir, dtype=tdt)], dim=-1)
         mask = torch.tensor(rast[..., 3] > 0)
