@@ -117,46 +117,101 @@ __device__ __forceinline__ void split_point(const SplitParams& P, const float* A
     for (int k = 0; k < 3; ++k) C[k] = __fadd_rn(__fmul_rn(tA, A[k]), __fmul_rn(tB, B[k]));
 }
 
-// Walks the split tree of face t.  Counting pass (EMIT false): returns the
-// number of splits.  Emitting pass: writes the family's faces, its new
-// vertices from vbase and its new slots from fbase.  Both passes take the
-// same decisions; a family that would exceed max_splits (or the stack) stops
-// splitting and raises DS_STATUS_SPLIT_LIMIT, which the host turns into an
-// error after the counting pass.
-template <bool EMIT>
-__device__ int64_t walk_family(const SplitParams& P, SplitPlan plan, int quota, int t, const float* __restrict__ verts,
-                               const int* __restrict__ faces, bool splittable, int64_t max_splits, int64_t vbase,
-                               int64_t fbase, float* __restrict__ out_verts, int* __restrict__ out_faces,
-                               int* __restrict__ status, unsigned long long* __restrict__ total) {
-    SplitNode stack[kSplitStack];
-    int top = 0;
-    SplitNode cur;
+// The longest considered edge of a node: e = 0 (0,1), 1 (1,2), 2 (2,0),
+// first of equals; -1 when no edge is considered.
+__device__ __forceinline__ int longest_edge(const SplitParams& P, const SplitNode& cur, const ClipPoint* q,
+                                            float& best) {
+    int e = -1;
+    best = 0.f;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        cur.id[k] = faces[(size_t)t * 3 + k];
-#pragma unroll
-        for (int j = 0; j < 3; ++j) cur.p[k * 3 + j] = verts[(size_t)cur.id[k] * 3 + j];
+        const float l2 = edge_len2(P, cur.p + k * 3, cur.p + ((k + 1) % 3) * 3, q[k], q[(k + 1) % 3]);
+        const bool considered = P.mode == 0 || l2 > 0.f;
+        if (considered && (e < 0 || l2 > best)) { e = k; best = l2; }
     }
-    cur.slot = t;
-    ClipPoint q[3];  // clip points of cur's corners (clip mode)
+    return e;
+}
+
+__device__ __forceinline__ void node_clip_points(const SplitParams& P, const SplitNode& n, ClipPoint* q) {
     if (P.mode == 1) {
 #pragma unroll
-        for (int k = 0; k < 3; ++k) q[k] = clip_point(P, cur.p + k * 3);
+        for (int k = 0; k < 3; ++k) q[k] = clip_point(P, n.p + k * 3);
     }
+}
+
+// Splits node cur at edge e as split number k of its family: the first child
+// (a, mA, cA) keeps the slot, the second (mB, b, c) takes slot fbase + k;
+// mA = vbase + 3k, mB = mA + 1, cA = mA + 2.  EMIT writes the three new
+// vertices and the new slot's face mapping (family t) and flag.
+template <bool EMIT>
+__device__ __forceinline__ void split_node(const SplitParams& P, const SplitNode& cur, const ClipPoint* q, int e,
+                                           int64_t k, int64_t vbase, int64_t fbase, int t, SplitNode& first,
+                                           SplitNode& second, float* __restrict__ out_verts, int* __restrict__ map,
+                                           int* __restrict__ flag) {
+    const int ia = e, ib = (e + 1) % 3, ic = (e + 2) % 3;  // edge (a, b), opposite c
+    float C[3];
+    split_point(P, cur.p + ia * 3, cur.p + ib * 3, q[ia], q[ib], C);
+    const int mA = (int)(vbase + 3 * k), mB = mA + 1, cA = mA + 2;
+    second.slot = (int)(fbase + k);
+    second.id[0] = mB; second.id[1] = cur.id[ib]; second.id[2] = cur.id[ic];
+    first.slot = cur.slot;
+    first.id[0] = cur.id[ia]; first.id[1] = mA; first.id[2] = cA;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        second.p[j] = C[j];
+        second.p[3 + j] = cur.p[ib * 3 + j];
+        second.p[6 + j] = cur.p[ic * 3 + j];
+        first.p[j] = cur.p[ia * 3 + j];
+        first.p[3 + j] = C[j];
+        first.p[6 + j] = cur.p[ic * 3 + j];
+    }
+    if (EMIT) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            out_verts[(size_t)mA * 3 + j] = C[j];
+            out_verts[(size_t)mB * 3 + j] = C[j];
+            out_verts[(size_t)cA * 3 + j] = cur.p[ic * 3 + j];
+        }
+        map[second.slot] = t;
+        flag[second.slot] = 0;
+    }
+}
+
+__device__ __forceinline__ SplitNode family_root(int t, const float* __restrict__ verts, const int* __restrict__ faces) {
+    SplitNode n;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        n.id[k] = faces[(size_t)t * 3 + k];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) n.p[k * 3 + j] = verts[(size_t)n.id[k] * 3 + j];
+    }
+    n.slot = t;
+    return n;
+}
+
+// Walks the split tree below `root` depth first (first child before second
+// child), numbering its splits k0, k0 + 1, ...  Counting pass (EMIT false):
+// returns the number of splits.  Emitting pass: writes the faces of its
+// leaves, its new vertices (from vbase) and new slots (from fbase).  Both
+// passes take the same decisions; a walk that would exceed max_splits (or
+// the stack) stops splitting and raises DS_STATUS_SPLIT_LIMIT, which the host
+// turns into an error after the counting pass.  `quota` counts down the
+// cut-off-length splits the walk may still take (a split budget's ties).
+template <bool EMIT>
+__device__ int64_t walk_subtree(const SplitParams& P, SplitPlan plan, int quota, SplitNode cur, bool splittable,
+                                int64_t max_splits, int64_t k0, int64_t vbase, int64_t fbase, int t,
+                                float* __restrict__ out_verts, int* __restrict__ out_faces, int* __restrict__ map,
+                                int* __restrict__ flag, int* __restrict__ status,
+                                unsigned long long* __restrict__ total) {
+    SplitNode stack[kSplitStack];
+    int top = 0;
+    ClipPoint q[3];  // clip points of cur's corners (clip mode)
+    node_clip_points(P, cur, q);
     int64_t splits = 0;
     bool stop = !splittable;
     while (true) {
-        // longest considered edge: e = 0 (0,1), 1 (1,2), 2 (2,0); first of equals
-        int e = -1;
         float best = 0.f;
-        if (!stop) {
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                const float l2 = edge_len2(P, cur.p + k * 3, cur.p + ((k + 1) % 3) * 3, q[k], q[(k + 1) % 3]);
-                const bool considered = P.mode == 0 || l2 > 0.f;
-                if (considered && (e < 0 || l2 > best)) { e = k; best = l2; }
-            }
-        }
+        const int e = stop ? -1 : longest_edge(P, cur, q, best);
         const bool tie = quota > 0 && best == plan.tie2;
         const bool split = e >= 0 && best > 0.f && (best >= plan.tau2 || tie);
         if (split && (top == kSplitStack || splits >= max_splits)) {
@@ -165,52 +220,24 @@ __device__ int64_t walk_family(const SplitParams& P, SplitPlan plan, int quota, 
             continue;
         }
         if (split) {
-            // the call's total, charged every 256 splits of a family
+            // the call's total, charged every 256 splits of a walk
             if (!EMIT && splits > 0 && (splits & 255) == 0 &&
                 atomicAdd(total, 256ull) > (unsigned long long)kMaxTotalSplits) {
                 atomicOr(status, DS_STATUS_SPLIT_LIMIT);
                 stop = true;
                 continue;
             }
-            const int ia = e, ib = (e + 1) % 3, ic = (e + 2) % 3;  // edge (a, b), opposite c
-            float C[3];
-            split_point(P, cur.p + ia * 3, cur.p + ib * 3, q[ia], q[ib], C);
             if (tie && !(best >= plan.tau2)) --quota;
-            const int64_t k = splits++;
-            const int mA = (int)(vbase + 3 * k), mB = mA + 1, cA = mA + 2;
-            SplitNode second;  // (mB, b, c) in a new slot
-            second.slot = (int)(fbase + k);
-            second.id[0] = mB; second.id[1] = cur.id[ib]; second.id[2] = cur.id[ic];
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                second.p[j] = C[j];
-                second.p[3 + j] = cur.p[ib * 3 + j];
-                second.p[6 + j] = cur.p[ic * 3 + j];
-            }
-            if (EMIT) {
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    out_verts[(size_t)mA * 3 + j] = C[j];
-                    out_verts[(size_t)mB * 3 + j] = C[j];
-                    out_verts[(size_t)cA * 3 + j] = cur.p[ic * 3 + j];
-                }
-            }
-            // (a, mA, cA) keeps the slot and is walked next
-            SplitNode first;
-            first.slot = cur.slot;
-            first.id[0] = cur.id[ia]; first.id[1] = mA; first.id[2] = cA;
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                first.p[j] = cur.p[ia * 3 + j];
-                first.p[3 + j] = C[j];
-                first.p[6 + j] = cur.p[ic * 3 + j];
-            }
+            SplitNode first, second;
+            split_node<EMIT>(P, cur, q, e, k0 + splits, vbase, fbase, t, first, second, out_verts, map, flag);
+            ++splits;
+            const int ia = e, ic = (e + 2) % 3;
             stack[top++] = second;
             cur = first;
             if (P.mode == 1) {  // corners (a, C, c)
                 const ClipPoint qa = q[ia], qc = q[ic];
                 q[0] = qa;
-                q[1] = clip_point(P, C);
+                q[1] = clip_point(P, cur.p + 3);
                 q[2] = qc;
             }
             continue;
@@ -221,48 +248,159 @@ __device__ int64_t walk_family(const SplitParams& P, SplitPlan plan, int quota, 
         }
         if (top == 0) break;
         cur = stack[--top];
-        if (P.mode == 1) {
-#pragma unroll
-            for (int k = 0; k < 3; ++k) q[k] = clip_point(P, cur.p + k * 3);
-        }
+        node_clip_points(P, cur, q);
     }
     return splits;
 }
 
-__global__ void __launch_bounds__(kSplitThreads) split_count_kernel(SplitParams P, SplitPlan plan, int M,
-                                                                    const float* __restrict__ verts,
-                                                                    const int* __restrict__ faces,
-                                                                    const int* __restrict__ valid,
-                                                                    const int* __restrict__ quota,
-                                                                    int* __restrict__ counts, int* __restrict__ status,
-                                                                    unsigned long long* __restrict__ total) {
+// A family's split tree is walked in two parts, so that one large family
+// does not serialise the launch: its top kTopLevels levels breadth first (by
+// one thread per family, split_top_kernel), then each of the up to
+// 2^kTopLevels subtrees hanging below them depth first (one thread per
+// subtree, split_task_kernel).  A family's splits are numbered in that order:
+// the top splits level by level, left to right (first child before second),
+// then the subtrees left to right, each in depth-first order.  The top
+// kernel records the split number of every top node in a heap-indexed table
+// (node v has children 2v, 2v + 1; -1: no split there), from which a subtree
+// task rebuilds its root by re-walking the D splits above it.  Families with
+// a tie quota (a split budget's cut-off) are walked depth first by the top
+// kernel alone, since their quota is consumed in walk order.
+constexpr int kTopLevels = 5;
+constexpr int kTopNodes = 1 << kTopLevels;  // subtrees per family; also the size of the heap table
+constexpr short kSerialFamily = -2;        // table[0] of a family walked whole by the top kernel
+
+template <bool EMIT>
+__global__ void __launch_bounds__(kSplitThreads) split_top_kernel(
+    SplitParams P, const SplitPlan* __restrict__ plan_dev, SplitPlan plan_arg, int N, int M,
+    const float* __restrict__ verts, const int* __restrict__ faces, const int* __restrict__ valid,
+    const int* __restrict__ quota, short* __restrict__ table, int* __restrict__ top_count,
+    const int64_t* __restrict__ offsets, float* __restrict__ out_verts, int* __restrict__ out_faces,
+    int* __restrict__ map, int* __restrict__ flag, int* __restrict__ status, unsigned long long* __restrict__ total) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= M) return;
+    const SplitPlan plan = EMIT ? *plan_dev : plan_arg;
     const bool splittable = P.mode == 0 || valid == nullptr || valid[t] > 0;
-    counts[t] = (int)walk_family<false>(P, plan, quota ? quota[t] : 0, t, verts, faces, splittable, kMaxFamilySplits,
-                                        0, 0, nullptr, nullptr, status, total);
+    short* tab = table + (size_t)t * kTopNodes;
+    const int64_t o = EMIT ? offsets[t] : 0, n = EMIT ? offsets[t + 1] - o : 0;
+    const int64_t vbase = N + 3 * o, fbase = M + o;
+    if (EMIT) {
+        map[t] = t;
+        flag[t] = n == 0 ? 1 : 0;
+    }
+    const int qt = quota ? quota[t] : 0;
+    if (qt > 0) {  // a tie quota: the whole family depth first, here
+        const int64_t c = walk_subtree<EMIT>(P, plan, qt, family_root(t, verts, faces), EMIT ? n > 0 : splittable,
+                                             EMIT ? n : kMaxFamilySplits, 0, vbase, fbase, t, out_verts, out_faces,
+                                             map, flag, status, total);
+        if (!EMIT) {
+            top_count[t] = (int)c;
+            tab[0] = kSerialFamily;
+        }
+        return;
+    }
+    SplitNode front[kTopNodes / 2], next[kTopNodes];
+    int fv[kTopNodes / 2], nv[kTopNodes];  // heap indices of the frontier nodes
+    int nf = 1;
+    front[0] = family_root(t, verts, faces);
+    fv[0] = 1;
+    if (!EMIT) {
+        for (int i = 0; i < kTopNodes; ++i) tab[i] = -1;
+    }
+    int k = 0;
+    const bool can = EMIT ? n > 0 : splittable;
+    for (int level = 0; level < kTopLevels && nf > 0; ++level) {
+        int nn = 0;
+        for (int i = 0; i < nf; ++i) {
+            const SplitNode cur = front[i];
+            ClipPoint q[3];
+            node_clip_points(P, cur, q);
+            float best = 0.f;
+            const int e = can ? longest_edge(P, cur, q, best) : -1;
+            if (e >= 0 && best > 0.f && best >= plan.tau2 && (!EMIT || k < n)) {
+                if (!EMIT) tab[fv[i]] = (short)k;
+                split_node<EMIT>(P, cur, q, e, k, vbase, fbase, t, next[nn], next[nn + 1], out_verts, map, flag);
+                nv[nn] = 2 * fv[i];
+                nv[nn + 1] = 2 * fv[i] + 1;
+                nn += 2;
+                ++k;
+            } else if (EMIT) {
+#pragma unroll
+                for (int j = 0; j < 3; ++j) out_faces[(size_t)cur.slot * 3 + j] = cur.id[j];
+            }
+        }
+        if (level + 1 == kTopLevels) break;  // next[] holds the subtree roots: the tasks' work
+        for (int i = 0; i < nn; ++i) {
+            front[i] = next[i];
+            fv[i] = nv[i];
+        }
+        nf = nn;
+    }
+    if (!EMIT) top_count[t] = k;
 }
 
-__global__ void __launch_bounds__(kSplitThreads) split_emit_kernel(SplitParams P, const SplitPlan* __restrict__ plan,
-                                                                   int N, int M, const float* __restrict__ verts,
-                                                                   const int* __restrict__ faces,
-                                                                   const int* __restrict__ quota,
-                                                                   const int64_t* __restrict__ offsets,
-                                                                   float* __restrict__ out_verts,
-                                                                   int* __restrict__ out_faces, int* __restrict__ map,
-                                                                   int* __restrict__ flag, int* __restrict__ status) {
+// Subtree task j of family t: rebuilds its root from the top table (the path
+// of first / second children given by the bits of j, top level first) and
+// walks it depth first.  Counting pass: task_counts[t * kTopNodes + j].
+// Emitting pass: its splits are numbered after the family's top splits and
+// the subtrees to its left (task_scan: inclusive scan of the task counts).
+template <bool EMIT>
+__global__ void __launch_bounds__(kSplitThreads) split_task_kernel(
+    SplitParams P, const SplitPlan* __restrict__ plan_dev, SplitPlan plan_arg, int N, int M,
+    const float* __restrict__ verts, const int* __restrict__ faces, const short* __restrict__ table,
+    const int* __restrict__ top_count, int* __restrict__ task_counts, const int* __restrict__ task_scan,
+    const int64_t* __restrict__ offsets, float* __restrict__ out_verts, int* __restrict__ out_faces,
+    int* __restrict__ map, int* __restrict__ flag, int* __restrict__ status, unsigned long long* __restrict__ total) {
+    const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= (int64_t)M * kTopNodes) return;
+    const int t = (int)(gid / kTopNodes), j = (int)(gid % kTopNodes);
+    const SplitPlan plan = EMIT ? *plan_dev : plan_arg;
+    const short* tab = table + (size_t)t * kTopNodes;
+    if (!EMIT) task_counts[gid] = 0;
+    if (tab[0] == kSerialFamily) return;
+    const int64_t o = EMIT ? offsets[t] : 0, n = EMIT ? offsets[t + 1] - o : 0;
+    if (EMIT && n == 0) return;  // nothing of this family splits (the count was reset)
+    const int64_t vbase = N + 3 * o, fbase = M + o;
+    SplitNode cur = family_root(t, verts, faces);
+    int v = 1;
+    for (int level = 0; level < kTopLevels; ++level) {
+        const int k = tab[v];
+        if (k < 0) return;  // the path ends above this subtree: no task
+        ClipPoint q[3];
+        node_clip_points(P, cur, q);
+        float best = 0.f;
+        const int e = longest_edge(P, cur, q, best);  // the split the top kernel made
+        SplitNode first, second;
+        split_node<false>(P, cur, q, e, k, vbase, fbase, t, first, second, nullptr, nullptr, nullptr);
+        const int bit = (j >> (kTopLevels - 1 - level)) & 1;
+        cur = bit ? second : first;
+        v = 2 * v + bit;
+    }
+    if (!EMIT) {
+        task_counts[gid] = (int)walk_subtree<false>(P, plan, 0, cur, true, kMaxFamilySplits, 0, 0, 0, t, nullptr,
+                                                    nullptr, nullptr, nullptr, status, total);
+        return;
+    }
+    const int64_t fam0 = t > 0 ? task_scan[(int64_t)t * kTopNodes - 1] : 0;  // tasks of earlier families
+    const int mine = task_scan[gid] - (gid > 0 ? task_scan[gid - 1] : 0);
+    const int64_t k0 = top_count[t] + (task_scan[gid] - mine - fam0);
+    if (k0 + mine > n) {  // inconsistent with the offsets given: write nothing out of range
+        atomicOr(status, DS_STATUS_SPLIT_LIMIT);
+        return;
+    }
+    walk_subtree<true>(P, plan, 0, cur, mine > 0, mine, k0, vbase, fbase, t, out_verts, out_faces, map, flag, status,
+                       nullptr);
+}
+
+// counts[t] = the family's top splits + its subtree tasks' splits.
+__global__ void split_family_kernel(int M, const int* __restrict__ top_count, const int* __restrict__ task_scan,
+                                    int* __restrict__ counts, int* __restrict__ status) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= M) return;
-    const int64_t o = offsets[t], n = offsets[t + 1] - o;
-    walk_family<true>(P, *plan, quota[t], t, verts, faces, n > 0, n, N + 3 * o, M + o, out_verts, out_faces, status,
-                      nullptr);
-    // faceMapping / sameAsOriginal of the family's slots (src/remesh.cpp:35-50)
-    map[t] = t;
-    flag[t] = n == 0 ? 1 : 0;
-    for (int64_t k = 0; k < n; ++k) {
-        map[M + o + k] = t;
-        flag[M + o + k] = 0;
-    }
+    const int64_t hi = task_scan[(int64_t)t * kTopNodes + kTopNodes - 1];
+    const int64_t lo = t > 0 ? task_scan[(int64_t)t * kTopNodes - 1] : 0;
+    const int64_t c = top_count[t] + (hi - lo);
+    if (c > kMaxFamilySplits) atomicOr(status, DS_STATUS_SPLIT_LIMIT);
+    counts[t] = (int)(c < kMaxFamilySplits ? c : kMaxFamilySplits);
 }
 
 // Largest considered squared edge length over the faces that may split (as
@@ -320,7 +458,12 @@ static size_t al256(size_t n) { return (n + 255) & ~(size_t)255; }
 struct SplitWs {
     int* counts;
     int* quota;
+    short* table;      // per family: split numbers of its top nodes (heap order)
+    int* top_count;    // per family: splits of its top levels (or of the whole family, walked serially)
+    int* task_counts;  // per (family, subtree): splits of the subtree
+    int* task_scan;    // inclusive scan of task_counts
     void* scan;
+    void* scan_tasks;
     unsigned long long* total;  // limit accounting of a counting pass
     int* probe_status;          // status of the current counting pass
     unsigned* max_bits;         // largest edge (split budget)
@@ -334,7 +477,12 @@ static SplitWs carve_split(void* ws, int M, size_t* bytes) {
     SplitWs w;
     w.counts = reinterpret_cast<int*>(p + o); o += al256(m * sizeof(int));
     w.quota = reinterpret_cast<int*>(p + o); o += al256(m * sizeof(int));
+    w.table = reinterpret_cast<short*>(p + o); o += al256(m * kTopNodes * sizeof(short));
+    w.top_count = reinterpret_cast<int*>(p + o); o += al256(m * sizeof(int));
+    w.task_counts = reinterpret_cast<int*>(p + o); o += al256(m * kTopNodes * sizeof(int));
+    w.task_scan = reinterpret_cast<int*>(p + o); o += al256(m * kTopNodes * sizeof(int));
     w.scan = p + o; o += al256(scan_workspace_bytes((int64_t)m));
+    w.scan_tasks = p + o; o += al256(scan_workspace_bytes((int64_t)m * kTopNodes));
     w.total = reinterpret_cast<unsigned long long*>(p + o);
     w.probe_status = reinterpret_cast<int*>(p + o + 8);
     w.max_bits = reinterpret_cast<unsigned*>(p + o + 12);
@@ -352,10 +500,18 @@ static int64_t count_pass(const SplitParams& P, SplitPlan plan, const int* quota
                           int* rc) {
     *rc = DS_OK;
     if (cudaMemsetAsync(w.total, 0, 16, st) != cudaSuccess) { *rc = check_launch("split_soup_count"); return -1; }
-    if (M > 0)
-        split_count_kernel<<<blocks_for(M, kSplitThreads), kSplitThreads, 0, st>>>(P, plan, M, verts, faces, valid,
-                                                                                    quota, w.counts, w.probe_status,
-                                                                                    w.total);
+    if (M > 0) {
+        split_top_kernel<false><<<blocks_for(M, kSplitThreads), kSplitThreads, 0, st>>>(
+            P, nullptr, plan, 0, M, verts, faces, valid, quota, w.table, w.top_count, nullptr, nullptr, nullptr,
+            nullptr, nullptr, w.probe_status, w.total);
+        split_task_kernel<false><<<blocks_for((int64_t)M * kTopNodes, kSplitThreads), kSplitThreads, 0, st>>>(
+            P, nullptr, plan, 0, M, verts, faces, w.table, w.top_count, w.task_counts, nullptr, nullptr, nullptr,
+            nullptr, nullptr, nullptr, w.probe_status, w.total);
+        if ((*rc = device_scan<int, int>(w.task_counts, (int64_t)M * kTopNodes, w.task_scan, true, w.scan_tasks, st)))
+            return -1;
+        split_family_kernel<<<blocks_for(M, kSplitThreads), kSplitThreads, 0, st>>>(M, w.top_count, w.task_scan,
+                                                                                     w.counts, w.probe_status);
+    }
     int64_t* total_dev = nullptr;
     if ((*rc = device_scan<int, int64_t>(w.counts, M, offsets, false, w.scan, st, &total_dev))) return -1;
     int64_t total = 0;
@@ -493,7 +649,12 @@ int ds_split_soup_count(int mode, const float* mvp_host, float aspect_wh, float 
     if (total == 0) {
         // nothing to split: zero offsets
         plan = SplitPlan{INFINITY, 0.f};
-        if (M > 0) DS_CUDA(cudaMemsetAsync(w.counts, 0, (size_t)M * sizeof(int), st));
+        if (M > 0) {
+            DS_CUDA(cudaMemsetAsync(w.counts, 0, (size_t)M * sizeof(int), st));
+            DS_CUDA(cudaMemsetAsync(w.table, 0xff, (size_t)M * kTopNodes * sizeof(short), st));  // every entry -1
+            DS_CUDA(cudaMemsetAsync(w.top_count, 0, (size_t)M * sizeof(int), st));
+            DS_CUDA(cudaMemsetAsync(w.task_scan, 0, (size_t)M * kTopNodes * sizeof(int), st));
+        }
         if ((rc = device_scan<int, int64_t>(w.counts, M, split_offsets, false, w.scan, st))) return rc;
         DS_CUDA(cudaMemsetAsync(split_offsets + M, 0, sizeof(int64_t), st));
         total = 0;
@@ -529,9 +690,14 @@ int ds_split_soup_emit(int mode, const float* mvp_host, float aspect_wh, int N, 
         copy_floats_kernel<<<b < cap ? b : cap, kThreads, 0, st>>>((int64_t)N * 3,
                                                                                                    verts, out_verts);
     }
-    if (M > 0)
-        split_emit_kernel<<<blocks_for(M, kSplitThreads), kSplitThreads, 0, st>>>(
-            P, w.plan, N, M, verts, faces, w.quota, split_offsets, out_verts, out_faces, out_map, out_flag, status);
+    if (M > 0) {
+        split_top_kernel<true><<<blocks_for(M, kSplitThreads), kSplitThreads, 0, st>>>(
+            P, w.plan, SplitPlan{}, N, M, verts, faces, nullptr, w.quota, w.table, w.top_count, split_offsets,
+            out_verts, out_faces, out_map, out_flag, status, nullptr);
+        split_task_kernel<true><<<blocks_for((int64_t)M * kTopNodes, kSplitThreads), kSplitThreads, 0, st>>>(
+            P, w.plan, SplitPlan{}, N, M, verts, faces, w.table, w.top_count, nullptr, w.task_scan, split_offsets,
+            out_verts, out_faces, out_map, out_flag, status, nullptr);
+    }
     return check_launch("split_soup_emit");
 }
 

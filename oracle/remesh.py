@@ -5,8 +5,9 @@
   oracle/_ref/libremesh_ref.so by oracle/Makefile, wrapper oracle/ref_remesh.cpp).
 * `restated_split` restates them in numpy single precision (every operation
   rounded, no fused multiply-add, as the reference's host build computes) with
-  the output numbering of the GPU remesher: per input face, its split tree
-  walked depth first.  It is pinned to the reference through
+  the output numbering of the GPU remesher: per input face, the top TOP_LEVELS
+  levels of its split tree breadth first (left to right, first child before
+  second), then the subtrees below them left to right, each depth first.  It is pinned to the reference through
   `families`, which compares the two as sets of triangles per input face.
 """
 
@@ -119,6 +120,9 @@ def _split_point(mode, m, A, B):
     return [f32(f32(tA * A[k]) + f32(tB * B[k])) for k in range(3)]
 
 
+TOP_LEVELS = 5  # split levels of a family numbered breadth first (csrc/remesh.cu kTopLevels)
+
+
 def restated_split(verts, faces, tau: float, mvp=None, valid=None, aspect_wh: float = 1.0):
     """Threshold mode (num_splits = -1) of either remesher, numbered per input
     face depth first: (verts, faces, face_mapping, face_flags)."""
@@ -136,32 +140,47 @@ def restated_split(verts, faces, tau: float, mvp=None, valid=None, aspect_wh: fl
         ids = [int(x) for x in fc[face]]
         P = [v[i].copy() for i in ids]
         splittable = tau > 0 and (mode == 0 or valid is None or int(valid[face]) > 0)
-        stack = []
-        cur = (face, ids, P)
-        new_verts, fam_leaves, k = [], [], 0
-        while True:
-            slot, cid, cp = cur
+        new_verts, fam_leaves = [], []
+
+        def split(node):
+            """The node's children (first, second) if it splits, else None (a leaf)."""
+            slot, cid, cp = node
             e, best = -1, f32(0)
             if splittable:
                 for q in range(3):
                     l2 = _len2(mode, m, aspect, cp[q], cp[(q + 1) % 3])
                     if (mode == 0 or l2 > 0) and (e < 0 or l2 > best):
                         e, best = q, l2
-            if e >= 0 and best >= tau2 and best > 0:
-                ia, ib, ic = e, (e + 1) % 3, (e + 2) % 3
-                Cp = np.array(_split_point(mode, m, cp[ia], cp[ib]), np.float32)
-                new_verts += [Cp, Cp, cp[ic].copy()]
-                mA = -(3 * k + 1)  # placeholders, resolved once the family's offset is known
-                second = (("new", k), [mA - 1, cid[ib], cid[ic]], [Cp, cp[ib], cp[ic]])
-                first = (slot, [cid[ia], mA, mA - 2], [cp[ia], Cp, cp[ic]])
-                k += 1
-                stack.append(second)
-                cur = first
-                continue
-            fam_leaves.append((slot, cid))
-            if not stack:
-                break
-            cur = stack.pop()
+            if not (e >= 0 and best >= tau2 and best > 0):
+                fam_leaves.append((slot, cid))
+                return None
+            k = len(new_verts) // 3
+            ia, ib, ic = e, (e + 1) % 3, (e + 2) % 3
+            Cp = np.array(_split_point(mode, m, cp[ia], cp[ib]), np.float32)
+            new_verts.extend([Cp, Cp, cp[ic].copy()])
+            mA = -(3 * k + 1)  # placeholders, resolved once the family's offset is known
+            second = (("new", k), [mA - 1, cid[ib], cid[ic]], [Cp, cp[ib], cp[ic]])
+            first = (slot, [cid[ia], mA, mA - 2], [cp[ia], Cp, cp[ic]])
+            return first, second
+
+        front = [(face, ids, P)]
+        for _ in range(TOP_LEVELS):  # top levels breadth first
+            nxt = []
+            for node in front:
+                ch = split(node)
+                if ch is not None:
+                    nxt.extend(ch)
+            front = nxt
+        for root in front:  # then each subtree depth first, left to right
+            stack = [root]
+            while stack:
+                cur = stack.pop()
+                while True:
+                    ch = split(cur)
+                    if ch is None:
+                        break
+                    stack.append(ch[1])
+                    cur = ch[0]
         fam_splits.append(new_verts)
         leaves.append(fam_leaves)
     counts = np.array([len(nv) // 3 for nv in fam_splits], np.int64)
