@@ -60,7 +60,7 @@ PRECISION_TEXT = {
     "bf16": "bf16: BF16 features and MLP operands on the tensor cores, FP32 accumulation; feature and MLP gradients "
             "up to ~1.6e-2 / ~5e-3 from the FP64 oracle (the rounding of the BF16 inputs)",
 }
-N_INPUT_SETS = 4  # rotating view batches: 4 x 61 MB of targets, larger than the 126 MB L2
+N_INPUT_SETS = 10  # rotating view batches: 10 x 15.4 MB of 8-bit targets, larger than the 126 MB L2
 
 
 def parse():
@@ -163,7 +163,8 @@ def bench_config(world: int, nviews: int = 8) -> dict:
     return {"workload": WORKLOAD if nviews == 8 else WORKLOAD.replace("8 views", f"{nviews} views"),
             "views_per_step": nviews, "triangles": 15000, "resolution": "800x800",
             "parallelism": f"replicas x{world}",
-            "l2": f"{N_INPUT_SETS} rotating input sets (4 x 61 MB targets) larger than L2"}
+            "targets": "8-bit images (value / 255), as the reference's datasets",
+            "l2": f"{N_INPUT_SETS} rotating input sets ({N_INPUT_SETS} x 15.4 MB of targets) larger than L2"}
 
 
 def make_inputs(rank: int, nviews: int = 8, scenes=None):
@@ -183,9 +184,15 @@ def make_inputs(rank: int, nviews: int = 8, scenes=None):
             views.append(scenes._make_view(eye, 800, 800))
         mvp = np.stack([v.mvp for v in views]).astype(np.float32)
         inv = np.stack([v.inv_mvp for v in views]).astype(np.float32)
-        tgt = rng.uniform(0, 1, size=(nviews * 800 * 800, 3)).astype(np.float32)
+        # U[0,1] targets as 8-bit images (value / 255)
+        tgt = rng.integers(0, 256, size=(nviews * 800 * 800, 3), dtype=np.uint8)
         sets.append((mvp, inv, tgt))
     return sc, mlp, sets
+
+
+def target_f32(u8: np.ndarray) -> np.ndarray:
+    """An 8-bit target as the fp32 values the step reads (value / 255, correctly rounded)."""
+    return u8.astype(np.float32) / np.float32(255)
 
 
 def mlp_flat(mlp):
@@ -212,7 +219,7 @@ def run_reference(args):
         b = i % 8
         inp = P.StepInputs(verts=sc.verts, tri=sc.tri, mvps=mvp[b:b + 1], inv_mvps=inv[b:b + 1], hw=[(800, 800)],
                            feat_src=sc.feat_src, alpha_src=sc.alpha_src[..., 0], mlp=mlp,
-                           targets=[tgt.reshape(8, 800, 800, 3)[b]], min_level=sc.min_level,
+                           targets=[target_f32(tgt).reshape(8, 800, 800, 3)[b]], min_level=sc.min_level,
                            max_level=sc.max_level, stochastic=True, seed=7, iteration=i)
         P.train_step(inp, "f32")
 
@@ -283,7 +290,7 @@ def run_ours(args):
     params = t(mlp_flat(mlp))
     dsets = [(t(m), t(i), t(g)) for m, i, g in sets]
     step = TrainStep(T, V, hw, sc.feat_dim, sc.min_level, sc.max_level, sc.hidden_dim, sc.n_layers,
-                     stochastic=True, seed=1234 + rank, device=dev, precision=args.precision)
+                     stochastic=True, seed=1234 + rank, device=dev, precision=args.precision, target_u8=True)
 
     def kw(s):
         return dict(verts=verts, tri=tri, mvp=s[0], inv_mvp=s[1], feat_src=feat_src, alpha_src=alpha_src,
@@ -424,7 +431,7 @@ def run_ours(args):
     if rank == 0 and args.side:
         other = "bf16" if args.precision == "split" else "split"
         ostep = TrainStep(T, V, hw, sc.feat_dim, sc.min_level, sc.max_level, sc.hidden_dim, sc.n_layers,
-                          stochastic=True, seed=1234 + rank, device=dev, precision=other)
+                          stochastic=True, seed=1234 + rank, device=dev, precision=other, target_u8=True)
         ostep.capacity = step.capacity
         ostep.cfg.frag_records = step.cfg.frag_records
         ostep.cfg.block_shape = step.cfg.block_shape
@@ -696,7 +703,7 @@ def run_plain(sc, mlp, s, dev, n_views: int):
             lin.weight.copy_(t(W))
             lin.bias.copy_(t(b))
     mvps, invs = t(mvp), t(inv)
-    tg = t(tgt.reshape(-1, 800, 800, 3))
+    tg = t(target_f32(tgt).reshape(-1, 800, 800, 3))
     lo, hi = sc.min_level, sc.max_level
 
     def one(b):
@@ -869,7 +876,7 @@ def run_cpu_baseline(sc, mlp, s):
         b = n % 8
         inp = P.StepInputs(verts=sc.verts, tri=sc.tri, mvps=mvp[b:b + 1], inv_mvps=inv[b:b + 1], hw=[(800, 800)],
                            feat_src=sc.feat_src, alpha_src=sc.alpha_src[..., 0], mlp=mlp,
-                           targets=[tgt.reshape(-1, 800, 800, 3)[b]], min_level=sc.min_level, max_level=sc.max_level,
+                           targets=[target_f32(tgt).reshape(-1, 800, 800, 3)[b]], min_level=sc.min_level, max_level=sc.max_level,
                            stochastic=True, seed=7, iteration=n)
         P.train_step(inp, "f32")
         n += 1

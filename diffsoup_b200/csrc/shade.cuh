@@ -96,7 +96,8 @@ struct ShadeArgs {
     const float* feat_f32;        // [T,S,C] the same in fp32 (read by the SPLIT kernels)
     int level, S;
     const float* inv_mvp;         // [B,16]
-    const float* target;          // [P,3]
+    const float* target;          // [P,3] fp32, or
+    const uint8_t* target_u8;     // [P,3] 8-bit, value / 255 (used when non-null)
     const float* params;          // packed fp32 MLP parameters
     float inv_n;                  // 1 / (P * 3)
     float* color;                 // [P,3]
@@ -137,6 +138,13 @@ __device__ __forceinline__ void mma_planes(float acc[4], const uint32_t a[K::NS]
         mma_16816(acc, a[0], b[K::NS - 1]);
         mma_16816(acc, a[K::NS - 1], b[0]);
     }
+}
+
+// Target channel c of pixel p: fp32, or an 8-bit value / 255 (correctly
+// rounded, so that an fp32 target holding the same quotient gives the same
+// step).
+__device__ __forceinline__ float target_at(const ShadeArgs& a, int64_t p, int c) {
+    return a.target_u8 ? __fdiv_rn((float)a.target_u8[p * 3 + c], 255.f) : a.target[p * 3 + c];
 }
 
 // Relu mask of an activation element stored as bf16 in smem.
@@ -269,7 +277,7 @@ __global__ void __launch_bounds__(K::WARPS * 32, K::REG_GRADS ? DSB_SHADE_MIN_CT
                 float l1 = 0.f;
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
-                    const float diff = 1.f - a.target[p * 3 + c];
+                    const float diff = 1.f - target_at(a, p, c);
                     loss_acc += diff * diff;
                     a.color[p * 3 + c] = 1.f;
                     a.grad_color[p * 3 + c] = 2.f * diff * a.inv_n;
@@ -383,7 +391,7 @@ __global__ void __launch_bounds__(K::WARPS * 32, K::REG_GRADS ? DSB_SHADE_MIN_CT
             for (int c = 0; c < 3; ++c) {
                 s[c] = 1.f / (1.f + expf(-(ws.scr[lane * K::LDS + c] + sm.bo[c])));
                 col[c] = mask ? (1.f - res) * x[c] + res * s[c] : 1.f;
-                tg[c] = a.target[p * 3 + c];
+                tg[c] = target_at(a, p, c);
                 const float diff = col[c] - tg[c];
                 loss_acc += diff * diff;
                 const float gc = 2.f * diff * a.inv_n;

@@ -228,7 +228,7 @@ __global__ void __launch_bounds__(kShadeRegWarps * 32, K::MIN_CTAS) shade_reg_ke
         float tgt[3] = {0.f, 0.f, 0.f};  // requested here, used after the MLP forward
         if (valid) {
 #pragma unroll
-            for (int c = 0; c < 3; ++c) tgt[c] = a.target[p * 3 + c];
+            for (int c = 0; c < 3; ++c) tgt[c] = target_at(a, p, c);
         }
         const int t = (int)r.w - 1;
         const bool mask = valid && t >= 0;

@@ -717,7 +717,7 @@ int ds_step_mlp_param_count(const ds_step_config* cfg) {
 
 int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_tiles, int64_t num_pixels,
                   const float* verts, const int* tri, const float* mvp, const float* inv_mvp, const float* feat_src,
-                  const float* alpha_src, const float* mlp_params, const float* target, uint64_t* rng,
+                  const float* alpha_src, const float* mlp_params, const void* target, uint64_t* rng,
                   float* loss, float* grad_verts, float* grad_feat_src, float* grad_alpha_src,
                   float* grad_mlp_params, float* rast_out, float* color_out, void* workspace, size_t workspace_bytes,
                   int64_t list_capacity, int* status, ds_stream_t stream) {
@@ -729,6 +729,7 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     DS_CHECK_ARG(c.precision == 0 || c.precision == 1, "train_step: precision must be 0 (bf16) or 1 (split bf16)");
     DS_CHECK_ARG(c.block_shape >= 0 && c.block_shape <= 2, "train_step: block_shape must be 0 (8x4), 1 (16x2) or 2 (4x8)");
     DS_CHECK_ARG(c.view_enc == 0 || c.view_enc == 1, "train_step: view_enc must be 0 (direction) or 1 (SH2)");
+    DS_CHECK_ARG(c.target_u8 == 0 || c.target_u8 == 1, "train_step: target_u8 must be 0 (fp32) or 1 (8-bit)");
     const int shape = shade_shape(c);
     DS_CHECK_ARG(shape != kShadeUnsupported,
                  "train_step: unsupported MLP (C=%d, %s, hidden=%d, layers=%d); built: 8+dir->16->3, "
@@ -802,7 +803,9 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     ShadeArgs a;
     a.B = c.B; a.views = views; a.num_pixels = num_pixels; a.rast = rast; a.feat = w.feat_bf16;
     a.feat_f32 = w.feat_acc;
-    a.level = c.max_level; a.S = ST; a.inv_mvp = inv_mvp; a.target = target; a.params = mlp_params;
+    a.level = c.max_level; a.S = ST; a.inv_mvp = inv_mvp; a.params = mlp_params;
+    a.target = c.target_u8 ? nullptr : reinterpret_cast<const float*>(target);
+    a.target_u8 = c.target_u8 ? reinterpret_cast<const uint8_t*>(target) : nullptr;
     a.inv_n = (float)(1.0 / ((double)num_pixels * 3.0));
     a.color = color_out ? color_out : w.color; a.grad_color = w.grad_color; a.l1 = w.l1;
     a.grad_feat = w.grad_feat_acc; a.grad_params = grad_mlp_params; a.loss_sum = w.loss_sum;

@@ -40,7 +40,8 @@ class StepConfig(C.Structure):
     _fields_ = [("B", C.c_int32), ("T", C.c_int32), ("V", C.c_int32), ("C", C.c_int32), ("min_level", C.c_int32),
                 ("max_level", C.c_int32), ("hidden", C.c_int32), ("n_layers", C.c_int32),
                 ("stochastic", C.c_int32), ("thr_const", C.c_float), ("frag_records", C.c_float),
-                ("precision", C.c_int32), ("block_shape", C.c_int32), ("view_enc", C.c_int32)]
+                ("precision", C.c_int32), ("block_shape", C.c_int32), ("view_enc", C.c_int32),
+                ("target_u8", C.c_int32)]
 
 
 _L = _core.lib
@@ -96,7 +97,8 @@ class TrainStep:
     def __init__(self, T: int, V: int, hw: Sequence[Tuple[int, int]], C_: int, min_level: int, max_level: int,
                  hidden: int, n_layers: int, stochastic: bool = True, seed: int = 0,
                  device: Optional[torch.device] = None, list_capacity: Optional[int] = None,
-                 frag_records: float = 2.0, precision: str = "bf16", view_enc: str = "dir3"):
+                 frag_records: float = 2.0, precision: str = "bf16", view_enc: str = "dir3",
+                 target_u8: bool = False):
         self.device = torch.device(device or "cuda")
         self.hw = [(int(h), int(w)) for h, w in hw]
         self.B = len(self.hw)
@@ -105,12 +107,14 @@ class TrainStep:
         # precision: "bf16" (BF16 operands) or "split" (every MLP operand as bf16 hi + lo, three
         # tensor-core products each; gradients within ~1e-5 of FP64)
         # view_enc: "dir3" (the 3-D view direction) or "sh2" (encode_view_dir_sh2, 9 inputs)
+        # target_u8: targets are 8-bit images [pixels,3] uint8 (read as value / 255) instead of fp32
         if precision not in ("bf16", "split"):
             raise ValueError(f"precision must be 'bf16' or 'split', not {precision!r}")
         if view_enc not in ("dir3", "sh2"):
             raise ValueError(f"view_enc must be 'dir3' or 'sh2', not {view_enc!r}")
         self.cfg = StepConfig(self.B, T, V, C_, min_level, max_level, hidden, n_layers, int(stochastic), 0.5,
-                              float(frag_records), 1 if precision == "split" else 0, 0, 1 if view_enc == "sh2" else 0)
+                              float(frag_records), 1 if precision == "split" else 0, 0, 1 if view_enc == "sh2" else 0,
+                              int(bool(target_u8)))
         self.views, self.num_tiles, self.num_pixels, self.pix_offsets = _tiles.view_table(self.hw, self.device)
         self.S = sum(_core.feats_at_level(l) for l in range(min_level, max_level + 1))
         self.nparam = int(_L.ds_step_mlp_param_count(C.byref(self.cfg)))
@@ -161,6 +165,9 @@ class TrainStep:
             feat_src: torch.Tensor, alpha_src: torch.Tensor, mlp_params: torch.Tensor, target: torch.Tensor,
             rast_out: Optional[torch.Tensor] = None, color_out: Optional[torch.Tensor] = None) -> torch.Tensor:
         """Enqueue one step on the current stream; returns the device loss."""
+        want = torch.uint8 if self.cfg.target_u8 else torch.float32
+        if target.dtype != want or target.numel() != self.num_pixels * 3 or not target.is_contiguous():
+            raise ValueError(f"target must be a contiguous [{self.num_pixels}, 3] {want} tensor")
         p = _core.ptr
         _core.check(_L.ds_train_step(C.byref(self.cfg), p(self.views), self.num_tiles, self.num_pixels, p(verts),
                                      p(tri), p(mvp), p(inv_mvp), p(feat_src), p(alpha_src), p(mlp_params), p(target),

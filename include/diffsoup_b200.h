@@ -254,6 +254,9 @@ typedef struct {
     /* View encoding appended to the features: 0 = the 3-D view direction
      * (3 inputs), 1 = its SH2 coefficients (9 inputs, encoding.cu:56-118). */
     int32_t view_enc;
+    /* Target images: 0 = fp32 [pixels,3]; 1 = 8-bit [pixels,3] (the
+     * reference's datasets are 8-bit images), read as value / 255. */
+    int32_t target_u8;
 } ds_step_config;
 
 /* Packed MLP parameter layout (fp32): W0[hidden][C+3] b0[hidden]
@@ -287,12 +290,13 @@ int ds_train_step_layout(const ds_step_config* cfg, int num_tiles, int64_t num_p
                          int64_t* offsets);
 
 /* verts [V,3], tri [T,3], mvp/inv_mvp [B,4,4], feat_src [T,S,C],
- * alpha_src [T,S], target [pixels,3] (views packed by ds_view_desc),
+ * alpha_src [T,S], target [pixels,3] fp32 or uint8 (cfg->target_u8; views
+ * packed by ds_view_desc),
  * loss [1]; grad_* match their parameters.  rast_out [pixels,4] and
  * color_out [pixels,3] are optional (NULL: kept in the workspace). */
 int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_tiles, int64_t num_pixels,
                   const float* verts, const int* tri, const float* mvp, const float* inv_mvp, const float* feat_src,
-                  const float* alpha_src, const float* mlp_params, const float* target, uint64_t* rng, float* loss,
+                  const float* alpha_src, const float* mlp_params, const void* target, uint64_t* rng, float* loss,
                   float* grad_verts, float* grad_feat_src, float* grad_alpha_src, float* grad_mlp_params,
                   float* rast_out, float* color_out, void* workspace, size_t workspace_bytes, int64_t list_capacity,
                   int* status, ds_stream_t stream);

@@ -80,13 +80,15 @@ def test_benchmark_workload_full_size(precision):
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(DEV)  # noqa: E731
     kw = dict(verts=t(sc.verts), tri=t(sc.tri), mvp=t(mvp), inv_mvp=t(inv), feat_src=t(sc.feat_src),
               alpha_src=t(sc.alpha_src[..., 0]), mlp_params=t(bench.mlp_flat(mlp)), target=t(tgt))
+    assert tgt.dtype == np.uint8  # the benchmark's 8-bit targets
     seed = 1234
     step = TrainStep(sc.T, sc.verts.shape[0], hw, sc.feat_dim, sc.min_level, sc.max_level, sc.hidden_dim,
-                     sc.n_layers, stochastic=True, seed=seed, device=DEV, precision=precision)
+                     sc.n_layers, stochastic=True, seed=seed, device=DEV, precision=precision, target_u8=True)
     tuned = step.autotune(**kw)
     assert step.record_capacity > 0
     inp = P.StepInputs(verts=sc.verts, tri=sc.tri, mvps=mvp, inv_mvps=inv, hw=hw, feat_src=sc.feat_src,
-                       alpha_src=sc.alpha_src[..., 0], mlp=mlp, targets=list(tgt.reshape(B, 800, 800, 3)),
+                       alpha_src=sc.alpha_src[..., 0], mlp=mlp,
+                       targets=list(bench.target_f32(tgt).reshape(B, 800, 800, 3)),
                        min_level=sc.min_level, max_level=sc.max_level, stochastic=True, seed=seed, iteration=0)
     errs = _check(sc, hw, sc.tri, mvp, step, kw, inp, seed, "none" if precision == "split" else "bf16")
     assert not step.record_fallback()

@@ -141,6 +141,32 @@ def test_train_step_matches_fp64_oracle(config, seed, kw, precision):
         assert errs[k] <= tol, (k, errs[k])
 
 
+def test_eight_bit_targets_equal_their_fp32_quotients():
+    """target_u8: 8-bit targets read as value / 255 give the step that the
+    same quotients in fp32 give (colours bit for bit; loss and gradients up to
+    the order of the floating-point atomics)."""
+    sc, hw, inp, _, d = _setup(2, 4, "split", num_tris=2000, num_views=2, resolution=(96, 112))
+    P_ = sum(h * w for h, w in hw)
+    u8 = np.random.default_rng(5).integers(0, 256, size=(P_, 3), dtype=np.uint8)
+    f32 = u8.astype(np.float32) / np.float32(255)
+    outs = []
+    for is_u8, tgt in ((False, f32), (True, u8)):
+        step = TrainStep(sc.T, sc.verts.shape[0], hw, sc.feat_dim, sc.min_level, sc.max_level, sc.hidden_dim,
+                         sc.n_layers, stochastic=True, seed=4242, precision="split", target_u8=is_u8)
+        color = torch.empty(step.num_pixels, 3, device=DEV)
+        loss = float(step.run(**dict(d, target=torch.from_numpy(tgt).to(DEV)), color_out=color).item())
+        torch.cuda.synchronize()
+        outs.append((loss, color.cpu().numpy(), step.grad_verts.cpu().numpy(), step.grad_feat_src.cpu().numpy(),
+                     step.grad_mlp.cpu().numpy()))
+    (l0, c0, v0, f0, m0), (l1, c1, v1, f1, m1) = outs
+    assert np.array_equal(c0.view(np.uint32), c1.view(np.uint32))
+    assert abs(l0 - l1) <= 1e-6 * l0
+    for a, b in ((v0, v1), (f0, f1), (m0, m1)):
+        assert rel(b, a) < 1e-5
+    with pytest.raises(ValueError):
+        step.run(**dict(d, target=torch.from_numpy(f32).to(DEV)))  # fp32 target given to an 8-bit step
+
+
 def test_train_step_graph_replay():
     sc, hw, inp, step, d = _setup(1, 5, num_tris=1000, num_views=2, resolution=(64, 64))
     step.run(**d)
