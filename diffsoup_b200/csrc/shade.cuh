@@ -57,6 +57,11 @@ struct ShadeCfg {
     // whole kernel (mma accumulators that persist across pixel chunks)
     // instead of adding every chunk's tiles into shared memory.
     static constexpr bool REG_GRADS = NL == 1 && HID * IN_PAD <= 256;
+    // Otherwise the weight gradients are computed per round of WARPS chunks:
+    // every warp owns some of the weight-gradient tiles and sums them over
+    // all the CTA's chunks of the round (no atomics); the dZ_l tiles of a
+    // chunk stay in its warp's two DH buffers, which holds for NL <= 2.
+    static_assert(REG_GRADS || NL <= 2, "distributed weight gradients need NL <= 2");
     static_assert(IN_PAD % 16 == 0 && IN_PAD >= IN_REAL && HID % 16 == 0, "MLP dims");
     static_assert((LDX * 2) % 16 == 0 && (LDH * 2) % 16 == 0 && (LDO * 2) % 16 == 0, "ldmatrix row alignment");
 };
@@ -84,6 +89,7 @@ struct __align__(16) ShadeSmem {
     // fp32 gradient accumulators of this CTA (same packing as the parameters)
     float g[K::NPARAM];
     float loss[K::WARPS];
+    int ran[K::WARPS];  // per warp: its chunk of the current round left MLP tiles in its shared memory
     __align__(16) ShadeWarpSmem<K> w[K::WARPS];
 };
 
@@ -215,8 +221,15 @@ __global__ void __launch_bounds__(K::WARPS * 32, K::REG_GRADS ? DSB_SHADE_MIN_CT
         gbh[i][0] = gbh[i][1] = 0.f;
     }
     const int64_t nchunks = (a.num_pixels + 31) / 32;
-    for (int64_t chunk = (int64_t)blockIdx.x * K::WARPS + warp; chunk < nchunks;
-         chunk += (int64_t)gridDim.x * K::WARPS) {
+    // Every warp runs the same number of rounds (the CTA synchronises once per
+    // round for the weight gradients); a warp whose chunk lies past the end
+    // takes part with no pixels.
+    const int64_t per_round = (int64_t)gridDim.x * K::WARPS;
+    const int64_t rounds = (nchunks + per_round - 1) / per_round;
+    for (int64_t rd = 0; rd < rounds; ++rd) {
+      const int64_t chunk = rd * per_round + (int64_t)blockIdx.x * K::WARPS + warp;
+      bool ran = false;  // this warp's chunk ran the MLP: its tiles in shared memory feed the weight gradients
+      do {  // one chunk; `continue` leaves it
         // ---------------- pixel front: gather features, view direction ----------
         const int64_t p = chunk * 32 + lane;
         const bool valid = p < a.num_pixels;
@@ -432,9 +445,9 @@ __global__ void __launch_bounds__(K::WARPS * 32, K::REG_GRADS ? DSB_SHADE_MIN_CT
         __syncwarp();
 
         // ---------------- MLP backward ------------------------------------------
-        // dWo[o][h] += sum_px dz[px][o] * H_last[px][h]
+        // dWo[o][h] += sum_px dz[px][o] * H_last[px][h]  (REG_GRADS; else per round below)
 #pragma unroll
-        for (int nt = 0; nt < HID / 8; ++nt) {
+        for (int nt = 0; nt < (K::REG_GRADS ? HID / 8 : 0); ++nt) {
             float acc[4] = {0.f, 0.f, 0.f, 0.f};
             float* d = K::REG_GRADS ? gwo[nt < GWO ? nt : 0] : acc;
 #pragma unroll
@@ -506,9 +519,9 @@ __global__ void __launch_bounds__(K::WARPS * 32, K::REG_GRADS ? DSB_SHADE_MIN_CT
             const int ldw = l == 0 ? K::LDX : K::LDH;
             const int pw = l == 0 ? K::P_W0 : K::P_WH + (l - 1) * (HID * HID + HID);
             const int win = l == 0 ? K::IN_REAL : HID;  // row length of the packed W_l
-            // dW_l[h][i] += sum_px dZ_l[px][h] * A_in[px][i]
+            // dW_l[h][i] += sum_px dZ_l[px][h] * A_in[px][i]  (REG_GRADS; else per round below)
 #pragma unroll
-            for (int mh = 0; mh < HID / 16; ++mh) {
+            for (int mh = 0; mh < (K::REG_GRADS ? HID / 16 : 0); ++mh) {
 #pragma unroll
                 for (int ni = 0; ni < nin / 8; ++ni) {
                     float acc[4] = {0.f, 0.f, 0.f, 0.f};
@@ -598,6 +611,77 @@ __global__ void __launch_bounds__(K::WARPS * 32, K::REG_GRADS ? DSB_SHADE_MIN_CT
             }
         }
         __syncwarp();
+        ran = true;
+      } while (false);
+      if (!K::REG_GRADS) {
+        // ---------------- weight gradients of the round's chunks ---------------------
+        // Warp w owns the hidden-row m-tiles mh = w, w + WARPS, ... of every dW_l and
+        // the hidden n-tiles nt = w, w + WARPS, ... of dWo, and sums them over the
+        // chunks of all the CTA's warps that ran the MLP; owned entries of sm.g are
+        // plain read-modify-writes.
+        if (lane == 0) sm.ran[warp] = ran ? 1 : 0;
+        __syncthreads();
+#pragma unroll
+        for (int l = 0; l < K::NL; ++l) {
+            const int buf = (K::NL - 1 - l) & 1;  // the DH buffer that holds dZ_l
+            const int ldin = l == 0 ? K::LDX : K::LDH;
+            const int nin = l == 0 ? IN_PAD : HID;
+            const int pw = l == 0 ? K::P_W0 : K::P_WH + (l - 1) * (HID * HID + HID);
+            const int win = l == 0 ? K::IN_REAL : HID;
+            for (int mh = warp; mh < HID / 16; mh += K::WARPS) {
+#pragma unroll
+                for (int ni = 0; ni < nin / 8; ++ni) {
+                    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+                    for (int src = 0; src < K::WARPS; ++src) {
+                        if (!sm.ran[src]) continue;  // CTA-uniform
+                        const ShadeWarpSmem<K>& os = sm.w[src];
+#pragma unroll
+                        for (int kt = 0; kt < 2; ++kt) {
+                            uint32_t af[K::NS][4], bf[K::NS][2];
+#pragma unroll
+                            for (int s2 = 0; s2 < K::NS; ++s2) {
+                                load_a_t(af[s2], os.DH[buf][s2], K::LDH, kt * 16, mh * 16);
+                                load_b_t(bf[s2], l == 0 ? os.X[s2] : os.H[l > 0 ? l - 1 : 0][s2], ldin, kt * 16,
+                                         ni * 8);
+                            }
+                            mma_planes<K>(acc, af, bf);
+                        }
+                    }
+                    const int i0 = ni * 8 + 2 * q, h0 = mh * 16 + g;
+                    if (i0 < win) {
+                        sm.g[pw + h0 * win + i0] += acc[0];
+                        sm.g[pw + (h0 + 8) * win + i0] += acc[2];
+                    }
+                    if (i0 + 1 < win) {
+                        sm.g[pw + h0 * win + i0 + 1] += acc[1];
+                        sm.g[pw + (h0 + 8) * win + i0 + 1] += acc[3];
+                    }
+                }
+            }
+        }
+        for (int nt = warp; nt < HID / 8; nt += K::WARPS) {
+            float acc[4] = {0.f, 0.f, 0.f, 0.f};
+            for (int src = 0; src < K::WARPS; ++src) {
+                if (!sm.ran[src]) continue;
+                const ShadeWarpSmem<K>& os = sm.w[src];
+#pragma unroll
+                for (int kt = 0; kt < 2; ++kt) {
+                    uint32_t af[K::NS][4], bf[K::NS][2];
+#pragma unroll
+                    for (int s2 = 0; s2 < K::NS; ++s2) {
+                        load_a_t(af[s2], os.DZO[s2], K::LDO, kt * 16, 0);
+                        load_b_t(bf[s2], os.H[K::NL - 1][s2], K::LDH, kt * 16, nt * 8);
+                    }
+                    mma_planes<K>(acc, af, bf);
+                }
+            }
+            if (g < K::OUT) {
+                sm.g[K::P_WO + g * HID + nt * 8 + 2 * q] += acc[0];
+                sm.g[K::P_WO + g * HID + nt * 8 + 2 * q + 1] += acc[1];
+            }
+        }
+        __syncthreads();  // the warps' tiles are rewritten in the next round
+      }
     }
 
     if (K::REG_GRADS) {

@@ -218,7 +218,7 @@ class TrainStep:
         device and workload (`autotune_cache`).  Returns them."""
         key = (torch.cuda.get_device_name(self.device), self.B, tuple(self.hw), self.cfg.T, self.cfg.V, self.cfg.C,
                self.cfg.min_level, self.cfg.max_level, self.cfg.hidden, self.cfg.n_layers, self.cfg.precision,
-               self.cfg.stochastic, self.cfg.view_enc)
+               self.cfg.stochastic, self.cfg.view_enc, self.cfg.target_u8, self.cfg.frag_records > 0)
         it0 = self.rng[1].clone()
         hit = autotune_cache.get(key)
         if hit is not None:

@@ -10,7 +10,13 @@
   * configurations 3 and 5 at their full triangle counts and resolutions on
     a subset of their views (the smallest and the largest view of the 64
     uneven ones of configuration 3; two 1920x1080 views of configuration 5,
-    200,000 triangles, MLP 19-64-64-3): the same checks, split precision.
+    200,000 triangles, MLP 19-64-64-3): the same checks, split precision,
+    except for the vertex gradients.  There the reference's own FP32
+    estimator (the FP32 oracle, run on the same ID buffers) is itself about
+    2e-3 from FP64 on these views: its case decisions (is the neighbour's
+    centre inside the triangle, which edge does the pair cross) flip near
+    edges between FP32 and FP64.  The step's vertex gradients must be within
+    max(1e-3, 1.5 x that error) of FP64, and close to the FP32 oracle.
 
 The oracle (oracle/pipeline.py) restates the reference's kernels
 (rasterize.cu:653-992 for the edge and opacity estimators) and runs the
@@ -37,7 +43,7 @@ def rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
 
 
-def _check(sc_like, hw, tri, mvps, step, kw, inp, seed, mlp_rounding="none"):
+def _check(sc_like, hw, tri, mvps, step, kw, inp, seed, mlp_rounding="none", with_f32=False):
     rast = torch.empty(step.num_pixels, 4, device=DEV)
     color = torch.empty(step.num_pixels, 3, device=DEV)
     step.rng[1] = 0
@@ -60,7 +66,7 @@ def _check(sc_like, hw, tri, mvps, step, kw, inp, seed, mlp_rounding="none"):
     c = color.cpu().numpy()
     sq = [(c[step.pix_offsets[b]:step.pix_offsets[b] + H * W] - ref.color[b].reshape(-1, 3)) ** 2
           for b, (H, W) in enumerate(hw)]
-    return {
+    errs = {
         "loss": abs(loss - ref.loss) / ref.loss,
         "image_rms": float(np.sqrt(np.concatenate(sq).mean())),
         "grad_verts": rel(step.grad_verts.cpu().numpy(), ref.grad_verts),
@@ -69,6 +75,12 @@ def _check(sc_like, hw, tri, mvps, step, kw, inp, seed, mlp_rounding="none"):
         "mlp": rel(step.grad_mlp.cpu().numpy(),
                    np.concatenate([np.concatenate([W.reshape(-1), b]) for W, b in ref.grad_mlp])),
     }
+    if not with_f32:
+        return errs
+    # the reference's FP32 arithmetic on the same ID buffers
+    r32 = P.train_step(inp, "f32", rast_in=rasts, pos32=pos, alpha32=alpha32)
+    return errs, {"f32_vs_f64": rel(r32.grad_verts, ref.grad_verts),
+                  "step_vs_f32": rel(step.grad_verts.cpu().numpy(), r32.grad_verts)}
 
 
 @pytest.mark.parametrize("precision", ["split", "bf16"])
@@ -122,8 +134,13 @@ def test_full_size_subset_gradients(config):
     inp = P.StepInputs(verts=full.verts, tri=full.tri, mvps=mvp, inv_mvps=inv, hw=hw, feat_src=full.feat_src,
                        alpha_src=full.alpha_src[..., 0], mlp=mlp, targets=targets, min_level=full.min_level,
                        max_level=full.max_level, stochastic=True, seed=seed, iteration=0)
-    errs = _check(full, hw, full.tri, mvp, step, kw, inp, seed)
+    errs, ref32 = _check(full, hw, full.tri, mvp, step, kw, inp, seed, with_f32=True)
     print(f"config{config}: views {pick} ({', '.join(f'{w}x{h}' for h, w in hw)}), {full.T} triangles, split "
-          "precision vs FP64 oracle: " + ", ".join(f"{k}={v:.2e}" for k, v in errs.items()))
+          "precision vs FP64 oracle: " + ", ".join(f"{k}={v:.2e}" for k, v in errs.items())
+          + f"; vertex gradients of the FP32 oracle vs FP64 {ref32['f32_vs_f64']:.2e}, step vs FP32 oracle "
+          f"{ref32['step_vs_f32']:.2e}")
     for k, v in errs.items():
-        assert v <= 1e-3, (k, v)
+        if k != "grad_verts":
+            assert v <= 1e-3, (k, v)
+    assert errs["grad_verts"] <= max(1e-3, 1.5 * ref32["f32_vs_f64"]), (errs["grad_verts"], ref32)
+    assert ref32["step_vs_f32"] <= max(1e-3, 1.5 * ref32["f32_vs_f64"]), ref32

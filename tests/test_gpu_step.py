@@ -226,20 +226,20 @@ def test_level_accumulation_matches_oracle(config, kw):
     assert rel(step.grad_feat_src.cpu().numpy(), want_gf) < 1e-5
 
 
-@pytest.mark.parametrize("precision", ["split", "bf16"])
 @pytest.mark.parametrize("config", [1, 5])
-def test_train_step_gradients_match_central_differences(config, precision):
-    """The step's feature and MLP gradients against FP64 central differences
-    (step 1e-4) of the oracle's loss over the step's own ID buffer: relative
-    L2 over the sampled entries within 1e-3 in split precision, within
-    BF16_INPUT_TOL in BF16."""
+def test_train_step_gradients_match_central_differences(config):
+    """The split-precision step's feature and MLP gradients against FP64
+    central differences (step 1e-4) of the oracle's loss over the step's own
+    ID buffer: relative L2 over the sampled entries within 1e-3.  (BF16
+    precision is pinned by the BF16-rounding oracle above: the rounding of its
+    operands alone puts it 5e-3..2e-2 from the exact gradients.)"""
     from test_fd_gradients import fd_feature, fd_mlp, fd_scene, feature_entries
 
     sc, inp, _ = fd_scene(2, config)
     hw = list(inp.hw)
     step = TrainStep(sc.T, sc.verts.shape[0], hw, sc.feat_dim, sc.min_level, sc.max_level, sc.hidden_dim,
-                     sc.n_layers, stochastic=True, seed=inp.seed, precision=precision)
-    tol = SPLIT_TOL if precision == "split" else BF16_INPUT_TOL
+                     sc.n_layers, stochastic=True, seed=inp.seed, precision="split")
+    tol = SPLIT_TOL
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(DEV)  # noqa: E731
     mlp32 = [(W.astype(np.float32), b.astype(np.float32)) for W, b in inp.mlp]
     rast = torch.empty(step.num_pixels, 4, device=DEV)
@@ -256,7 +256,9 @@ def test_train_step_gradients_match_central_differences(config, precision):
     for idx in feature_entries(gf, 12, rng):
         got.append(gf[idx])
         want.append(fd_feature(inp, rasts, idx))
-    assert rel(got, want) <= tol["grad_feat_src"], (got, want)
+    r = rel(got, want)
+    print(f"config{config} split feature gradients vs FP64 central differences: {r:.2e}")
+    assert r <= tol["grad_feat_src"], (r, got, want)
     # MLP parameters, packed as [W0, b0, (W, b)..., Wo, bo] like the step's grad_mlp
     got, want, off = [], [], 0
     for layer, (W, b) in enumerate(inp.mlp):
@@ -266,7 +268,9 @@ def test_train_step_gradients_match_central_differences(config, precision):
                 got.append(g[idx])
                 want.append(fd_mlp(inp, rasts, layer, which, idx))
             off += arr.size
-    assert rel(got, want) <= tol["mlp"], (got, want)
+    r = rel(got, want)
+    print(f"config{config} split MLP gradients vs FP64 central differences: {r:.2e}")
+    assert r <= tol["mlp"], (r, got, want)
 
 
 def test_block_shapes_give_identical_results_and_autotune_picks_one():
