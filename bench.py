@@ -245,12 +245,14 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
-def algorithmic_bytes(phase: str, P_: int, B: int, T: int, V: int, ST: int, C_: int, feat_bytes: int = 2) -> float:
+def algorithmic_bytes(phase: str, P_: int, B: int, T: int, V: int, ST: int, C_: int, feat_bytes: int = 2,
+                      target_bytes: int = 12) -> float:
     """Minimal DRAM bytes of one launch of each step kernel: what the kernel must read and write
     once (per-pixel buffers, per-(view, triangle) records, lattice samples), no re-reads.  feat_bytes:
-    2 when the shading kernel gathers BF16 features, 4 for FP32 (split precision)."""
-    if phase == "shade":  # rast 16 R, target 12 R, colour 12 W, dL/dcolour 12 W, |c-t| 4 W; features + fp32 grads
-        return P_ * 56.0 + T * ST * C_ * (feat_bytes + 8)
+    2 when the shading kernel gathers BF16 features, 4 for FP32 (split precision); target_bytes: 12 per
+    pixel for fp32 targets, 3 for 8-bit ones."""
+    if phase == "shade":  # rast 16 R, target R, colour 12 W, dL/dcolour 12 W, |c-t| 4 W; features + fp32 grads
+        return P_ * (44.0 + target_bytes) + T * ST * C_ * (feat_bytes + 8)
     # fragment records: 16 B each, about one per pixel on this workload (fragments in front of the surface)
     if phase == "raster":  # rast 16 W + records 16 W per pixel; triangle records 64 B per (view, tri); opacities
         return P_ * 32.0 + B * T * 64.0 + T * ST * 4.0
@@ -265,12 +267,13 @@ def algorithmic_bytes(phase: str, P_: int, B: int, T: int, V: int, ST: int, C_: 
     return 0.0
 
 
-def step_algorithmic_bytes(B: int, T: int, V: int, S: int, C_: int, P_: int) -> float:
+def step_algorithmic_bytes(B: int, T: int, V: int, S: int, C_: int, P_: int, target_bytes: int = 12) -> float:
     """Minimal DRAM bytes of a whole training step: 12 B per triangle, features and opacities read and
     their gradients written (8 B per lattice sample and channel, C + 1 channels), and per view the clip
     positions read and their gradients written (32 B per vertex) plus, per pixel, the ID buffer written
-    (16 B), the colour written (12 B), the target read (12 B) and dL/dcolour read (12 B)."""
-    return 12.0 * T + 8.0 * T * S * (C_ + 1) + B * 32.0 * V + P_ * (16.0 + 12.0 + 12.0 + 12.0)
+    (16 B), the colour written (12 B), the target read (12 B, or 3 B for 8-bit targets) and dL/dcolour read
+    (12 B)."""
+    return 12.0 * T + 8.0 * T * S * (C_ + 1) + B * 32.0 * V + P_ * (16.0 + 12.0 + target_bytes + 12.0)
 
 
 def run_ours(args):
@@ -414,7 +417,7 @@ def run_ours(args):
     dom = max(["raster", "shade", "aux", "edge"], key=lambda n: phase_ms[n])
     ST = _core.feats_at_level(sc.max_level)
     P_ = step.num_pixels
-    alg = algorithmic_bytes(dom, P_, B, T, V, ST, sc.feat_dim, 4 if args.precision == "split" else 2)
+    alg = algorithmic_bytes(dom, P_, B, T, V, ST, sc.feat_dim, 4 if args.precision == "split" else 2, 3)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -423,7 +426,7 @@ def run_ours(args):
     peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
     achieved = alg / (phase_ms[dom] / 1000.0) / 1e9
-    step_bytes = step_algorithmic_bytes(B, T, V, _core.total_feats(sc.min_level, sc.max_level), sc.feat_dim, P_)
+    step_bytes = step_algorithmic_bytes(B, T, V, _core.total_feats(sc.min_level, sc.max_level), sc.feat_dim, P_, 3)
     traffic = read_traffic(dom)
 
     # ---------------- the headline workload in the other precision -------------
