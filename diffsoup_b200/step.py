@@ -41,7 +41,7 @@ class StepConfig(C.Structure):
                 ("max_level", C.c_int32), ("hidden", C.c_int32), ("n_layers", C.c_int32),
                 ("stochastic", C.c_int32), ("thr_const", C.c_float), ("frag_records", C.c_float),
                 ("precision", C.c_int32), ("block_shape", C.c_int32), ("view_enc", C.c_int32),
-                ("target_u8", C.c_int32)]
+                ("target_u8", C.c_int32), ("raster_mode", C.c_int32)]
 
 
 _L = _core.lib
@@ -114,7 +114,7 @@ class TrainStep:
             raise ValueError(f"view_enc must be 'dir3' or 'sh2', not {view_enc!r}")
         self.cfg = StepConfig(self.B, T, V, C_, min_level, max_level, hidden, n_layers, int(stochastic), 0.5,
                               float(frag_records), 1 if precision == "split" else 0, 0, 1 if view_enc == "sh2" else 0,
-                              int(bool(target_u8)))
+                              int(bool(target_u8)), 1)
         self.views, self.num_tiles, self.num_pixels, self.pix_offsets = _tiles.view_table(self.hw, self.device)
         self.S = sum(_core.feats_at_level(l) for l in range(min_level, max_level + 1))
         self.nparam = int(_L.ds_step_mlp_param_count(C.byref(self.cfg)))
@@ -200,8 +200,10 @@ class TrainStep:
         raise RuntimeError("tile list capacity did not converge")
 
     BLOCK_SHAPES = {0: "8x4", 1: "16x2", 2: "4x8"}
+    RASTER_MODES = {0: "walk", 1: "pairs"}
 
-    def autotune(self, *args, steps: int = 5, shapes: Sequence[int] = (0, 1, 2), **kwargs) -> Dict[str, object]:
+    def autotune(self, *args, steps: int = 5, shapes: Sequence[int] = (0, 1, 2), modes: Sequence[int] = (0, 1),
+                 **kwargs) -> Dict[str, object]:
         """Chooses the launch layout of this step for its inputs (the step's own
         autotuner, run eagerly before training and before any capture):
 
@@ -210,8 +212,11 @@ class TrainStep:
           * the fragment-record store, sized to the records a step reserves
             plus a quarter, so that no block is re-enumerated;
           * the pixel block of a rasterizer warp (8x4, 16x2 or 4x8 pixels of a
-            16x16 tile, 8 warps per tile): each is timed with CUDA events over
-            `steps` eager steps after a warm-up, and the fastest kept.
+            16x16 tile, 8 warps per tile) and the rasterizer's work layout
+            (walk: one candidate triangle at a time; pairs: queued (triangle,
+            pixel) pairs, 32 per instruction): each combination is timed with
+            CUDA events over `steps` eager steps after a warm-up, and the
+            fastest kept.
 
         Results do not depend on the choices.  The RNG iteration is restored,
         so tuning does not advance the training state.  Choices are cached per
@@ -225,6 +230,7 @@ class TrainStep:
             self.capacity = max(self.capacity, hit["list_capacity"])
             self.cfg.frag_records = hit["frag_records"]
             self.cfg.block_shape = hit["block_shape"]
+            self.cfg.raster_mode = hit["raster_mode"]
             self._alloc()
             return dict(hit)
         self.fit_capacity(*args, **kwargs)
@@ -236,8 +242,10 @@ class TrainStep:
             self.cfg.frag_records = float(min(max(1.25 * need, 0.5), 16.0))
             self._alloc()
         times = {}
-        for shape in shapes:
-            self.cfg.block_shape = int(shape)
+        combos = [(int(sh), int(md)) for md in modes for sh in shapes]
+        name = lambda c: f"{self.BLOCK_SHAPES[c[0]]}/{self.RASTER_MODES[c[1]]}"  # noqa: E731
+        for combo in combos:
+            self.cfg.block_shape, self.cfg.raster_mode = combo
             for _ in range(2):
                 self.run(*args, **kwargs)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -246,13 +254,14 @@ class TrainStep:
                 self.run(*args, **kwargs)
             e1.record()
             torch.cuda.synchronize()
-            times[self.BLOCK_SHAPES[int(shape)]] = e0.elapsed_time(e1) / steps
-        best = min(shapes, key=lambda sh: times[self.BLOCK_SHAPES[int(sh)]])
-        self.cfg.block_shape = int(best)
+            times[name(combo)] = e0.elapsed_time(e1) / steps
+        best = min(combos, key=lambda c: times[name(c)])
+        self.cfg.block_shape, self.cfg.raster_mode = best
         self.rng[1].copy_(it0)
         self.status.zero_()
         out = {"list_capacity": int(self.capacity), "frag_records": float(self.cfg.frag_records),
-               "block_shape": int(best), "block": self.BLOCK_SHAPES[int(best)], "ms_per_step": times}
+               "block_shape": best[0], "block": self.BLOCK_SHAPES[best[0]], "raster_mode": best[1],
+               "raster": self.RASTER_MODES[best[1]], "ms_per_step": times}
         autotune_cache[key] = dict(out)
         return out
 

@@ -257,6 +257,11 @@ typedef struct {
     /* Target images: 0 = fp32 [pixels,3]; 1 = 8-bit [pixels,3] (the
      * reference's datasets are 8-bit images), read as value / 255. */
     int32_t target_u8;
+    /* Rasterizer work layout (same results; TrainStep.autotune times them):
+     * 0 = each warp walks its pixel block's candidate triangles one at a
+     * time; 1 = the per-pixel work of each group of 32 candidates as a queue
+     * of (triangle, pixel) pairs dealt out 32 per warp instruction. */
+    int32_t raster_mode;
 } ds_step_config;
 
 /* Packed MLP parameter layout (fp32): W0[hidden][C+3] b0[hidden]
