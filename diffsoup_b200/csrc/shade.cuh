@@ -112,6 +112,7 @@ struct ShadeArgs {
     float* grad_feat;             // [T,S,C] fp32, accumulates
     float* grad_params;           // packed, accumulates
     double* loss_sum;             // [1], accumulates sum of squared errors
+    int* status;                  // step status bits (DS_STATUS_*), may be null
 };
 
 // bf16 planes of two values: hi = bf16(v), lo = bf16(v - hi).

@@ -17,6 +17,7 @@
 #include "edge_math.cuh"
 #include "shade.cuh"
 #include "shade_reg.cuh"
+#include "shade_tc.cuh"
 #include "tiled.cuh"
 
 namespace dsb {
@@ -507,6 +508,23 @@ static int launch_shade_reg(const ShadeArgs& a, cudaStream_t st) {
     return check_launch("shade_reg");
 }
 
+// The tcgen05 kernel of the wide BF16 MLP: persistent over 128-pixel tiles.
+static int launch_shade_tc(const ShadeArgs& a, cudaStream_t st) {
+    const size_t smem = sizeof(TcSmem);
+    static int per_sm = 0;  // set on the first (eager) call, before any graph capture
+    if (per_sm == 0) {
+        DS_CUDA(cudaFuncSetAttribute(shade_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        DS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, shade_tc_kernel, kTcThreads, smem));
+        if (per_sm <= 0) return set_error(DS_ERR_CUDA, "shade_tc: kernel does not fit on an SM");
+        if (per_sm > 2) per_sm = 2;  // 256 TMEM columns per CTA: two CTAs fill an SM's 512
+    }
+    const int64_t tiles = (a.num_pixels + kTcThreads - 1) / kTcThreads;
+    const int64_t cap = (int64_t)sm_count() * per_sm;
+    const unsigned grid = (unsigned)(tiles < 1 ? 1 : (tiles < cap ? tiles : cap));
+    shade_tc_kernel<<<grid, kTcThreads, smem, st>>>(a);
+    return check_launch("shade_tc");
+}
+
 static inline size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
 
 // Optional phase events (profiling): recorded on the step's stream at the
@@ -731,6 +749,7 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     DS_CHECK_ARG(c.view_enc == 0 || c.view_enc == 1, "train_step: view_enc must be 0 (direction) or 1 (SH2)");
     DS_CHECK_ARG(c.target_u8 == 0 || c.target_u8 == 1, "train_step: target_u8 must be 0 (fp32) or 1 (8-bit)");
     DS_CHECK_ARG(c.raster_mode == 0 || c.raster_mode == 1, "train_step: raster_mode must be 0 (walk) or 1 (pairs)");
+    DS_CHECK_ARG(c.shade_mode == 0 || c.shade_mode == 1, "train_step: shade_mode must be 0 (mma.sync) or 1 (tcgen05)");
     const int shape = shade_shape(c);
     DS_CHECK_ARG(shape != kShadeUnsupported,
                  "train_step: unsupported MLP (C=%d, %s, hidden=%d, layers=%d); built: 8+dir->16->3, "
@@ -809,7 +828,7 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     a.target_u8 = c.target_u8 ? reinterpret_cast<const uint8_t*>(target) : nullptr;
     a.inv_n = (float)(1.0 / ((double)num_pixels * 3.0));
     a.color = color_out ? color_out : w.color; a.grad_color = w.grad_color; a.l1 = w.l1;
-    a.grad_feat = w.grad_feat_acc; a.grad_params = grad_mlp_params; a.loss_sum = w.loss_sum;
+    a.grad_feat = w.grad_feat_acc; a.grad_params = grad_mlp_params; a.loss_sum = w.loss_sum; a.status = status;
     const bool split = c.precision == 1;
     switch (shape) {
         case kShadeC8Dir16:
@@ -819,7 +838,8 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
             rc = split ? launch_shade_reg<ShadeC7Sh2_16x2Split>(a, st) : launch_shade_reg<ShadeC7Sh2_16x2>(a, st);
             break;
         default:
-            rc = split ? launch_shade<ShadeC16H64Split>(a, st) : launch_shade<ShadeC16H64>(a, st);
+            if (split) rc = launch_shade<ShadeC16H64Split>(a, st);
+            else rc = c.shade_mode == 1 ? launch_shade_tc(a, st) : launch_shade<ShadeC16H64>(a, st);
     }
     if (rc || (rc = mark(4, st))) return rc;
 

@@ -43,6 +43,8 @@ enum {
     DS_STATUS_LIST_OVERFLOW = 1, /* tile lists exceeded capacity; affected tiles ran the exhaustive path */
     DS_STATUS_RECORD_FALLBACK = 2, /* some blocks' fragment records did not fit; they were re-enumerated */
     DS_STATUS_SPLIT_LIMIT = 4, /* ds_split_soup_count: a face's split tree exceeded its limits (see there) */
+    DS_STATUS_MMA_TIMEOUT = 8, /* a tensor-core stage of the training step's shading did not complete within its
+                                  bounded wait; the step's outputs are not valid */
 };
 
 const char* ds_last_error(void);
@@ -262,6 +264,12 @@ typedef struct {
      * time; 1 = the per-pixel work of each group of 32 candidates as a queue
      * of (triangle, pixel) pairs dealt out 32 per warp instruction. */
     int32_t raster_mode;
+    /* Shading kernel of the 16 + direction -> 64 -> 64 -> 3 MLP in BF16
+     * precision: 0 = warp-level tensor-core products (mma.sync) with operand
+     * tiles in shared memory; 1 = tcgen05.mma on 128-pixel tiles with the
+     * accumulators (and the weight gradients of the whole launch) in tensor
+     * memory.  Other MLPs and split precision ignore it. */
+    int32_t shade_mode;
 } ds_step_config;
 
 /* Packed MLP parameter layout (fp32): W0[hidden][C+3] b0[hidden]

@@ -141,6 +141,38 @@ def test_train_step_matches_fp64_oracle(config, seed, kw, precision):
         assert errs[k] <= tol, (k, errs[k])
 
 
+@pytest.mark.parametrize("config,seed,kw", [
+    (4, 3, dict(num_tris=800, num_views=2, resolution=(80, 96))),
+    (4, 13, dict(num_tris=1500, num_views=3, resolution=(120, 136))),
+    (5, 0, dict(num_tris=4000, num_views=2, resolution=(90, 160))),
+])
+def test_tcgen05_shading_matches_the_bf16_rounding_oracle(config, seed, kw):
+    """The tcgen05 kernel of the wide BF16 MLP (shade_mode 1: 128-pixel
+    tiles, accumulators and the launch's weight gradients in tensor memory)
+    against the FP64 oracle with the same BF16 operand rounding (every group
+    within 1e-3) and against the mma.sync kernel of the same step."""
+    sc, hw, inp, step, d = _setup(config, seed, "bf16", **kw)
+    assert step.tcgen05_shading()
+    step.cfg.shade_mode = 1
+    loss, c, rasts, pos, alpha32 = _run_and_check_ids(sc, hw, step, d)
+    ref = P.train_step(inp, "f64", rast_in=rasts, pos32=pos, alpha32=alpha32, mlp_rounding="bf16")
+    errs = _errors(step, hw, loss, c, ref)
+    print(f"config{config} tcgen05 shading vs BF16-rounding FP64 oracle: "
+          + ", ".join(f"{k}={v:.2e}" for k, v in errs.items()))
+    assert not (int(step.status.item()) & 8)  # DS_STATUS_MMA_TIMEOUT
+    for k, v in errs.items():
+        assert v <= 1e-3, (k, v)
+    got = {k: getattr(step, k).clone() for k in ("grad_feat_src", "grad_mlp", "grad_verts")}
+    step.cfg.shade_mode = 0
+    step.rng[1] = 0
+    c0 = torch.empty(step.num_pixels, 3, device=DEV)
+    step.run(**d, color_out=c0)
+    torch.cuda.synchronize()
+    assert float(np.abs(c0.cpu().numpy() - c).max()) < 1e-5
+    for k, v in got.items():
+        assert rel(v.cpu().numpy(), getattr(step, k).cpu().numpy()) < 1e-3, k
+
+
 def test_eight_bit_targets_equal_their_fp32_quotients():
     """target_u8: 8-bit targets read as value / 255 give the step that the
     same quotients in fp32 give (colours bit for bit; loss and gradients up to
