@@ -390,11 +390,12 @@ __device__ __forceinline__ EdgePair edge_pair(const EdgeHalo& h, const EdgeFrame
 
 // Edge-gradient estimator of one pixel from the staged tile: the pixel's
 // triangle (or -1) is returned and its clip-space vertex gradients are in
-// acc.g[vertex*4 + xyzw].  Interior and opacity-edge pairs (midpoint
-// contributions) are evaluated in the first pass over the four neighbours;
-// geometric-edge pairs and pairs that may be triangle intersections are
-// only marked there and evaluated in two further passes, where pass k takes
-// each lane's k-th marked pair, so that lanes run the rarer cases together.
+// acc.g[vertex*4 + xyzw].  A first pass over the four neighbours only
+// classifies the pairs; interior and opacity-edge pairs (midpoint
+// contributions), geometric-edge pairs and pairs that may be triangle
+// intersections are then evaluated in three passes, where round k of a pass
+// takes each lane's k-th pair of that kind, so that the lanes of a warp run
+// the same case together.
 // `active` false: the lane has no pixel (it takes part in the warp-wide steps only).
 __device__ __forceinline__ int edge_grad_pixel_staged(const EdgeHalo& h, int hidx, int y0, int x0, int H, int W,
                                                       const TriVerts* __restrict__ tverts, EdgeAccum& acc,
@@ -403,7 +404,7 @@ __device__ __forceinline__ int edge_grad_pixel_staged(const EdgeHalo& h, int hid
     for (int k = 0; k < 12; ++k) acc.g[k] = 0.f;
     acc.any = false;
     const int it0 = active ? h.it[hidx] : -1;
-    unsigned geo = 0u, isect = 0u;  // pairs (bit e) of the second and third passes
+    unsigned mid = 0u, geo = 0u, isect = 0u;  // pairs (bit e) of the midpoint, edge-crossing and intersection passes
     EdgeFrame f;
     // pixel-centre NDC with one reciprocal per axis (this path is compared to
     // the oracle with a tolerance; the 1-ulp difference is far below it)
@@ -438,7 +439,7 @@ __device__ __forceinline__ int edge_grad_pixel_staged(const EdgeHalo& h, int hid
             const EdgePair p = edge_pair(h, f, hidx, e, H, W, sx, sy);
             if (p.gx == 0.f && p.gy == 0.f) continue;  // zero adjoint
             if (interior) {
-                edge_midpoint(f, p.hx, p.hy, 2.f * p.gx, 2.f * p.gy, 0.f, acc);
+                mid |= 1u << e;
                 continue;
             }
             const float depth1 = h.dep[n];
@@ -452,12 +453,23 @@ __device__ __forceinline__ int edge_grad_pixel_staged(const EdgeHalo& h, int hid
                     // behind depth0 at this pixel (never when its far depth bound is in front)
                     if (!(h.zhi[n] < f.depth)) isect |= 1u << e;
                 } else if (it1 < 0 || f.depth < depth1) {  // active opacity edge
-                    edge_midpoint(f, p.hx, p.hy, p.gx, p.gy, 0.f, acc);
+                    mid |= 1u << e;
                 }
             } else if (it1 < 0 || f.depth < depth1) {  // active geometric edge
                 geo |= 1u << e;
             }
         }
+    }
+    // midpoint contributions (interior pairs, counted twice, and opacity edges), in neighbour order;
+    // pass k takes each lane's k-th marked pair, so that the lanes evaluate them together
+    const int nmid = __reduce_max_sync(0xffffffffu, (unsigned)__popc(mid));
+    for (int r = 0; r < nmid; ++r) {
+        if (mid == 0u) continue;
+        const int e = __ffs(mid) - 1;
+        mid &= mid - 1u;
+        const EdgePair p = edge_pair(h, f, hidx, e, H, W, sx, sy);
+        const float m = h.it[p.n] == it0 ? 2.f : 1.f;
+        edge_midpoint(f, p.hx, p.hy, m * p.gx, m * p.gy, 0.f, acc);
     }
     // geometric edges: the exit edge is the first edge function to change sign along p0 -> p1,
     // in the reference's test order (0,1) = k 2, (1,2) = k 0, (2,0) = k 1
