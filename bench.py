@@ -438,7 +438,6 @@ def run_ours(args):
         ostep.capacity = step.capacity
         ostep.cfg.frag_records = step.cfg.frag_records
         ostep.cfg.block_shape = step.cfg.block_shape
-        ostep.cfg.raster_mode = step.cfg.raster_mode
         ostep._alloc()
         og = [ostep.capture(**kw(s)) for s in dsets]
         for i in range(args.warmup):
@@ -488,7 +487,7 @@ def run_ours(args):
         "precision": PRECISION_TEXT[args.precision],
         "config": bench_config(world, B),
         "graph": "one CUDA graph per step", "list_overflow": overflow,
-        "autotuned": {"block": tuned["block"], "raster": tuned["raster"],
+        "autotuned": {"block": tuned["block"], "shade": tuned["shade"],
                       "frag_records_per_px": round(tuned["frag_records"], 3),
                       "list_capacity": tuned["list_capacity"],
                       "ms_per_step_by_layout": {k: round(v, 4) for k, v in tuned["ms_per_step"].items()}},
@@ -629,7 +628,7 @@ def measure_workload(dev, sc, mlp, precision: str, steps: int, warmup: int, peak
            "device_memory_bytes": int(mem), "workspace_bytes": int(step.workspace.numel()),
            "fragment_records": "tile-wise recomputation" if step.record_capacity == 0 else
                                f"stored ({step.cfg.frag_records:.3f} per pixel)",
-           "autotuned": {"block": tuned["block"], "raster": tuned["raster"], "list_capacity": tuned["list_capacity"]},
+           "autotuned": {"block": tuned["block"], "shade": tuned["shade"], "list_capacity": tuned["list_capacity"]},
            "list_overflow": overflow}
     del step, kw
     if cpu_sample:

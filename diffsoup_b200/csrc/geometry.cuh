@@ -90,15 +90,17 @@ __device__ __forceinline__ void edge_terms(float ndc_y, float ndc_x, float4 p0, 
 //    |A2| > 2^-20 (|A| + |A0| + |A1|): from A = rn(rn(A0 + A1) + A2),
 //    (b0 + b1) >= (1 - 2u)(1 + k - 2u - uk - um) with u = 2^-24,
 //    k = -A2/A and m = (|A0| + |A1|)/|A|, which exceeds 1 once k > 16u(1 + m).
+// Written without branches: with s_k = A_k oriented by the sign of A, "A_k
+// nonzero, of the opposite sign and |A_k| > m" is s_k < -m (m >= 0; NaN
+// compares false either way).
 __device__ __forceinline__ bool surely_outside(float A0, float A1, float A2, float A) {
-    if (A == 0.f) return true;
     const float aA = fabsf(A);
-    if (!(aA >= 0x1p-60f && aA <= 0x1p60f)) return false;
     const bool negA = A < 0.f;
-    if (A0 != 0.f && (A0 < 0.f) != negA && fabsf(A0) > aA * 0x1p-100f) return true;
-    if (A1 != 0.f && (A1 < 0.f) != negA && fabsf(A1) > aA * 0x1p-100f) return true;
-    if (A2 != 0.f && (A2 < 0.f) != negA && fabsf(A2) > 0x1p-20f * (aA + fabsf(A0) + fabsf(A1))) return true;
-    return false;
+    const float s0 = negA ? -A0 : A0, s1 = negA ? -A1 : A1, s2 = negA ? -A2 : A2;
+    const float m01 = aA * 0x1p-100f;
+    const float m2 = 0x1p-20f * (aA + fabsf(A0) + fabsf(A1));
+    const bool in_range = aA >= 0x1p-60f && aA <= 0x1p60f;
+    return A == 0.f || (in_range && (s0 < -m01 || s1 < -m01 || s2 < -m2));
 }
 
 // True only when no pixel centre of a block, whose pixel-centre NDC
@@ -321,6 +323,18 @@ __device__ __forceinline__ float interp_scalar(float b0, float b1, uint32_t lo, 
         acc = madd(acc, w[2], __ldg(src + off + idx[2]));
         off += feats_at_level(l);
     }
+    return acc;
+}
+
+// interp_scalar over one level (lo == hi): the same operations without the
+// level loop.
+__device__ __forceinline__ float interp_level(float b0, float b1, uint32_t level, const float* src) {
+    uint32_t idx[3]; float w[3];
+    lattice_cell(b0, b1, level, idx, w);
+    float acc = 0.f;
+    acc = madd(acc, w[0], __ldg(src + idx[0]));
+    acc = madd(acc, w[1], __ldg(src + idx[1]));
+    acc = madd(acc, w[2], __ldg(src + idx[2]));
     return acc;
 }
 

@@ -748,7 +748,6 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     DS_CHECK_ARG(c.block_shape >= 0 && c.block_shape <= 2, "train_step: block_shape must be 0 (8x4), 1 (16x2) or 2 (4x8)");
     DS_CHECK_ARG(c.view_enc == 0 || c.view_enc == 1, "train_step: view_enc must be 0 (direction) or 1 (SH2)");
     DS_CHECK_ARG(c.target_u8 == 0 || c.target_u8 == 1, "train_step: target_u8 must be 0 (fp32) or 1 (8-bit)");
-    DS_CHECK_ARG(c.raster_mode == 0 || c.raster_mode == 1, "train_step: raster_mode must be 0 (walk) or 1 (pairs)");
     DS_CHECK_ARG(c.shade_mode == 0 || c.shade_mode == 1, "train_step: shade_mode must be 0 (mma.sync) or 1 (tcgen05)");
     const int shape = shade_shape(c);
     DS_CHECK_ARG(shape != kShadeUnsupported,
@@ -816,7 +815,7 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     if (rc || (rc = mark(2, st))) return rc;
     if (side && (rc = join_from(side, 0, st))) return rc;  // the rasterizer reads the accumulated opacities
     rc = tiles_rasterize_impl(c.B, views, num_tiles, c.T, c.max_level, ST, w.alpha_acc, c.stochastic ? 1 : 0,
-                              c.thr_const, rng, rast, w.tiles, list_capacity, rs, st, block_shape_log2(c), c.raster_mode);
+                              c.thr_const, rng, rast, w.tiles, list_capacity, rs, st, block_shape_log2(c));
     if (rc || (rc = mark(3, st))) return rc;
 
     // fused shading forward + backward

@@ -551,8 +551,6 @@ struct WarpRecs {
     int t[kRecCap];
     float b0[kRecCap], b1[kRecCap], z[kRecCap];
     unsigned char lane[kRecCap];
-    float fin_z[32];  // per lane: depth of the visible surface (+inf when empty)
-    int fin_t[32];    // per lane: visible triangle (-1 when empty)
 };
 
 __device__ __forceinline__ void push_fallback(const RecordStore& rs, int item) {
@@ -560,60 +558,54 @@ __device__ __forceinline__ void push_fallback(const RecordStore& rs, int item) {
 }
 
 // Writes the records of the finished block that lie in front of (or level
-// with) each lane's final surface into the warp's chunk, reserving a new
-// chunk when the current one is full.  `cid` = current chunk (-1: none,
-// -2: the store is exhausted), `cfill` = records in it.
-__device__ __noinline__ void flush_records(const RecordStore& rs, WarpRecs& R, int nrec, int item, uint32_t pix,
+// with) each lane's final surface into the warp's chunk.  The chunk must
+// hold all nrec of them (the kept count is not known before the pass), so a
+// new one is reserved when it does not; `cid` = current chunk (-1: none,
+// -2: the store is exhausted), `cfill` = records in it.  Record j's lane
+// passes its pixel, surface depth and visible triangle by shuffle.
+__device__ __forceinline__ void flush_records(const RecordStore& rs, const WarpRecs& R, int nrec, int item, uint32_t pix,
                                               unsigned long long best, float bz, int& cid, int& cfill) {
     const int lane = threadIdx.x & 31;
     if (nrec > kRecCap) {
         push_fallback(rs, item);
         return;
     }
-    R.fin_z[lane] = best == ~0ull ? INFINITY : bz;
-    // the visible triangle as the backward pass reads it back from rast (id + 1 stored as a float)
-    R.fin_t[lane] = best == ~0ull ? -1 : (int)(float)((uint32_t)(best & 0xffffffffu) + 1u) - 1;
-    __syncwarp();
-    int n = 0;
-    for (int j0 = 0; j0 < nrec; j0 += 32) {
-        const int j = j0 + lane;
-        const bool keep = j < nrec && R.z[j] <= R.fin_z[R.lane[j]];
-        n += __popc(__ballot_sync(0xffffffffu, keep));
-    }
-    if (n == 0) return;
-    if (cid == -1 || (cid >= 0 && cfill + n > kRecChunk)) {
+    // the surface depth (+inf when empty) and the visible triangle as the backward pass reads it back from
+    // rast (id + 1 stored as a float; -1 when empty)
+    const float fz = best == ~0ull ? INFINITY : bz;
+    const int ft = best == ~0ull ? -1 : (int)(float)((uint32_t)(best & 0xffffffffu) + 1u) - 1;
+    if (cid == -1 || (cid >= 0 && cfill + nrec > kRecChunk)) {
         if (cid >= 0 && lane == 0) rs.chunk_fill[cid] = cfill;
         int base = 0;
         if (lane == 0) base = atomicAdd(rs.counters, kRecChunk);
         base = __shfl_sync(0xffffffffu, base, 0);
-        if ((int64_t)base + kRecChunk <= rs.capacity) {
-            cid = base / kRecChunk;
-        } else {
-            cid = -2;
-        }
+        cid = (int64_t)base + kRecChunk <= rs.capacity ? base / kRecChunk : -2;
         cfill = 0;
     }
     if (cid == -2) {
         push_fallback(rs, item);
         return;
     }
-    int at = cfill;
+    int4* out = rs.rec + (int64_t)cid * kRecChunk + cfill;
+    const unsigned below = (1u << lane) - 1u;
+    int at = 0;
     for (int j0 = 0; j0 < nrec; j0 += 32) {
         const int j = j0 + lane;
-        const int jj = j < nrec ? j : 0;
-        const int src = R.lane[jj];
+        const bool in = j < nrec;
+        const int src = in ? (int)R.lane[j] : 0;
+        const float sz = __shfl_sync(0xffffffffu, fz, src);
+        const int stri = __shfl_sync(0xffffffffu, ft, src);
         const uint32_t p = __shfl_sync(0xffffffffu, pix, src);
-        const bool keep = j < nrec && R.z[jj] <= R.fin_z[src];
+        const bool keep = in && R.z[j] <= sz;
         const unsigned m = __ballot_sync(0xffffffffu, keep);
         if (keep) {
-            const int t = R.t[jj];
-            const uint32_t tv = (uint32_t)t | (t == R.fin_t[src] ? 0x80000000u : 0u);
-            rs.rec[(int64_t)cid * kRecChunk + at + __popc(m & ((1u << lane) - 1u))] =
-                make_int4((int)p, (int)tv, __float_as_int(R.b0[jj]), __float_as_int(R.b1[jj]));
+            const int t = R.t[j];
+            const uint32_t tv = (uint32_t)t | (t == stri ? 0x80000000u : 0u);
+            out[at + __popc(m & below)] = make_int4((int)p, (int)tv, __float_as_int(R.b0[j]), __float_as_int(R.b1[j]));
         }
         at += __popc(m);
     }
-    cfill = at;
+    cfill += at;
 }
 
 // Forward: depth test with stochastic opacity.  Each warp walks the
@@ -629,7 +621,7 @@ __device__ __noinline__ void flush_records(const RecordStore& rs, WarpRecs& R, i
 // bound at every point of the walk, so the walk meets and keeps all of them;
 // at the end of the block those behind the final surface are dropped.
 #ifndef DSB_RASTER_MIN_CTAS
-#define DSB_RASTER_MIN_CTAS 5  // resident 8-warp CTAs per SM the register budget is sized for (48 registers)
+#define DSB_RASTER_MIN_CTAS 4  // resident 8-warp CTAs per SM the register budget is sized for (64 registers)
 #endif
 
 template <bool REC>
@@ -696,9 +688,12 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, DSB_RASTER_MIN_CTAS) raster
                             if (REC) rec = (key >> 32) <= (best >> 32);
                             if (depth > -1.f) {
                                 if (key < best) {
-                                    const float alpha = interp_scalar(b0, b1, level, level, alpha_src + (size_t)t * S);
-                                    const float thr = thr_mode == 1 ? philox_uniform_tri(php, seed, t) : thr_const;
-                                    if (!(alpha < thr)) {
+                                    const float alpha = interp_level(b0, b1, level, alpha_src + (size_t)t * S);
+                                    // Philox thresholds lie in [0, 1): an opacity of 1 passes without a draw
+                                    const bool pass = thr_mode == 1
+                                                          ? alpha >= 1.f || !(alpha < philox_uniform_tri(php, seed, t))
+                                                          : !(alpha < thr_const);
+                                    if (pass) {
                                         best = key; bb0 = b0; bb1 = b1; bz = depth;
                                         improved = true;
                                     }
@@ -739,208 +734,12 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, DSB_RASTER_MIN_CTAS) raster
     if (REC && cid >= 0 && lane == 0) rs.chunk_fill[cid] = cfill;
 }
 
-// The same depth test with the per-pixel work of a staged group done as a
-// queue of (triangle, pixel) pairs, 32 pairs per warp instruction.  A
-// triangle that covers a pixel centre of an 8x4 block covers 7 of its 32 on
-// average, so the walk above runs its exact coverage, depth, opacity and
-// threshold work at a quarter of the lanes.  Here each staged group is walked
-// twice: first every candidate is tested against the block with the cheap
-// edge-sign test (all lanes, one pixel each) and its coverage mask queued;
-// then the queued pairs are dealt out 32 at a time in list order, lane i
-// taking pair i: exact coverage, depth key and -- in front of the pixel's
-// current winner -- lattice opacity and Philox threshold; passing fragments
-// take the pixel's winner with a shared-memory atomicMin on the depth key
-// (the key holds the triangle index, so the minimum is unique), and the
-// owners read the round's winners back.  The result is the same minimum
-// over passing fragments as the walk's; pairs a round skips lie behind a
-// fragment that passed, so none of them could win.  REC keeps every
-// fragment whose key does not lie behind the pixel's winner when it is
-// evaluated: a superset of the walk's, filtered to the final surface at the
-// end of the block.
-struct WarpPairs {
-    unsigned long long best[32];  // per pixel lane: the winner's depth key (~0: none)
-    float pay[3][32];             // per pixel lane: the winner's b0, b1, z
-    unsigned mask[32];            // per queued candidate: lanes whose centre it may cover
-    int pre[32];                  // inclusive prefix of the queued candidates' lane counts
-    unsigned char cand[32];       // per queued candidate: its index in the stage
-};
-
-// Shared memory of the pair-queue rasterizer (dynamic: above the 48 KB static limit with records).
-template <bool REC>
-struct PairsSmem {
-    WarpStage stage[kWarpsPerCta];
-    WarpRecs rec[REC ? kWarpsPerCta : 1];
-    WarpPairs pairs[kWarpsPerCta];
-};
-
-#ifndef DSB_PAIRS_MIN_CTAS
-#define DSB_PAIRS_MIN_CTAS 4  // resident 8-warp CTAs per SM (the record buffers' shared memory allows 4): 64 registers
-#endif
-
-template <bool REC>
-__global__ void __launch_bounds__(kWarpsPerCta * 32, DSB_PAIRS_MIN_CTAS) raster_pairs_kernel(
-    int B, const ds_view_desc* __restrict__ views, int num_tiles, int T, const TriBox* __restrict__ boxes,
-    const TriVerts* __restrict__ verts, const TriEdges* __restrict__ edges, const int64_t* __restrict__ offsets,
-    const int* __restrict__ sorted, const ListEntry* __restrict__ list, int64_t capacity, int level, int S,
-    const float* __restrict__ alpha_src, int thr_mode, float thr_const, const uint64_t* __restrict__ rng, int* work,
-    float* __restrict__ rast, RecordStore rs, int bwl) {
-    extern __shared__ __align__(16) unsigned char pairs_smem_raw[];
-    PairsSmem<REC>& sm = *reinterpret_cast<PairsSmem<REC>*>(pairs_smem_raw);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    WarpStage& st = sm.stage[warp];
-    WarpRecs& R = sm.rec[REC ? warp : 0];
-    WarpPairs& Q = sm.pairs[warp];
-    uint64_t seed = 0;
-    uint32_t iter = 0;
-    if (thr_mode == 1) { seed = rng[0]; iter = (uint32_t)rng[1]; }
-    int cid = -1, cfill = 0;  // REC: the warp's current record chunk
-    const int items = num_tiles * kBlocksPerTile;
-    for (int item = warp_next(work); item < items; item = warp_next(work)) {
-        const BlockGeom g = block_geometry(item, B, views, T, offsets, sorted, capacity, bwl);
-        const float ndc_x = pix_ndc(g.px, g.W), ndc_y = pix_ndc(g.py, g.H);
-        unsigned long long best = ~0ull;
-        float bb0 = 0.f, bb1 = 0.f, bz = 0.f;
-        Q.best[lane] = ~0ull;
-        int nrec = 0;
-        float warp_far = warp_max(g.valid ? INFINITY : -INFINITY);
-        bool all_won = false;
-        __syncwarp();
-        for (int64_t g0 = g.begin; g0 < g.end; g0 += 32) {
-            float head;
-            const int nc = stage_group(g, g0, boxes, verts, edges, list, T, warp_far, st, &head);
-            if (g.ordered && head > warp_far) break;  // this group and all later ones lie behind
-            // ---- candidates against the block: coverage masks of the edge-sign test ----
-            int nq = 0;
-            for (int k = 0; k < nc; ++k) {
-                if (st.box[k].zlo > warp_far) {
-                    if (g.ordered) break;
-                    continue;
-                }
-                const float4 p0 = st.v[k].p0, p1 = st.v[k].p1, p2 = st.v[k].p2;
-                const TriBox r = st.box[k];
-                const bool near = g.valid && g.px >= r.x0 && g.px < r.x1 && g.py >= r.y0 && g.py < r.y1 &&
-                                  !(best != ~0ull && r.zlo > bz);
-                if (!__any_sync(0xffffffffu, near)) continue;  // warp-uniform
-                float A0, A1, A2, A;
-                edge_terms(ndc_y, ndc_x, p0, p1, p2, A0, A1, A2, A);
-                const unsigned m = __ballot_sync(0xffffffffu, near && !surely_outside(A0, A1, A2, A));
-                if (m == 0u) continue;
-                if (lane == 0) {
-                    Q.mask[nq] = m;
-                    Q.cand[nq] = (unsigned char)k;
-                }
-                ++nq;
-            }
-            if (nq == 0) {
-                __syncwarp();  // the stage is rewritten by the next group
-                continue;
-            }
-            __syncwarp();
-            int pre = lane < nq ? __popc(Q.mask[lane]) : 0;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int v = __shfl_up_sync(0xffffffffu, pre, o);
-                if (lane >= o) pre += v;
-            }
-            Q.pre[lane] = pre;
-            const int total = __shfl_sync(0xffffffffu, pre, 31);
-            __syncwarp();
-            // ---- the queued (triangle, pixel) pairs, 32 per round, in list order ----
-            for (int e0 = 0; e0 < total; e0 += 32) {
-                const int e = e0 + lane;
-                const bool act = e < total;
-                int j = 0;  // the queued candidate of pair e: the first with pre > e
-                if (act) {
-                    int lo = 0, hi = nq - 1;
-                    while (lo < hi) {
-                        const int mid = (lo + hi) >> 1;
-                        if (Q.pre[mid] > e) hi = mid; else lo = mid + 1;
-                    }
-                    j = lo;
-                }
-                const int rank = act ? e - (j > 0 ? Q.pre[j - 1] : 0) : 0;
-                const int L = act ? (int)__fns(Q.mask[j], 0u, rank + 1) : 0;  // the pair's pixel lane
-                const int k = act ? (int)Q.cand[j] : 0;
-                const uint32_t t = (uint32_t)st.t[k];
-                bool pass = false, rec = false;
-                float b0 = 0.f, b1 = 0.f, depth = 0.f;
-                unsigned long long key = ~0ull;
-                if (act) {
-                    const int pxL = g.wx0 + (L & (g.bw - 1)), pyL = g.wy0 + (L >> bwl);
-                    const float4 p0 = st.v[k].p0, p1 = st.v[k].p1, p2 = st.v[k].p2;
-                    float A0, A1, A2, A;
-                    edge_terms(pix_ndc(pyL, g.H), pix_ndc(pxL, g.W), p0, p1, p2, A0, A1, A2, A);
-                    float z, w;
-                    if (finish_coverage(A0, A1, A, p0, p1, p2, b0, b1, z, w)) {
-                        depth = __fdiv_rn(z, w);
-                        if (depth >= -1.f && depth <= 1.f) {
-                            key = depth_key(depth, t);
-                            const unsigned long long cur = Q.best[L];
-                            if (REC) rec = (key >> 32) <= (cur >> 32);
-                            if (depth > -1.f && key < cur) {
-                                const float alpha = interp_scalar(b0, b1, level, level, alpha_src + (size_t)t * S);
-                                float thr = thr_const;
-                                if (thr_mode == 1) {
-                                    const PhiloxPixel pp = philox_pixel(seed, iter, (uint32_t)g.b,
-                                                                        (uint32_t)(pyL * g.W + pxL));
-                                    thr = philox_uniform_tri(pp, seed, t);
-                                }
-                                pass = !(alpha < thr);
-                            }
-                        }
-                    }
-                }
-                if (pass) atomicMin(&Q.best[L], key);
-                __syncwarp();
-                if (pass && Q.best[L] == key) {
-                    Q.pay[0][L] = b0;
-                    Q.pay[1][L] = b1;
-                    Q.pay[2][L] = depth;
-                }
-                if (REC) {
-                    const unsigned m = __ballot_sync(0xffffffffu, rec);
-                    const int at = nrec + __popc(m & ((1u << lane) - 1u));
-                    if (rec && at < kRecCap) {
-                        R.t[at] = (int)t; R.b0[at] = b0; R.b1[at] = b1; R.z[at] = depth;
-                        R.lane[at] = (unsigned char)L;
-                    }
-                    nrec += __popc(m);
-                }
-                __syncwarp();
-                // owners take the round's winners
-                const unsigned long long nb = Q.best[lane];
-                const bool improved = nb != best;
-                if (improved) {
-                    best = nb;
-                    bb0 = Q.pay[0][lane]; bb1 = Q.pay[1][lane]; bz = Q.pay[2][lane];
-                }
-                if (__any_sync(0xffffffffu, improved)) {
-                    if (!all_won) all_won = __all_sync(0xffffffffu, !g.valid || best != ~0ull);
-                    if (all_won) warp_far = warp_max(!g.valid ? -INFINITY : bz);
-                }
-            }
-            __syncwarp();  // the stage and the queue are rewritten by the next group
-        }
-        if (g.valid) {
-            float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (best != ~0ull) o = make_float4(bb0, bb1, bz, (float)((uint32_t)(best & 0xffffffffu) + 1u));
-            reinterpret_cast<float4*>(rast)[g.pix] = o;
-        }
-        if (REC && nrec > 0) {
-            __syncwarp();
-            flush_records(rs, R, nrec, item, (uint32_t)g.pix, best, bz, cid, cfill);
-        }
-        __syncwarp();  // the buffers are rewritten by the next block
-    }
-    if (REC && cid >= 0 && lane == 0) rs.chunk_fill[cid] = cfill;
-}
-
 // dL/dalpha of one fragment scattered through the lattice adjoint
 // (rasterize.cu:951-970 followed by multires.cu:130-222).
 __device__ __forceinline__ void aux_scatter(float b0, float b1, int level, int S, const float* __restrict__ alpha_src,
                                             int t, float loss, bool visible, float scale,
                                             float* __restrict__ grad_alpha_src) {
-    const float alpha = interp_scalar(b0, b1, level, level, alpha_src + (size_t)t * S);
+    const float alpha = interp_level(b0, b1, level, alpha_src + (size_t)t * S);
     const float ga = aux_alpha_grad(loss, alpha, visible) * scale;
     uint32_t idx[3];
     float w[3];
@@ -1082,7 +881,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) aux_kernel(
                 }
                 if (!__any_sync(0xffffffffu, hit)) continue;
                 if (hit) {
-                    const float alpha = interp_scalar(b0, b1, level, level, alpha_src + (size_t)t * S);
+                    const float alpha = interp_level(b0, b1, level, alpha_src + (size_t)t * S);
                     const float ga = aux_alpha_grad(loss, alpha, tp >= 0 && t == tp) * scale;
                     uint32_t idx[3];
                     float w[3];
@@ -1176,31 +975,14 @@ static unsigned block_grid(int num_tiles, const void* kernel, int& per_sm, size_
     return (unsigned)(ctas < 1 ? 1 : (ctas < cap ? ctas : cap));
 }
 
-static int g_occ_raster = 0, g_occ_raster_rec = 0, g_occ_aux = 0, g_occ_pairs = 0, g_occ_pairs_rec = 0;
+static int g_occ_raster = 0, g_occ_raster_rec = 0, g_occ_aux = 0;
 
 int tiles_rasterize_impl(int B, const ds_view_desc* views, int num_tiles, int T, int level, int S,
                          const float* alpha_src, int thr_mode, float thr_const, const uint64_t* rng, float* rast,
-                         void* workspace, int64_t list_capacity, const RecordStore* rs, cudaStream_t st, int bwl,
-                         int mode) {
+                         void* workspace, int64_t list_capacity, const RecordStore* rs, cudaStream_t st, int bwl) {
     if (num_tiles == 0) return DS_OK;
     TileWs w = carve(workspace, B, T, num_tiles, list_capacity, nullptr);
     DS_CUDA(cudaMemsetAsync(w.work, 0, sizeof(int), st));
-    if (mode == 1) {  // pair queue
-        if (rs != nullptr) {
-            const void* k = reinterpret_cast<const void*>(&raster_pairs_kernel<true>);
-            const size_t smem = sizeof(PairsSmem<true>);
-            raster_pairs_kernel<true><<<block_grid(num_tiles, k, g_occ_pairs_rec, smem), kWarpsPerCta * 32, smem, st>>>(
-                B, views, num_tiles, T, w.boxes, w.verts, w.edges, w.offsets, w.sorted, w.list, list_capacity, level,
-                S, alpha_src, thr_mode, thr_const, rng, w.work, rast, *rs, bwl);
-        } else {
-            const void* k = reinterpret_cast<const void*>(&raster_pairs_kernel<false>);
-            const size_t smem = sizeof(PairsSmem<false>);
-            raster_pairs_kernel<false><<<block_grid(num_tiles, k, g_occ_pairs, smem), kWarpsPerCta * 32, smem, st>>>(
-                B, views, num_tiles, T, w.boxes, w.verts, w.edges, w.offsets, w.sorted, w.list, list_capacity, level,
-                S, alpha_src, thr_mode, thr_const, rng, w.work, rast, RecordStore{}, bwl);
-        }
-        return check_launch("tiles_rasterize");
-    }
     if (rs != nullptr) {
         const void* k = reinterpret_cast<const void*>(&raster_kernel<true>);
         raster_kernel<true><<<block_grid(num_tiles, k, g_occ_raster_rec), kWarpsPerCta * 32, 0, st>>>(
@@ -1263,7 +1045,7 @@ int ds_tiles_rasterize(int B, const ds_view_desc* views, int num_tiles, int V, c
     DS_CHECK_ARG(thr_mode == 0 || (thr_mode == 1 && rng != nullptr), "tiles_rasterize: bad threshold mode");
     DS_CHECK_ARG(((uintptr_t)rast & 15) == 0, "tiles_rasterize: rast not 16-byte aligned");
     return tiles_rasterize_impl(B, views, num_tiles, T, level, S, alpha_src, thr_mode, thr_const, rng, rast,
-                                workspace, list_capacity, nullptr, (cudaStream_t)stream, kDefaultBlockShape, 0);
+                                workspace, list_capacity, nullptr, (cudaStream_t)stream, kDefaultBlockShape);
 }
 
 int ds_tiles_opacity_aux(int B, const ds_view_desc* views, int num_tiles, int V, const float* pos, int T,

@@ -65,13 +65,9 @@ struct RecordStore {
 constexpr int kDefaultBlockShape = 3;
 
 // Rasterizer of ds_tiles_rasterize; records fragments when rs != nullptr.
-// mode 0: each warp walks its block's candidates one triangle at a time;
-// mode 1: the per-pixel work of each staged group as a queue of (triangle,
-// pixel) pairs, 32 per round (same results).
 int tiles_rasterize_impl(int B, const ds_view_desc* views, int num_tiles, int T, int level, int S,
                          const float* alpha_src, int thr_mode, float thr_const, const uint64_t* rng, float* rast,
-                         void* workspace, int64_t list_capacity, const RecordStore* rs, cudaStream_t st, int bwl,
-                         int mode);
+                         void* workspace, int64_t list_capacity, const RecordStore* rs, cudaStream_t st, int bwl);
 
 // Opacity auxiliary gradient with a per-pixel loss l1 [pixels]: from the
 // records plus the fallback blocks when rs != nullptr, else by

@@ -41,7 +41,7 @@ class StepConfig(C.Structure):
                 ("max_level", C.c_int32), ("hidden", C.c_int32), ("n_layers", C.c_int32),
                 ("stochastic", C.c_int32), ("thr_const", C.c_float), ("frag_records", C.c_float),
                 ("precision", C.c_int32), ("block_shape", C.c_int32), ("view_enc", C.c_int32),
-                ("target_u8", C.c_int32), ("raster_mode", C.c_int32), ("shade_mode", C.c_int32)]
+                ("target_u8", C.c_int32), ("shade_mode", C.c_int32)]
 
 
 _L = _core.lib
@@ -112,9 +112,11 @@ class TrainStep:
             raise ValueError(f"precision must be 'bf16' or 'split', not {precision!r}")
         if view_enc not in ("dir3", "sh2"):
             raise ValueError(f"view_enc must be 'dir3' or 'sh2', not {view_enc!r}")
-        self.cfg = StepConfig(self.B, T, V, C_, min_level, max_level, hidden, n_layers, int(stochastic), 0.5,
-                              float(frag_records), 1 if precision == "split" else 0, 0, 1 if view_enc == "sh2" else 0,
-                              int(bool(target_u8)), 1, 0)
+        self.cfg = StepConfig(B=self.B, T=T, V=V, C=C_, min_level=min_level, max_level=max_level, hidden=hidden,
+                              n_layers=n_layers, stochastic=int(stochastic), thr_const=0.5,
+                              frag_records=float(frag_records), precision=1 if precision == "split" else 0,
+                              block_shape=0, view_enc=1 if view_enc == "sh2" else 0, target_u8=int(bool(target_u8)),
+                              shade_mode=0)
         self.views, self.num_tiles, self.num_pixels, self.pix_offsets = _tiles.view_table(self.hw, self.device)
         self.S = sum(_core.feats_at_level(l) for l in range(min_level, max_level + 1))
         self.nparam = int(_L.ds_step_mlp_param_count(C.byref(self.cfg)))
@@ -200,7 +202,6 @@ class TrainStep:
         raise RuntimeError("tile list capacity did not converge")
 
     BLOCK_SHAPES = {0: "8x4", 1: "16x2", 2: "4x8"}
-    RASTER_MODES = {0: "walk", 1: "pairs"}
     SHADE_MODES = {0: "mma.sync", 1: "tcgen05"}
 
     def tcgen05_shading(self) -> bool:
@@ -209,8 +210,7 @@ class TrainStep:
         c = self.cfg
         return (c.C == 16 and c.hidden == 64 and c.n_layers == 2 and c.view_enc == 0 and c.precision == 0)
 
-    def autotune(self, *args, steps: int = 5, shapes: Sequence[int] = (0, 1, 2), modes: Sequence[int] = (0, 1),
-                 **kwargs) -> Dict[str, object]:
+    def autotune(self, *args, steps: int = 5, shapes: Sequence[int] = (0, 1, 2), **kwargs) -> Dict[str, object]:
         """Chooses the launch layout of this step for its inputs (the step's own
         autotuner, run eagerly before training and before any capture):
 
@@ -219,9 +219,7 @@ class TrainStep:
           * the fragment-record store, sized to the records a step reserves
             plus a quarter, so that no block is re-enumerated;
           * the pixel block of a rasterizer warp (8x4, 16x2 or 4x8 pixels of a
-            16x16 tile, 8 warps per tile) and the rasterizer's work layout
-            (walk: one candidate triangle at a time; pairs: queued (triangle,
-            pixel) pairs, 32 per instruction), and for the wide BF16 MLP the
+            16x16 tile, 8 warps per tile) and, for the wide BF16 MLP, the
             shading kernel (warp-level mma.sync or tcgen05 with TMEM
             accumulators): each combination is timed with CUDA events over
             `steps` eager steps after a warm-up, and the fastest kept.
@@ -238,7 +236,6 @@ class TrainStep:
             self.capacity = max(self.capacity, hit["list_capacity"])
             self.cfg.frag_records = hit["frag_records"]
             self.cfg.block_shape = hit["block_shape"]
-            self.cfg.raster_mode = hit["raster_mode"]
             self.cfg.shade_mode = hit["shade_mode"]
             self._alloc()
             return dict(hit)
@@ -252,11 +249,11 @@ class TrainStep:
             self._alloc()
         times = {}
         shade_modes = (0, 1) if self.tcgen05_shading() else (0,)
-        combos = [(int(sh), int(md), sm) for sm in shade_modes for md in modes for sh in shapes]
-        name = lambda c: (f"{self.BLOCK_SHAPES[c[0]]}/{self.RASTER_MODES[c[1]]}"  # noqa: E731
-                          + (f"/{self.SHADE_MODES[c[2]]}" if len(shade_modes) > 1 else ""))
+        combos = [(int(sh), sm) for sm in shade_modes for sh in shapes]
+        name = lambda c: (self.BLOCK_SHAPES[c[0]]  # noqa: E731
+                          + (f"/{self.SHADE_MODES[c[1]]}" if len(shade_modes) > 1 else ""))
         for combo in combos:
-            self.cfg.block_shape, self.cfg.raster_mode, self.cfg.shade_mode = combo
+            self.cfg.block_shape, self.cfg.shade_mode = combo
             for _ in range(2):
                 self.run(*args, **kwargs)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -267,12 +264,12 @@ class TrainStep:
             torch.cuda.synchronize()
             times[name(combo)] = e0.elapsed_time(e1) / steps
         best = min(combos, key=lambda c: times[name(c)])
-        self.cfg.block_shape, self.cfg.raster_mode, self.cfg.shade_mode = best
+        self.cfg.block_shape, self.cfg.shade_mode = best
         self.rng[1].copy_(it0)
         self.status.zero_()
         out = {"list_capacity": int(self.capacity), "frag_records": float(self.cfg.frag_records),
-               "block_shape": best[0], "block": self.BLOCK_SHAPES[best[0]], "raster_mode": best[1],
-               "raster": self.RASTER_MODES[best[1]], "shade_mode": best[2], "shade": self.SHADE_MODES[best[2]],
+               "block_shape": best[0], "block": self.BLOCK_SHAPES[best[0]], "shade_mode": best[1],
+               "shade": self.SHADE_MODES[best[1]],
                "ms_per_step": times}
         autotune_cache[key] = dict(out)
         return out

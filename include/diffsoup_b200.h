@@ -259,11 +259,6 @@ typedef struct {
     /* Target images: 0 = fp32 [pixels,3]; 1 = 8-bit [pixels,3] (the
      * reference's datasets are 8-bit images), read as value / 255. */
     int32_t target_u8;
-    /* Rasterizer work layout (same results; TrainStep.autotune times them):
-     * 0 = each warp walks its pixel block's candidate triangles one at a
-     * time; 1 = the per-pixel work of each group of 32 candidates as a queue
-     * of (triangle, pixel) pairs dealt out 32 per warp instruction. */
-    int32_t raster_mode;
     /* Shading kernel of the 16 + direction -> 64 -> 64 -> 3 MLP in BF16
      * precision: 0 = warp-level tensor-core products (mma.sync) with operand
      * tiles in shared memory; 1 = tcgen05.mma on 128-pixel tiles with the

@@ -82,6 +82,29 @@ def test_train_step_binding_argument_errors():
     assert S.mlp_param_count(16, 64, 2) == 64 * 19 + 64 + 64 * 64 + 64 + 3 * 64 + 3
 
 
+def test_step_config_matches_the_header():
+    """diffsoup_b200.step.StepConfig lays out ds_step_config field for field
+    (names, order and 32-bit types), so a change on one side fails here."""
+    from diffsoup_b200 import step as S
+
+    src = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    body = re.search(r"typedef struct \{([^}]*)\}\s*ds_step_config;", src).group(1)
+    want = []
+    for decl in body.split(";"):
+        decl = decl.strip()
+        if not decl:
+            continue
+        ctype, names = decl.split(None, 1)
+        want += [(n.strip(), ctype) for n in names.split(",")]
+    got = [(n, {C.c_int32: "int32_t", C.c_float: "float"}[t]) for n, t in S.StepConfig._fields_]
+    assert got == want
+    # construction by name sets every field
+    cfg = S.StepConfig(B=2, T=3, V=9, C=8, min_level=0, max_level=2, hidden=16, n_layers=1, stochastic=1,
+                       thr_const=0.5, frag_records=2.0, precision=1, block_shape=0, view_enc=0, target_u8=1,
+                       shade_mode=0)
+    assert (cfg.B, cfg.target_u8, cfg.shade_mode) == (2, 1, 0)
+
+
 def declared_prototypes():
     """name -> list of parameter declarations of every ds_* prototype."""
     src = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)

@@ -306,16 +306,14 @@ def test_train_step_gradients_match_central_differences(config):
 
 
 def test_block_shapes_give_identical_results_and_autotune_picks_one():
-    """The three pixel-block shapes of the rasterizer warps (8x4, 16x2, 4x8),
-    each with both work layouts (candidate walk, pair queue), give
-    bit-identical ID buffers, the same loss and the same opacity gradients
+    """The three pixel-block shapes of the rasterizer warps (8x4, 16x2, 4x8)
+    give bit-identical ID buffers, the same loss and the same opacity gradients
     (which read the rasterizer's fragment records); the autotuner times them,
     keeps one and leaves the RNG iteration where it was."""
     sc, hw, inp, step, d = _setup(2, 6, num_tris=3000, num_views=2, resolution=(128, 160))
     outs = []
-    for shape, mode in [(s_, m_) for m_ in (0, 1) for s_ in (0, 1, 2)]:
+    for shape in (0, 1, 2):
         step.cfg.block_shape = shape
-        step.cfg.raster_mode = mode
         step.rng[1] = 0
         rast = torch.empty(step.num_pixels, 4, device=DEV)
         loss = float(step.run(**d, rast_out=rast).item())
@@ -327,7 +325,7 @@ def test_block_shapes_give_identical_results_and_autotune_picks_one():
         assert rel(ga.cpu().numpy(), outs[0][2].cpu().numpy()) < 1e-5
     step.rng[1] = 3
     choice = step.autotune(**d, steps=2)
-    assert choice["block_shape"] in (0, 1, 2) and choice["raster_mode"] in (0, 1)
-    assert set(choice["ms_per_step"]) == {f"{b}/{m}" for b in ("8x4", "16x2", "4x8") for m in ("walk", "pairs")}
+    assert choice["block_shape"] in (0, 1, 2)
+    assert set(choice["ms_per_step"]) == {"8x4", "16x2", "4x8"}
     assert int(step.rng[1].item()) == 3
     assert step.autotune(**d, steps=2)["block_shape"] == choice["block_shape"]  # cached
