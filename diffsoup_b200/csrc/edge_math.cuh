@@ -370,15 +370,21 @@ struct EdgePair {
     float A1[3];
 };
 
-__device__ __forceinline__ EdgePair edge_pair(const EdgeHalo& h, const EdgeFrame& f, int hidx, int e, int H, int W,
-                                              float sx, float sy) {
+// Adjoint of the colour step between staged pixels a and b.
+__device__ __forceinline__ float pair_adjoint(const EdgeHalo& h, int a, int b) {
+    float adj = 0.f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) adj += 0.5f * (h.g[i][a] + h.g[i][b]) * (h.c[i][a] - h.c[i][b]);
+    return adj;
+}
+
+// The pair towards neighbour e given its adjoint.
+__device__ __forceinline__ EdgePair edge_pair(const EdgeFrame& f, int hidx, int e, float adj, int H, int W, float sx,
+                                              float sy) {
     EdgePair p;
     p.DX = (e == 0) - (e == 1);
     p.DY = (e == 3) - (e == 2);
     p.n = hidx + p.DX + p.DY * kHaloW;
-    float adj = 0.f;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) adj += 0.5f * (h.g[i][hidx] + h.g[i][p.n]) * (h.c[i][hidx] - h.c[i][p.n]);
     p.gx = adj * (float)p.DX * (float)W / 2.f;
     p.gy = adj * (float)p.DY * (float)H / 2.f;
     p.hx = 0.5f * (float)p.DX * sx;
@@ -391,15 +397,18 @@ __device__ __forceinline__ EdgePair edge_pair(const EdgeHalo& h, const EdgeFrame
 // Edge-gradient estimator of one pixel from the staged tile: the pixel's
 // triangle (or -1) is returned and its clip-space vertex gradients are in
 // acc.g[vertex*4 + xyzw].  A first pass over the four neighbours only
-// classifies the pairs; interior and opacity-edge pairs (midpoint
+// classifies the pairs (keeping each marked pair's adjoint in
+// adj[e * kEdgeLanes]); interior and opacity-edge pairs (midpoint
 // contributions), geometric-edge pairs and pairs that may be triangle
 // intersections are then evaluated in three passes, where round k of a pass
 // takes each lane's k-th pair of that kind, so that the lanes of a warp run
 // the same case together.
 // `active` false: the lane has no pixel (it takes part in the warp-wide steps only).
+constexpr int kEdgeLanes = DS_TILE * DS_TILE;  // threads of the edge kernel: the stride of adj
+
 __device__ __forceinline__ int edge_grad_pixel_staged(const EdgeHalo& h, int hidx, int y0, int x0, int H, int W,
                                                       const TriVerts* __restrict__ tverts, EdgeAccum& acc,
-                                                      bool active = true) {
+                                                      float* adj, bool active = true) {
 #pragma unroll
     for (int k = 0; k < 12; ++k) acc.g[k] = 0.f;
     acc.any = false;
@@ -427,8 +436,9 @@ __device__ __forceinline__ int edge_grad_pixel_staged(const EdgeHalo& h, int hid
         }
         f.sgn = As > 0.f ? 1.f : -1.f;  // orientation of the inside near the pixel
         // neighbours (+x, -x, -y, +y) as in rasterize.cu:691-692
-#pragma unroll 1
-        for (int e = 0; e < 4 && As != 0.f; ++e) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            if (As == 0.f) break;
             const int DX = (e == 0) - (e == 1);
             const int DY = (e == 3) - (e == 2);
             const int n = hidx + DX + DY * kHaloW;
@@ -436,8 +446,10 @@ __device__ __forceinline__ int edge_grad_pixel_staged(const EdgeHalo& h, int hid
             if (it1 == kOutside) continue;  // no neighbour in the view
             const bool interior = it1 == it0;
             if (interior && (DX < 0 || DY < 0)) continue;  // interior pair counted by the neighbour
-            const EdgePair p = edge_pair(h, f, hidx, e, H, W, sx, sy);
+            const float a = pair_adjoint(h, hidx, n);
+            const EdgePair p = edge_pair(f, hidx, e, a, H, W, sx, sy);
             if (p.gx == 0.f && p.gy == 0.f) continue;  // zero adjoint
+            adj[e * kEdgeLanes] = a;
             if (interior) {
                 mid |= 1u << e;
                 continue;
@@ -467,7 +479,7 @@ __device__ __forceinline__ int edge_grad_pixel_staged(const EdgeHalo& h, int hid
         if (mid == 0u) continue;
         const int e = __ffs(mid) - 1;
         mid &= mid - 1u;
-        const EdgePair p = edge_pair(h, f, hidx, e, H, W, sx, sy);
+        const EdgePair p = edge_pair(f, hidx, e, adj[e * kEdgeLanes], H, W, sx, sy);
         const float m = h.it[p.n] == it0 ? 2.f : 1.f;
         edge_midpoint(f, p.hx, p.hy, m * p.gx, m * p.gy, 0.f, acc);
     }
@@ -478,7 +490,7 @@ __device__ __forceinline__ int edge_grad_pixel_staged(const EdgeHalo& h, int hid
         if (geo == 0u) continue;
         const int e = __ffs(geo) - 1;
         geo &= geo - 1u;
-        const EdgePair p = edge_pair(h, f, hidx, e, H, W, sx, sy);
+        const EdgePair p = edge_pair(f, hidx, e, adj[e * kEdgeLanes], H, W, sx, sy);
         float tb = 2.f;
         int kb = -1;
 #pragma unroll
@@ -514,7 +526,7 @@ __device__ __forceinline__ int edge_grad_pixel_staged(const EdgeHalo& h, int hid
         if (isect == 0u) continue;
         const int e = __ffs(isect) - 1;
         isect &= isect - 1u;
-        const EdgePair p = edge_pair(h, f, hidx, e, H, W, sx, sy);
+        const EdgePair p = edge_pair(f, hidx, e, adj[e * kEdgeLanes], H, W, sx, sy);
         float ge_x, ge_y, ge_z;
         if (intersection_pair(f.P, tverts, h.it[p.n], f.depth, f.nx, f.ny, p.DX, p.gx, p.gy, ge_x, ge_y, ge_z))
             edge_midpoint(f, p.hx, p.hy, ge_x, ge_y, ge_z, acc);

@@ -428,10 +428,12 @@ __global__ void __launch_bounds__(kEdgeThreads, DSB_EDGE_MIN_CTAS) edge_step_ker
     const int ly = src / DS_TILE, lx = src % DS_TILE;
     const int y = ty0 + ly, x = tx0 + lx;
     EdgeAccum acc;
+    __shared__ float s_adj[4 * kEdgeLanes];  // per thread and neighbour: the marked pairs' adjoints
+    static_assert(kEdgeLanes == kEdgeThreads, "one thread per pixel of the tile");
     // every lane of the warp takes part (warp-wide reductions inside); lanes past the covered
     // pixels contribute nothing
     const int it0 = edge_grad_pixel_staged(h, (ly + 1) * kHaloW + lx + 1, y, x, vd.H, vd.W,
-                                           tab.verts + (size_t)b * T, acc, active);
+                                           tab.verts + (size_t)b * T, acc, s_adj + threadIdx.x, active);
     const int key = (it0 >= 0 && acc.any) ? it0 : -1 - lane;
     if (__ballot_sync(0xffffffffu, key >= 0) == 0) return;  // no lane of the warp has a contribution
     const int prev = __shfl_up_sync(0xffffffffu, key, 1);
