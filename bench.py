@@ -601,15 +601,28 @@ def measure_workload(dev, sc, mlp, precision: str, steps: int, warmup: int, peak
         e.record()
     torch.cuda.synchronize()
     _core.check(_core.lib.ds_train_step_set_events(ctypes_void_p_array(evs), 8))
-    acc = {n: 0.0 for n in names}
     M = 5
-    for _ in range(M):
-        step.run(**kw)
-        torch.cuda.synchronize()
-        for k, n in enumerate(names):
-            acc[n] += evs[k].elapsed_time(evs[k + 1])
+
+    def phases():
+        acc = {n: 0.0 for n in names}
+        for _ in range(M):
+            step.run(**kw)
+            torch.cuda.synchronize()
+            for k, n in enumerate(names):
+                acc[n] += evs[k].elapsed_time(evs[k + 1])
+        return {n: acc[n] / M for n in names}
+
+    phase_ms = phases()
+    # both shading kernels of the wide BF16 MLP, phase by phase (the autotuned one is kept)
+    shade_ab = None
+    if step.tcgen05_shading():
+        chosen = step.cfg.shade_mode
+        shade_ab = {}
+        for mode in (0, 1):
+            step.cfg.shade_mode = mode
+            shade_ab[step.SHADE_MODES[mode]] = round(phases()["shade"], 4)
+        step.cfg.shade_mode = chosen
     _core.check(_core.lib.ds_train_step_set_events(None, 0))
-    phase_ms = {n: acc[n] / M for n in names}
     dom = max(["raster", "shade", "aux", "edge"], key=lambda n: phase_ms[n])
     ST = _core.feats_at_level(sc.max_level)
     alg = algorithmic_bytes(dom, step.num_pixels, B, T, V, ST, sc.feat_dim, 4 if precision == "split" else 2)
@@ -628,8 +641,11 @@ def measure_workload(dev, sc, mlp, precision: str, steps: int, warmup: int, peak
            "device_memory_bytes": int(mem), "workspace_bytes": int(step.workspace.numel()),
            "fragment_records": "tile-wise recomputation" if step.record_capacity == 0 else
                                f"stored ({step.cfg.frag_records:.3f} per pixel)",
-           "autotuned": {"block": tuned["block"], "shade": tuned["shade"], "list_capacity": tuned["list_capacity"]},
+           "autotuned": {"block": tuned["block"], "shade": tuned["shade"], "list_capacity": tuned["list_capacity"],
+                         "ms_per_step_by_layout": {k: round(v, 4) for k, v in tuned["ms_per_step"].items()}},
            "list_overflow": overflow}
+    if shade_ab is not None:
+        out["shade_phase_ms_by_kernel"] = shade_ab
     del step, kw
     if cpu_sample:
         from oracle import cpu, pipeline as P
