@@ -516,7 +516,23 @@ static int launch_shade_tc(const ShadeArgs& a, cudaStream_t st) {
     static int per_sm = 0;  // set on the first (eager) call, before any graph capture
     if (per_sm == 0) {
         DS_CUDA(cudaFuncSetAttribute(shade_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        DS_CUDA(cudaFuncSetAttribute(shade_tc_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared));
         DS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, shade_tc_kernel, kTcThreads, smem));
+        // The query answers 1 for this kernel's 105 KB, while two CTAs fit the SM's shared memory and
+        // registers (and run together: measured 1.6x the throughput of one).  Take the count those two
+        // limits allow.
+        int dev = 0, smem_sm = 0, reserved = 0;
+        cudaFuncAttributes fa;
+        DS_CUDA(cudaGetDevice(&dev));
+        DS_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+        DS_CUDA(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+        DS_CUDA(cudaFuncGetAttributes(&fa, shade_tc_kernel));
+        const int by_smem = smem_sm / (int)(smem + (size_t)reserved);
+        const int regs = (fa.numRegs + 7) / 8 * 8;  // allocation granularity per thread
+        const int by_regs = regs > 0 ? 65536 / (regs * kTcThreads) : 1;
+        const int fit = by_smem < by_regs ? by_smem : by_regs;
+        if (fit > per_sm) per_sm = fit;
         if (per_sm <= 0) return set_error(DS_ERR_CUDA, "shade_tc: kernel does not fit on an SM");
         if (per_sm > 2) per_sm = 2;  // 256 TMEM columns per CTA: two CTAs fill an SM's 512
     }

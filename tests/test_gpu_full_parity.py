@@ -17,6 +17,9 @@
     centre inside the triangle, which edge does the pair cross) flip near
     edges between FP32 and FP64.  The step's vertex gradients must be within
     max(1e-3, 1.5 x that error) of FP64, and close to the FP32 oracle.
+    Configuration 5 also in BF16 precision on the tcgen05 shading kernel
+    (32,400 tiles of 128 pixels, two CTAs per SM), against the FP64 oracle
+    that rounds the same MLP operands to BF16.
 
 The oracle (oracle/pipeline.py) restates the reference's kernels
 (rasterize.cu:653-992 for the edge and opacity estimators) and runs the
@@ -111,8 +114,8 @@ def test_benchmark_workload_full_size(precision):
         assert v <= 1e-3, (k, v)
 
 
-@pytest.mark.parametrize("config", [3, 5])
-def test_full_size_subset_gradients(config):
+@pytest.mark.parametrize("config,precision", [(3, "split"), (5, "split"), (5, "bf16")])
+def test_full_size_subset_gradients(config, precision):
     full = scenes.make_scene(config, seed=0)
     sizes = [v.height * v.width for v in full.views]
     pick = sorted({int(np.argmin(sizes)), int(np.argmax(sizes))}) if config == 3 else [0, 5]
@@ -129,18 +132,25 @@ def test_full_size_subset_gradients(config):
               target=t(np.concatenate([x.reshape(-1, 3) for x in targets])))
     seed = 321
     step = TrainStep(full.T, full.verts.shape[0], hw, full.feat_dim, full.min_level, full.max_level,
-                     full.hidden_dim, full.n_layers, stochastic=True, seed=seed, device=DEV, precision="split")
+                     full.hidden_dim, full.n_layers, stochastic=True, seed=seed, device=DEV, precision=precision)
+    if precision == "bf16":
+        assert step.tcgen05_shading()
+        step.cfg.shade_mode = 1
     step.fit_capacity(**kw)
     inp = P.StepInputs(verts=full.verts, tri=full.tri, mvps=mvp, inv_mvps=inv, hw=hw, feat_src=full.feat_src,
                        alpha_src=full.alpha_src[..., 0], mlp=mlp, targets=targets, min_level=full.min_level,
                        max_level=full.max_level, stochastic=True, seed=seed, iteration=0)
-    errs, ref32 = _check(full, hw, full.tri, mvp, step, kw, inp, seed, with_f32=True)
-    print(f"config{config}: views {pick} ({', '.join(f'{w}x{h}' for h, w in hw)}), {full.T} triangles, split "
-          "precision vs FP64 oracle: " + ", ".join(f"{k}={v:.2e}" for k, v in errs.items())
+    rounding = "bf16" if precision == "bf16" else "none"
+    errs, ref32 = _check(full, hw, full.tri, mvp, step, kw, inp, seed, rounding, with_f32=True)
+    assert int(step.status.item()) & 8 == 0  # no tensor-core stage timed out
+    print(f"config{config}: views {pick} ({', '.join(f'{w}x{h}' for h, w in hw)}), {full.T} triangles, {precision} "
+          f"precision vs {'BF16-rounding ' if precision == 'bf16' else ''}FP64 oracle: "
+          + ", ".join(f"{k}={v:.2e}" for k, v in errs.items())
           + f"; vertex gradients of the FP32 oracle vs FP64 {ref32['f32_vs_f64']:.2e}, step vs FP32 oracle "
           f"{ref32['step_vs_f32']:.2e}")
     for k, v in errs.items():
         if k != "grad_verts":
             assert v <= 1e-3, (k, v)
     assert errs["grad_verts"] <= max(1e-3, 1.5 * ref32["f32_vs_f64"]), (errs["grad_verts"], ref32)
-    assert ref32["step_vs_f32"] <= max(1e-3, 1.5 * ref32["f32_vs_f64"]), ref32
+    if precision == "split":  # the FP32 oracle does not round the MLP operands to BF16
+        assert ref32["step_vs_f32"] <= max(1e-3, 1.5 * ref32["f32_vs_f64"]), ref32
