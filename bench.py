@@ -81,6 +81,10 @@ def parse():
                     help="skip timing the inference render (the viewer's frame) beside the training step")
     ap.add_argument("--views", type=int, default=8, help="views per step (8 is the benchmark workload; "
                     "fewer only for small profiling cases)")
+    ap.add_argument("--side-case", default=None, choices=[w[0] for w in SIDE_WORKLOADS],
+                    help="profiling: time only this side workload (on --side-views views when given) and print "
+                         "its entry")
+    ap.add_argument("--side-views", type=int, default=None)
     return ap.parse_args()
 
 
@@ -418,13 +422,7 @@ def run_ours(args):
     ST = _core.feats_at_level(sc.max_level)
     P_ = step.num_pixels
     alg = algorithmic_bytes(dom, P_, B, T, V, ST, sc.feat_dim, 4 if args.precision == "split" else 2, 3)
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except Exception:
-        pass
-    peak = float(peaks.get("hbm_gbs", 6650.0))
-    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    peak, peak_src = measured_peak()
     achieved = alg / (phase_ms[dom] / 1000.0) / 1e9
     step_bytes = step_algorithmic_bytes(B, T, V, _core.total_feats(sc.min_level, sc.max_level), sc.feat_dim, P_, 3)
     traffic = read_traffic(dom)
@@ -905,9 +903,35 @@ def run_cpu_baseline(sc, mlp, s):
             "sample": f"{n} views of config 2 (800x800, 15K tris) through the FP32 oracle port, {cores} threads"}
 
 
+def measured_peak():
+    """HBM copy bandwidth (GB/s) from MEASURED_PEAKS.json, else the pool's earlier measurement."""
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    return float(peaks.get("hbm_gbs", 6650.0)), ("measured" if "hbm_gbs" in peaks else "fallback")
+
+
+def run_side_case(args):
+    """One side workload alone (a small profiling case with --side-views)."""
+    from diffsoup_b200 import scenes
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    name, config, shading, precision, records = next(w for w in SIDE_WORKLOADS if w[0] == args.side_case)
+    sc = scenes.make_scene(config, seed=0, shading=shading, num_views=args.side_views)
+    mlp = scenes.mlp_weights(sc.mlp_input_dim, 3, sc.hidden_dim, sc.n_layers, seed=0)
+    r = measure_workload(dev, sc, mlp, precision, args.steps, args.warmup, measured_peak()[0], records,
+                         cpu_sample=False)
+    print(json.dumps({"side_case": name, "views": len(sc.views), **r}), flush=True)
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.side_case:
+        run_side_case(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -112,41 +112,72 @@ __global__ void __launch_bounds__(kPrepWarps * 32) accum_sigmoid_backward_kernel
 // lattices to the target lattice is the same sparse map for every triangle,
 // so each CTA builds it once in shared memory: the forward table lists, per
 // target sample, its (source sample, weight) pairs in level-then-corner
-// order (the summation order of accum_sigmoid_kernel, so results are
-// identical), and the backward table is the same map grouped by source
-// sample (CSR), which turns the adjoint into a gather without atomics.
-// Opacity (one channel) and features (C channels) go through one launch.
+// order (the summation order of accum_sigmoid_kernel), and the backward
+// table is the same map grouped by source sample, which turns the adjoint
+// into a gather without atomics.  Pairs of weight zero are left out (a
+// target sample that is a lattice vertex of a level takes one corner there):
+// about half of them, and adding 0 * x leaves a finite sum unchanged.
+//
+// The kernels run a warp over G = 32 / CP triangles at a time, lane (g, c)
+// taking channel c of triangle g: every lane walks the same table row, so
+// the table reads are broadcasts and the loops lane-uniform; the sources (or
+// the target gradients) of the G triangles sit in shared memory as
+// [sample][lane].  The opacities of the G triangles go through the same
+// table with lane (g, j) taking the target (or source) samples j, j + CP, ...
 // ---------------------------------------------------------------------------
-constexpr int kTabMax = 1024;   // (target sample, level, corner) entries
-constexpr int kTabRows = 256;   // source samples
+constexpr int kTabMax = 1024;  // (target sample, level, corner) entries
 constexpr int kTabWarps = 8;
+constexpr size_t kTabSmemMax = 100 * 1024;  // two CTAs per SM at most this size
 
-// The tables in dynamic shared memory (N entries, S rows), followed by one
-// staging buffer per warp.
+// The tables in dynamic shared memory (room for N nonzero pairs), followed
+// by each warp's staging buffer.
 struct LatticeTab {
-    int* fidx;
-    float* fw;
-    int* row;
-    float* cw;
-    short* ck;
+    int2* fent;  // per target sample (rows frow): {source sample, weight bits}
+    int* frow;   // [ST + 1]
+    int2* bent;  // per source sample (rows brow): {target sample, weight bits}
+    int* brow;   // [S + 1]
 };
 
-__host__ __device__ inline size_t lattice_tab_bytes(int N, int S) {
-    return ((size_t)N * 12 + (size_t)(S + 1) * 4 + (size_t)N * 2 + 15) & ~(size_t)15;
+__host__ __device__ inline size_t lattice_tab_bytes(int N, int S, int ST) {
+    return ((size_t)N * 16 + (size_t)(S + ST + 2) * 4 + 15) & ~(size_t)15;
 }
 
-__device__ inline LatticeTab lattice_tab_at(unsigned char* base, int N, int S) {
+__device__ inline LatticeTab lattice_tab_at(unsigned char* base, int N, int S, int ST) {
     LatticeTab L;
-    L.fidx = reinterpret_cast<int*>(base);
-    L.fw = reinterpret_cast<float*>(base + (size_t)N * 4);
-    L.cw = reinterpret_cast<float*>(base + (size_t)N * 8);
-    L.row = reinterpret_cast<int*>(base + (size_t)N * 12);
-    L.ck = reinterpret_cast<short*>(base + (size_t)N * 12 + (size_t)(S + 1) * 4);
+    L.fent = reinterpret_cast<int2*>(base);
+    L.bent = reinterpret_cast<int2*>(base + (size_t)N * 8);
+    L.frow = reinterpret_cast<int*>(base + (size_t)N * 16);
+    L.brow = L.frow + ST + 1;
     return L;
 }
 
-__device__ void build_lattice_tab(const LatticeTab& L, int lo, int hi, int ST, int S) {
+// Per-warp staging floats: a [rows][32] sample-by-lane buffer and the G
+// triangles' opacity rows (rows = S sources forward, ST targets backward).
+__host__ __device__ inline int tab_stage_floats(int rows, int CP) { return 32 * rows + (32 / CP) * (rows + 1); }
+
+// Exclusive prefix of rows[1..n] into rows[0..n] (rows[0] = 0), one warp.
+__device__ inline void tab_scan(int* rows, int n) {
+    const int lane = threadIdx.x & 31;
+    int carry = 0;
+    if (lane == 0) rows[0] = 0;
+    for (int d0 = 0; d0 < n; d0 += 32) {
+        const int d = d0 + lane;
+        int v = d < n ? rows[d + 1] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += u;
+        }
+        if (d < n) rows[d + 1] = carry + v;
+        carry += __shfl_sync(0xffffffffu, v, 31);
+    }
+}
+
+// Builds the tables; `scratch` holds N ints and N floats during the build.
+__device__ void build_lattice_tab(const LatticeTab& L, int lo, int hi, int ST, int S, unsigned char* scratch) {
     const int NL = hi - lo + 1, NE = NL * 3, N = ST * NE;
+    int* fidx = reinterpret_cast<int*>(scratch);
+    float* fw = reinterpret_cast<float*>(scratch + (size_t)N * 4);
     const float inv_r = 1.f / (float)(1u << hi);  // a power of two: x * inv_r == x / 2^hi exactly
     for (int u = threadIdx.x; u < ST * NL; u += blockDim.x) {
         const int k = u / NL, li = u - (u / NL) * NL, l = lo + li;
@@ -159,54 +190,52 @@ __device__ void build_lattice_tab(const LatticeTab& L, int lo, int hi, int ST, i
         for (int m = lo; m < l; ++m) off += feats_at_level((uint32_t)m);
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
-            L.fidx[k * NE + li * 3 + j] = (int)(off + idx[j]);
-            L.fw[k * NE + li * 3 + j] = w[j];
+            fidx[k * NE + li * 3 + j] = (int)(off + idx[j]);
+            fw[k * NE + li * 3 + j] = w[j];
         }
     }
     __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    for (int d = warp; d < S; d += nw) {  // row lengths
+    for (int k = threadIdx.x; k < ST; k += blockDim.x) {  // forward row lengths
         int cnt = 0;
-        for (int e0 = 0; e0 < N; e0 += 32) cnt += __popc(__ballot_sync(0xffffffffu, e0 + lane < N && L.fidx[e0 + lane] == d));
-        if (lane == 0) L.row[d + 1] = cnt;
+        for (int n = 0; n < NE; ++n) cnt += fw[k * NE + n] != 0.f;
+        L.frow[k + 1] = cnt;
     }
-    __syncthreads();
-    if (warp == 0) {  // exclusive prefix over the rows
-        int carry = 0;
-        if (lane == 0) L.row[0] = 0;
-        for (int d0 = 0; d0 < S; d0 += 32) {
-            const int d = d0 + lane;
-            int v = d < S ? L.row[d + 1] : 0;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int n = __shfl_up_sync(0xffffffffu, v, o);
-                if (lane >= o) v += n;
-            }
-            if (d < S) L.row[d + 1] = carry + v;
-            carry += __shfl_sync(0xffffffffu, v, 31);
-        }
-    }
-    __syncthreads();
-    for (int d = warp; d < S; d += nw) {  // entries of each row in (target, level, corner) order
-        int at = L.row[d];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int d = warp; d < S; d += nw) {  // backward row lengths
+        int cnt = 0;
         for (int e0 = 0; e0 < N; e0 += 32) {
             const int e = e0 + lane;
-            const bool hit = e < N && L.fidx[e] == d;
+            cnt += __popc(__ballot_sync(0xffffffffu, e < N && fidx[e] == d && fw[e] != 0.f));
+        }
+        if (lane == 0) L.brow[d + 1] = cnt;
+    }
+    __syncthreads();
+    if (warp == 0) tab_scan(L.frow, ST);
+    if (warp == 1 % nw) tab_scan(L.brow, S);
+    __syncthreads();
+    for (int k = threadIdx.x; k < ST; k += blockDim.x) {  // forward rows, in (level, corner) order
+        int at = L.frow[k];
+        for (int n = 0; n < NE; ++n)
+            if (fw[k * NE + n] != 0.f) L.fent[at++] = make_int2(fidx[k * NE + n], __float_as_int(fw[k * NE + n]));
+    }
+    for (int d = warp; d < S; d += nw) {  // backward rows, in (target, level, corner) order
+        int at = L.brow[d];
+        for (int e0 = 0; e0 < N; e0 += 32) {
+            const int e = e0 + lane;
+            const bool hit = e < N && fidx[e] == d && fw[e] != 0.f;
             const unsigned m = __ballot_sync(0xffffffffu, hit);
-            if (hit) {
-                const int pos = at + __popc(m & ((1u << lane) - 1u));
-                L.ck[pos] = (short)(e / NE);
-                L.cw[pos] = L.fw[e];
-            }
+            if (hit) L.bent[at + __popc(m & ((1u << lane) - 1u))] = make_int2(e / NE, __float_as_int(fw[e]));
             at += __popc(m);
         }
     }
     __syncthreads();
 }
 
+__device__ __forceinline__ float sigmoid_ref(float x) { return 1.f / (1.f + expf(-x)); }
+
 // alpha_out[t] = sigmoid(accumulate(alpha_src[t])), feat_out[t] likewise
 // per channel (+ a bf16 copy; both with the channel stride CP >= C, padding
-// channels zero); warp per triangle.
+// channels zero).
 template <int C, int CP>
 __global__ void __launch_bounds__(kTabWarps * 32) accum_tab_kernel(int T, int lo, int hi, int S, int ST,
                                                                    const float* __restrict__ alpha_src,
@@ -215,36 +244,72 @@ __global__ void __launch_bounds__(kTabWarps * 32) accum_tab_kernel(int T, int lo
                                                                    float* __restrict__ feat_out,
                                                                    __nv_bfloat16* __restrict__ feat_bf16,
                                                                    uint4* __restrict__ tab_out) {
+    constexpr int G = 32 / CP;
+    static_assert(CP == 8 || CP == 16, "channel stride of the accumulated tables");
     extern __shared__ __align__(16) unsigned char tab_smem[];
-    const int NE = (hi - lo + 1) * 3;
-    const LatticeTab L = lattice_tab_at(tab_smem, ST * NE, S);
-    build_lattice_tab(L, lo, hi, ST, S);
+    const int N = ST * (hi - lo + 1) * 3;
+    const size_t tab_bytes = lattice_tab_bytes(N, S, ST);
+    const LatticeTab L = lattice_tab_at(tab_smem, N, S, ST);
+    build_lattice_tab(L, lo, hi, ST, S, tab_smem + tab_bytes);
     if (blockIdx.x == 0) {  // the tables for the adjoint kernel of this step
         const uint4* src = reinterpret_cast<const uint4*>(tab_smem);
-        for (int i = threadIdx.x; i < (int)(lattice_tab_bytes(ST * NE, S) / 16); i += blockDim.x) tab_out[i] = src[i];
+        for (int i = threadIdx.x; i < (int)(tab_bytes / 16); i += blockDim.x) tab_out[i] = src[i];
     }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float* sa = reinterpret_cast<float*>(tab_smem + lattice_tab_bytes(ST * NE, S)) + (size_t)warp * S * (C + 1);
-    float* sf = sa + S;
-    for (int t = blockIdx.x * kTabWarps + warp; t < T; t += gridDim.x * kTabWarps) {
-        for (int i = lane; i < S; i += 32) sa[i] = alpha_src[(size_t)t * S + i];
-        for (int i = lane; i < S * C; i += 32) sf[i] = feat_src[(size_t)t * S * C + i];
-        __syncwarp();
-        for (int k = lane; k < ST; k += 32) {
-            float acc = 0.f;
-            for (int n = 0; n < NE; ++n) acc = madd(acc, L.fw[k * NE + n], sa[L.fidx[k * NE + n]]);
-            alpha_out[(size_t)t * ST + k] = 1.f / (1.f + expf(-acc));
+    const int g = lane / CP, c = lane % CP;
+    const int M = S;
+    float* sf = reinterpret_cast<float*>(tab_smem + tab_bytes) + (size_t)warp * tab_stage_floats(M, CP);
+    float* sa = sf + 32 * M;  // [G][M + 1]
+    __syncthreads();  // the build's scratch is the staging area
+    for (int t0 = (blockIdx.x * kTabWarps + warp) * G; t0 < T; t0 += gridDim.x * kTabWarps * G) {
+        const int t = t0 + g;
+        const bool tv = t < T;
+        // eight loads in flight per lane before their stores
+        for (int s0 = 0; s0 < S; s0 += 8) {
+            float v[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                v[j] = (s0 + j < S && tv && c < C) ? __ldg(feat_src + ((size_t)t * S + s0 + j) * C + c) : 0.f;
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                if (s0 + j < S) sf[(s0 + j) * 32 + lane] = v[j];
         }
-        for (int e = lane; e < ST * CP; e += 32) {
-            const int k = e / CP, c = e % CP;
-            float v = 0.f;
-            if (c < C) {
-                float acc = 0.f;
-                for (int n = 0; n < NE; ++n) acc = madd(acc, L.fw[k * NE + n], sf[L.fidx[k * NE + n] * C + c]);
-                v = 1.f / (1.f + expf(-acc));
+        for (int i0 = 0; i0 < G * S; i0 += 128) {
+            float v[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int i = i0 + j * 32 + lane, gi = i / S;
+                v[j] = i < G * S && t0 + gi < T ? __ldg(alpha_src + (size_t)t0 * S + i) : 0.f;
             }
-            feat_out[(size_t)t * ST * CP + e] = v;
-            feat_bf16[(size_t)t * ST * CP + e] = __float2bfloat16_rn(v);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int i = i0 + j * 32 + lane, gi = i / S;
+                if (i < G * S) sa[gi * (M + 1) + (i - gi * S)] = v[j];
+            }
+        }
+        __syncwarp();
+        // opacity: lane (g, j) takes targets j, j + CP, ...
+        for (int k = c; k < ST; k += CP) {
+            float acc = 0.f;
+            for (int n = L.frow[k]; n < L.frow[k + 1]; ++n) {
+                const int2 e = L.fent[n];
+                acc = madd(acc, __int_as_float(e.y), sa[g * (M + 1) + e.x]);
+            }
+            if (tv) alpha_out[(size_t)t * ST + k] = sigmoid_ref(acc);
+        }
+        // features: lane (g, c) takes channel c of every target
+        for (int k = 0; k < ST; ++k) {
+            float acc = 0.f;
+#pragma unroll 4
+            for (int n = L.frow[k]; n < L.frow[k + 1]; ++n) {
+                const int2 e = L.fent[n];
+                acc = madd(acc, __int_as_float(e.y), sf[e.x * 32 + lane]);
+            }
+            const float v = c < C ? sigmoid_ref(acc) : 0.f;
+            if (tv) {
+                feat_out[((size_t)t * ST + k) * CP + c] = v;
+                feat_bf16[((size_t)t * ST + k) * CP + c] = __float2bfloat16_rn(v);
+            }
         }
         __syncwarp();
     }
@@ -260,52 +325,99 @@ __global__ void __launch_bounds__(kTabWarps * 32) accum_tab_backward_kernel(
     int T, int lo, int hi, int S, int ST, const float* __restrict__ alpha_sig, const float* __restrict__ alpha_grad,
     const float* __restrict__ feat_sig, const float* __restrict__ feat_grad, float* __restrict__ alpha_src_grad,
     float* __restrict__ feat_src_grad, const uint4* __restrict__ tab_in) {
+    constexpr int G = 32 / CP;
     extern __shared__ __align__(16) unsigned char tab_smem[];
-    const int NE = (hi - lo + 1) * 3;
-    const LatticeTab L = lattice_tab_at(tab_smem, ST * NE, S);
+    const int N = ST * (hi - lo + 1) * 3;
+    const size_t tab_bytes = lattice_tab_bytes(N, S, ST);
+    const LatticeTab L = lattice_tab_at(tab_smem, N, S, ST);
     {
         uint4* dst = reinterpret_cast<uint4*>(tab_smem);
-        for (int i = threadIdx.x; i < (int)(lattice_tab_bytes(ST * NE, S) / 16); i += blockDim.x) dst[i] = tab_in[i];
+        for (int i = threadIdx.x; i < (int)(tab_bytes / 16); i += blockDim.x) dst[i] = tab_in[i];
         __syncthreads();
     }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float* ga = reinterpret_cast<float*>(tab_smem + lattice_tab_bytes(ST * NE, S)) + (size_t)warp * ST * (C + 1);
-    float* gf = ga + ST;
-    for (int t = blockIdx.x * kTabWarps + warp; t < T; t += gridDim.x * kTabWarps) {
-        for (int i = lane; i < ST; i += 32) {
-            const float s = alpha_sig[(size_t)t * ST + i];
-            ga[i] = alpha_grad[(size_t)t * ST + i] * s * (1.f - s);
+    const int g = lane / CP, c = lane % CP;
+    const int M = ST;
+    float* gf = reinterpret_cast<float*>(tab_smem + tab_bytes) + (size_t)warp * tab_stage_floats(M, CP);
+    float* ga = gf + 32 * M;  // [G][M + 1]
+    for (int t0 = (blockIdx.x * kTabWarps + warp) * G; t0 < T; t0 += gridDim.x * kTabWarps * G) {
+        const int t = t0 + g;
+        const bool tv = t < T;
+        // eight (sigmoid, gradient) pairs in flight per lane before their stores
+        for (int k0 = 0; k0 < ST; k0 += 8) {
+            float sg[8], gr[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const bool in = k0 + j < ST && tv && c < C;
+                const size_t o = ((size_t)t * ST + k0 + j) * CP + c;
+                sg[j] = in ? __ldg(feat_sig + o) : 0.f;
+                gr[j] = in ? __ldg(feat_grad + o) : 0.f;
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                if (k0 + j < ST) gf[(k0 + j) * 32 + lane] = gr[j] * sg[j] * (1.f - sg[j]);
         }
-        for (int i = lane; i < ST * C; i += 32) {
-            const size_t o = ((size_t)t * ST + i / C) * CP + i % C;
-            const float s = feat_sig[o];
-            gf[i] = feat_grad[o] * s * (1.f - s);
+        for (int i0 = 0; i0 < G * ST; i0 += 128) {
+            float sg[4], gr[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int i = i0 + j * 32 + lane, gi = i / ST;
+                const bool in = i < G * ST && t0 + gi < T;
+                sg[j] = in ? __ldg(alpha_sig + (size_t)t0 * ST + i) : 0.f;
+                gr[j] = in ? __ldg(alpha_grad + (size_t)t0 * ST + i) : 0.f;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int i = i0 + j * 32 + lane, gi = i / ST;
+                if (i < G * ST) ga[gi * (M + 1) + (i - gi * ST)] = gr[j] * sg[j] * (1.f - sg[j]);
+            }
         }
         __syncwarp();
-        for (int d = lane; d < S; d += 32) {
+        for (int d = c; d < S; d += CP) {  // opacity: lane (g, j) takes sources j, j + CP, ...
             float v = 0.f;
-            for (int n = L.row[d]; n < L.row[d + 1]; ++n) v = fmaf(L.cw[n], ga[L.ck[n]], v);
-            alpha_src_grad[(size_t)t * S + d] = v;
+            for (int n = L.brow[d]; n < L.brow[d + 1]; ++n) {
+                const int2 e = L.bent[n];
+                v = fmaf(__int_as_float(e.y), ga[g * (M + 1) + e.x], v);
+            }
+            if (tv) alpha_src_grad[(size_t)t * S + d] = v;
         }
-        for (int o = lane; o < S * C; o += 32) {
-            const int d = o / C, c = o % C;
+        for (int d = 0; d < S; ++d) {  // features: lane (g, c) takes channel c of every source
             float v = 0.f;
-            for (int n = L.row[d]; n < L.row[d + 1]; ++n) v = fmaf(L.cw[n], gf[L.ck[n] * C + c], v);
-            feat_src_grad[(size_t)t * S * C + o] = v;
+#pragma unroll 4
+            for (int n = L.brow[d]; n < L.brow[d + 1]; ++n) {
+                const int2 e = L.bent[n];
+                v = fmaf(__int_as_float(e.y), gf[e.x * 32 + lane], v);
+            }
+            if (tv && c < C) feat_src_grad[((size_t)t * S + d) * C + c] = v;
         }
         __syncwarp();
     }
 }
 
-// Dynamic shared memory of the table kernels: tables + per-warp staging.
-static size_t lattice_tab_smem(int lo, int hi, int S, int ST, int C) {
+// Dynamic shared memory of the table kernels: tables + per-warp staging of
+// the sources (forward, which also holds the build's scratch) or of the
+// target gradients (backward).
+static size_t lattice_tab_smem(int lo, int hi, int S, int ST, int CP, bool backward) {
     const int N = ST * (hi - lo + 1) * 3;
-    return lattice_tab_bytes(N, S) + (size_t)kTabWarps * (size_t)(S > ST ? S : ST) * (C + 1) * 4;
+    return lattice_tab_bytes(N, S, ST) + (size_t)kTabWarps * tab_stage_floats(backward ? ST : S, CP) * 4;
 }
 
 // Whether the table kernels cover this configuration.
-static bool lattice_tab_fits(int lo, int hi, int S, int ST, int C) {
-    return ST * (hi - lo + 1) * 3 <= kTabMax && S <= kTabRows && lattice_tab_smem(lo, hi, S, ST, C) <= 48 * 1024;
+static bool lattice_tab_fits(int lo, int hi, int S, int ST, int CP) {
+    return ST * (hi - lo + 1) * 3 <= kTabMax && (CP == 8 || CP == 16) &&
+           lattice_tab_smem(lo, hi, S, ST, CP, false) <= kTabSmemMax;
+}
+
+// The table kernels' dynamic shared memory above the 48 KB default (one
+// record per kernel: the template argument is the kernel itself).
+template <auto Kernel>
+static int tab_smem_attr(size_t smem) {
+    static size_t set = 0;
+    if (smem > set) {
+        DS_CUDA(cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        set = smem;
+    }
+    return DS_OK;
 }
 
 // clip[b][v] = mvp[b] . (verts[v], 1)  (examples/utils.py:412-426)
@@ -651,7 +763,7 @@ static StepWs carve_step(void* ws, const ds_step_config& c, int num_tiles, int64
     w.l1 = reinterpret_cast<float*>(base + o); o += al((size_t)P * 4);
     w.tab = reinterpret_cast<uint4*>(base + o);
     o += al(lattice_tab_bytes(ST * (c.max_level - c.min_level + 1) * 3,
-                              (int)total_feats((uint32_t)c.min_level, (uint32_t)c.max_level)));
+                              (int)total_feats((uint32_t)c.min_level, (uint32_t)c.max_level), ST));
     // zeroed together each step: grad_pos .. loss_sum
     w.grad_pos = reinterpret_cast<double*>(base + o); o += al((size_t)c.B * c.V * 32);
     w.grad_alpha_acc = reinterpret_cast<float*>(base + o); o += al((size_t)c.T * ST * 4);
@@ -799,18 +911,22 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
 
     // prep: opacity and feature accumulation + sigmoid (side), projection (st)
     const unsigned tb = (unsigned)((c.T + kPrepWarps - 1) / kPrepWarps);
-    const bool tab = lattice_tab_fits(c.min_level, c.max_level, S, ST, c.C);
-    const size_t tsm = lattice_tab_smem(c.min_level, c.max_level, S, ST, c.C);
-    const int64_t tw = ((int64_t)c.T + kTabWarps - 1) / kTabWarps;
+    const bool tab = lattice_tab_fits(c.min_level, c.max_level, S, ST, CP);
+    const size_t tsm = lattice_tab_smem(c.min_level, c.max_level, S, ST, CP, false);
+    const size_t tsm_bwd = lattice_tab_smem(c.min_level, c.max_level, S, ST, CP, true);
+    const int64_t tw = ((int64_t)c.T + (32 / CP) * kTabWarps - 1) / ((32 / CP) * kTabWarps);  // CTAs of 32/CP triangles a warp
     const int64_t nsm = sm_count();
     const unsigned tgrid = (unsigned)(tw < nsm * 4 ? tw : nsm * 4);  // persistent: tables built once per CTA
     // the adjoint copies the tables instead of building them, so more CTAs pay
     const unsigned tgrid_bwd = (unsigned)(tw < nsm * 8 ? tw : nsm * 8);
     if (c.T > 0 && tab) {
 #define DSB_ACCUM_TAB(CC, CPP)                                                                                     \
-    accum_tab_kernel<CC, CPP><<<tgrid, kTabWarps * 32, tsm, sst>>>(c.T, c.min_level, c.max_level, S, ST, alpha_src, \
-                                                                   feat_src, w.alpha_acc, w.feat_acc, w.feat_bf16, \
-                                                                   w.tab)
+    do {                                                                                                           \
+        if ((rc = tab_smem_attr<accum_tab_kernel<CC, CPP>>(tsm))) return rc;                                       \
+        accum_tab_kernel<CC, CPP><<<tgrid, kTabWarps * 32, tsm, sst>>>(c.T, c.min_level, c.max_level, S, ST,       \
+                                                                       alpha_src, feat_src, w.alpha_acc,           \
+                                                                       w.feat_acc, w.feat_bf16, w.tab);            \
+    } while (0)
         if (c.C == 8) DSB_ACCUM_TAB(8, 8);
         else if (c.C == 7) DSB_ACCUM_TAB(7, 8);
         else DSB_ACCUM_TAB(16, 16);
@@ -876,9 +992,12 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     // adjoints of sigmoid + level accumulation, and of the projection
     if (c.T > 0 && tab) {
 #define DSB_ACCUM_TAB_BWD(CC, CPP)                                                                                 \
-    accum_tab_backward_kernel<CC, CPP><<<tgrid_bwd, kTabWarps * 32, tsm, st>>>(                                    \
-        c.T, c.min_level, c.max_level, S, ST, w.alpha_acc, w.grad_alpha_acc, w.feat_acc, w.grad_feat_acc,          \
-        grad_alpha_src, grad_feat_src, w.tab)
+    do {                                                                                                           \
+        if ((rc = tab_smem_attr<accum_tab_backward_kernel<CC, CPP>>(tsm_bwd))) return rc;                          \
+        accum_tab_backward_kernel<CC, CPP><<<tgrid_bwd, kTabWarps * 32, tsm_bwd, st>>>(                            \
+            c.T, c.min_level, c.max_level, S, ST, w.alpha_acc, w.grad_alpha_acc, w.feat_acc, w.grad_feat_acc,      \
+            grad_alpha_src, grad_feat_src, w.tab);                                                                 \
+    } while (0)
         if (c.C == 8) DSB_ACCUM_TAB_BWD(8, 8);
         else if (c.C == 7) DSB_ACCUM_TAB_BWD(7, 8);
         else DSB_ACCUM_TAB_BWD(16, 16);
