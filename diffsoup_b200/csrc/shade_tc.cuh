@@ -217,33 +217,70 @@ __global__ void __launch_bounds__(kTcThreads, 2) shade_tc_kernel(ShadeArgs a) {
     };
 
     const int64_t ntiles = (a.num_pixels + kTcThreads - 1) / kTcThreads;
+    // ---- the pixel front, one tile ahead: the next tile's rast entry is requested before this tile's
+    // first product, its feature samples and target after that product (their latency hides behind
+    // the remaining products), and they are interpolated when this tile is done ---------------------
+    auto issue_rast = [&](int64_t tl, float4& r) {
+        const int64_t q = tl * kTcThreads + tid;
+        r = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (tl < ntiles && q < a.num_pixels) r = reinterpret_cast<const float4*>(a.rast)[q];
+    };
+    auto issue_feat = [&](int64_t tl, const float4& r, uint4 (&u)[3][2], uint32_t (&ix)[3], float (&wg)[3],
+                          float (&tg)[3]) {
+        const int64_t q = tl * kTcThreads + tid;
+        const bool ok = tl < ntiles && q < a.num_pixels;
+        const int tt = (int)r.w - 1;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            ix[k] = 0u; wg[k] = 0.f; tg[k] = 0.f;
+            u[k][0] = u[k][1] = make_uint4(0u, 0u, 0u, 0u);
+        }
+        if (ok && tt >= 0) {
+            lattice_cell(r.x, r.y, (uint32_t)a.level, ix, wg);
+            const __nv_bfloat16* tf = a.feat + (size_t)tt * a.S * 16;
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+                    u[k][h] = __ldg(reinterpret_cast<const uint4*>(tf + (size_t)ix[k] * 16 + 8 * h));
+        }
+        if (ok) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) tg[c] = target_at(a, q, c);
+        }
+    };
+    float4 r_cur;
+    uint4 u_cur[3][2];
+    uint32_t ix_cur[3];
+    float wg_cur[3], tg_cur[3];
+    issue_rast(blockIdx.x, r_cur);
+    issue_feat(blockIdx.x, r_cur, u_cur, ix_cur, wg_cur, tg_cur);
     for (int64_t tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
-        // ---------------- pixel front: gather features, view direction ----------
+        // ---------------- pixel front: interpolated features, view direction ----------
         const int64_t p = tile * kTcThreads + tid;
         const bool valid = p < a.num_pixels;
-        float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (valid) r = reinterpret_cast<const float4*>(a.rast)[p];
+        const float4 r = r_cur;
         const int t = (int)r.w - 1;
         const bool mask = valid && t >= 0;
         float x[K::IN_REAL];
 #pragma unroll
         for (int c = 0; c < K::IN_REAL; ++c) x[c] = 0.f;
-        uint32_t idx[3] = {0, 0, 0};
-        float wgt[3] = {0.f, 0.f, 0.f};
+        uint32_t idx[3];
+        float wgt[3], tgt[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { idx[k] = ix_cur[k]; wgt[k] = wg_cur[k]; tgt[k] = tg_cur[k]; }
         if (mask) {
-            lattice_cell(r.x, r.y, (uint32_t)a.level, idx, wgt);
-            const __nv_bfloat16* tf = a.feat + (size_t)t * a.S * 16;
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
 #pragma unroll
-                for (int c = 0; c < 16; c += 8) {
-                    const uint4 u = __ldg(reinterpret_cast<const uint4*>(tf + (size_t)idx[k] * 16 + c));
+                for (int h = 0; h < 2; ++h) {
+                    const uint4 u = u_cur[k][h];
                     const __nv_bfloat162* h2 = reinterpret_cast<const __nv_bfloat162*>(&u);
 #pragma unroll
                     for (int j = 0; j < 4; ++j) {
                         const float2 f = __bfloat1622float2(h2[j]);
-                        x[c + 2 * j] = __fmaf_rn(wgt[k], f.x, x[c + 2 * j]);
-                        x[c + 2 * j + 1] = __fmaf_rn(wgt[k], f.y, x[c + 2 * j + 1]);
+                        x[8 * h + 2 * j] = __fmaf_rn(wgt[k], f.x, x[8 * h + 2 * j]);
+                        x[8 * h + 2 * j + 1] = __fmaf_rn(wgt[k], f.y, x[8 * h + 2 * j + 1]);
                     }
                 }
             }
@@ -258,11 +295,9 @@ __global__ void __launch_bounds__(kTcThreads, 2) shade_tc_kernel(ShadeArgs a) {
             view_direction(pix_ndc(px, vd.W), pix_ndc(py, vd.H), M, d);
             x[16] = d[0]; x[17] = d[1]; x[18] = d[2];
         }
-        float tgt[3] = {0.f, 0.f, 0.f};
-        if (valid) {
-#pragma unroll
-            for (int c = 0; c < 3; ++c) tgt[c] = target_at(a, p, c);
-        }
+        const int64_t next = tile + gridDim.x;
+        float4 r_next;
+        issue_rast(next, r_next);
         if (!__syncthreads_or(mask)) {  // no covered pixel in the tile: background colour 1, no MLP and no gradients
             if (valid) {
                 float l1 = 0.f;
@@ -276,6 +311,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) shade_tc_kernel(ShadeArgs a) {
                 }
                 a.l1[p] = l1;
             }
+            r_cur = r_next;
+            issue_feat(next, r_cur, u_cur, ix_cur, wg_cur, tg_cur);
             continue;
         }
         {  // [X | 1] row
@@ -321,6 +358,8 @@ __global__ void __launch_bounds__(kTcThreads, 2) shade_tc_kernel(ShadeArgs a) {
             st_row16(sm.RA, 8, one);
             st_row16(sm.RA, 9, zero);
         }
+        r_cur = r_next;
+        issue_feat(next, r_cur, u_cur, ix_cur, wg_cur, tg_cur);  // the next tile's samples, in flight from here
         // Z2 = H1 W1^T -> R2
         if (!stage([&] {
                 for (int ks = 0; ks < 4; ++ks)

@@ -110,7 +110,9 @@ __global__ void __launch_bounds__(kPrepWarps * 32) accum_sigmoid_backward_kernel
 // ---------------------------------------------------------------------------
 // Table-driven level accumulation.  The interpolation from the levels'
 // lattices to the target lattice is the same sparse map for every triangle,
-// so each CTA builds it once in shared memory: the forward table lists, per
+// so each CTA of the forward kernel builds it in shared memory (the grid is
+// one wave of persistent CTAs) and the adjoint copies the forward's: the
+// forward table lists, per
 // target sample, its (source sample, weight) pairs in level-then-corner
 // order (the summation order of accum_sigmoid_kernel), and the backward
 // table is the same map grouped by source sample, which turns the adjoint
@@ -233,6 +235,16 @@ __device__ void build_lattice_tab(const LatticeTab& L, int lo, int hi, int ST, i
 
 __device__ __forceinline__ float sigmoid_ref(float x) { return 1.f / (1.f + expf(-x)); }
 
+// 4-byte global -> shared copy that bypasses registers (cp.async), and the wait for all of a thread's.
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+}
+
 // alpha_out[t] = sigmoid(accumulate(alpha_src[t])), feat_out[t] likewise
 // per channel (+ a bf16 copy; both with the channel stride CP >= C, padding
 // channels zero).
@@ -250,7 +262,7 @@ __global__ void __launch_bounds__(kTabWarps * 32) accum_tab_kernel(int T, int lo
     const int N = ST * (hi - lo + 1) * 3;
     const size_t tab_bytes = lattice_tab_bytes(N, S, ST);
     const LatticeTab L = lattice_tab_at(tab_smem, N, S, ST);
-    build_lattice_tab(L, lo, hi, ST, S, tab_smem + tab_bytes);
+    build_lattice_tab(L, lo, hi, ST, S, tab_smem + tab_bytes);  // the scratch is the staging area
     if (blockIdx.x == 0) {  // the tables for the adjoint kernel of this step
         const uint4* src = reinterpret_cast<const uint4*>(tab_smem);
         for (int i = threadIdx.x; i < (int)(tab_bytes / 16); i += blockDim.x) tab_out[i] = src[i];
@@ -260,33 +272,22 @@ __global__ void __launch_bounds__(kTabWarps * 32) accum_tab_kernel(int T, int lo
     const int M = S;
     float* sf = reinterpret_cast<float*>(tab_smem + tab_bytes) + (size_t)warp * tab_stage_floats(M, CP);
     float* sa = sf + 32 * M;  // [G][M + 1]
-    __syncthreads();  // the build's scratch is the staging area
     for (int t0 = (blockIdx.x * kTabWarps + warp) * G; t0 < T; t0 += gridDim.x * kTabWarps * G) {
         const int t = t0 + g;
         const bool tv = t < T;
-        // eight loads in flight per lane before their stores
-        for (int s0 = 0; s0 < S; s0 += 8) {
-            float v[8];
-#pragma unroll
-            for (int j = 0; j < 8; ++j)
-                v[j] = (s0 + j < S && tv && c < C) ? __ldg(feat_src + ((size_t)t * S + s0 + j) * C + c) : 0.f;
-#pragma unroll
-            for (int j = 0; j < 8; ++j)
-                if (s0 + j < S) sf[(s0 + j) * 32 + lane] = v[j];
+        // every sample copied without registers (cp.async), then one wait: one round trip a pass
+        for (int s = 0; s < S; ++s) {
+            float* dst = sf + s * 32 + lane;
+            if (tv && c < C) cp_async4(dst, feat_src + ((size_t)t * S + s) * C + c);
+            else *dst = 0.f;
         }
-        for (int i0 = 0; i0 < G * S; i0 += 128) {
-            float v[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int i = i0 + j * 32 + lane, gi = i / S;
-                v[j] = i < G * S && t0 + gi < T ? __ldg(alpha_src + (size_t)t0 * S + i) : 0.f;
-            }
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int i = i0 + j * 32 + lane, gi = i / S;
-                if (i < G * S) sa[gi * (M + 1) + (i - gi * S)] = v[j];
-            }
+        for (int i = lane; i < G * S; i += 32) {
+            const int gi = i / S;
+            float* dst = sa + gi * (M + 1) + (i - gi * S);
+            if (t0 + gi < T) cp_async4(dst, alpha_src + (size_t)t0 * S + i);
+            else *dst = 0.f;
         }
+        cp_async_wait_all();
         __syncwarp();
         // opacity: lane (g, j) takes targets j, j + CP, ...
         for (int k = c; k < ST; k += CP) {
@@ -316,9 +317,7 @@ __global__ void __launch_bounds__(kTabWarps * 32) accum_tab_kernel(int T, int lo
 }
 
 // Adjoint of accum_tab_kernel: grad_src[t][d] = sum over the targets k that
-// read d of w * grad_out[t][k] * s (1 - s); a gather, written once.  The
-// tables are the ones the forward kernel of the step built (copied, not
-// rebuilt: this kernel sits on the step's critical path).  feat_sig and
+// read d of w * grad_out[t][k] * s (1 - s); a gather, written once.  feat_sig and
 // feat_grad have the channel stride CP, feat_src_grad the stride C.
 template <int C, int CP>
 __global__ void __launch_bounds__(kTabWarps * 32) accum_tab_backward_kernel(
@@ -343,18 +342,18 @@ __global__ void __launch_bounds__(kTabWarps * 32) accum_tab_backward_kernel(
     for (int t0 = (blockIdx.x * kTabWarps + warp) * G; t0 < T; t0 += gridDim.x * kTabWarps * G) {
         const int t = t0 + g;
         const bool tv = t < T;
-        // eight (sigmoid, gradient) pairs in flight per lane before their stores
-        for (int k0 = 0; k0 < ST; k0 += 8) {
-            float sg[8], gr[8];
+        // sixteen (sigmoid, gradient) pairs in flight per lane before their stores
+        for (int k0 = 0; k0 < ST; k0 += 16) {
+            float sg[16], gr[16];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
+            for (int j = 0; j < 16; ++j) {
                 const bool in = k0 + j < ST && tv && c < C;
                 const size_t o = ((size_t)t * ST + k0 + j) * CP + c;
                 sg[j] = in ? __ldg(feat_sig + o) : 0.f;
                 gr[j] = in ? __ldg(feat_grad + o) : 0.f;
             }
 #pragma unroll
-            for (int j = 0; j < 8; ++j)
+            for (int j = 0; j < 16; ++j)
                 if (k0 + j < ST) gf[(k0 + j) * 32 + lane] = gr[j] * sg[j] * (1.f - sg[j]);
         }
         for (int i0 = 0; i0 < G * ST; i0 += 128) {
@@ -395,7 +394,7 @@ __global__ void __launch_bounds__(kTabWarps * 32) accum_tab_backward_kernel(
 }
 
 // Dynamic shared memory of the table kernels: tables + per-warp staging of
-// the sources (forward, which also holds the build's scratch) or of the
+// the sources (forward) or of the
 // target gradients (backward).
 static size_t lattice_tab_smem(int lo, int hi, int S, int ST, int CP, bool backward) {
     const int N = ST * (hi - lo + 1) * 3;
@@ -408,15 +407,20 @@ static bool lattice_tab_fits(int lo, int hi, int S, int ST, int CP) {
            lattice_tab_smem(lo, hi, S, ST, CP, false) <= kTabSmemMax;
 }
 
-// The table kernels' dynamic shared memory above the 48 KB default (one
-// record per kernel: the template argument is the kernel itself).
+// The table kernels' dynamic shared memory above the 48 KB default, and
+// the CTAs of that size one SM holds (one record per kernel: the template
+// argument is the kernel itself).
 template <auto Kernel>
-static int tab_smem_attr(size_t smem) {
+static int tab_smem_attr(size_t smem, int* per_sm = nullptr) {
     static size_t set = 0;
-    if (smem > set) {
+    static int fit = 1;
+    if (smem != set) {
         DS_CUDA(cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        DS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, Kernel, kTabWarps * 32, smem));
+        if (fit < 1) fit = 1;
         set = smem;
     }
+    if (per_sm) *per_sm = fit;
     return DS_OK;
 }
 
@@ -916,13 +920,15 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     const size_t tsm_bwd = lattice_tab_smem(c.min_level, c.max_level, S, ST, CP, true);
     const int64_t tw = ((int64_t)c.T + (32 / CP) * kTabWarps - 1) / ((32 / CP) * kTabWarps);  // CTAs of 32/CP triangles a warp
     const int64_t nsm = sm_count();
-    const unsigned tgrid = (unsigned)(tw < nsm * 4 ? tw : nsm * 4);  // persistent: tables built once per CTA
-    // the adjoint copies the tables instead of building them, so more CTAs pay
+    // the adjoint: persistent CTAs, each copying the forward's tables once
     const unsigned tgrid_bwd = (unsigned)(tw < nsm * 8 ? tw : nsm * 8);
     if (c.T > 0 && tab) {
 #define DSB_ACCUM_TAB(CC, CPP)                                                                                     \
     do {                                                                                                           \
-        if ((rc = tab_smem_attr<accum_tab_kernel<CC, CPP>>(tsm))) return rc;                                       \
+        int per_sm = 1;                                                                                            \
+        if ((rc = tab_smem_attr<accum_tab_kernel<CC, CPP>>(tsm, &per_sm))) return rc;                              \
+        /* one wave of persistent CTAs, each building the tables once */                                           \
+        const unsigned tgrid = (unsigned)(tw < nsm * per_sm ? tw : nsm * per_sm);                                  \
         accum_tab_kernel<CC, CPP><<<tgrid, kTabWarps * 32, tsm, sst>>>(c.T, c.min_level, c.max_level, S, ST,       \
                                                                        alpha_src, feat_src, w.alpha_acc,           \
                                                                        w.feat_acc, w.feat_bf16, w.tab);            \
