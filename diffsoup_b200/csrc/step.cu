@@ -982,40 +982,52 @@ int ds_train_step(const ds_step_config* cfg, const ds_view_desc* views, int num_
     }
     if (rc || (rc = mark(4, st))) return rc;
 
+    // adjoints of sigmoid + level accumulation: they read the opacity and feature gradients, not the
+    // vertex gradients, so with a side stream they run there after the opacity pass, beside the edge
+    // gradients
+    auto accum_backward = [&](cudaStream_t s) -> int {
+        int r = DS_OK;
+        if (c.T > 0 && tab) {
+#define DSB_ACCUM_TAB_BWD(CC, CPP)                                                                                 \
+    do {                                                                                                           \
+        if ((r = tab_smem_attr<accum_tab_backward_kernel<CC, CPP>>(tsm_bwd))) return r;                            \
+        accum_tab_backward_kernel<CC, CPP><<<tgrid_bwd, kTabWarps * 32, tsm_bwd, s>>>(                             \
+            c.T, c.min_level, c.max_level, S, ST, w.alpha_acc, w.grad_alpha_acc, w.feat_acc, w.grad_feat_acc,      \
+            grad_alpha_src, grad_feat_src, w.tab);                                                                 \
+    } while (0)
+            if (c.C == 8) DSB_ACCUM_TAB_BWD(8, 8);
+            else if (c.C == 7) DSB_ACCUM_TAB_BWD(7, 8);
+            else DSB_ACCUM_TAB_BWD(16, 16);
+#undef DSB_ACCUM_TAB_BWD
+        } else if (c.T > 0) {
+            accum_sigmoid_backward_kernel<<<tb, kPrepWarps * 32, 0, s>>>(c.T, c.min_level, c.max_level, c.max_level,
+                                                                         S, ST, 1, 1, w.alpha_acc, w.grad_alpha_acc,
+                                                                         grad_alpha_src);
+            accum_sigmoid_backward_kernel<<<tb, kPrepWarps * 32, 0, s>>>(c.T, c.min_level, c.max_level, c.max_level,
+                                                                         S, ST, c.C, CP, w.feat_acc,
+                                                                         w.grad_feat_acc, grad_feat_src);
+        }
+        return r;
+    };
+
     // opacity auxiliary gradient (scaled by 1/numel(colour), rasterize.py:183-195), on the side
     // stream beside the edge gradients
     if (side && (rc = fork_to(side, 1, st))) return rc;
     rc = tiles_aux_impl(c.B, views, num_tiles, c.T, c.max_level, ST, w.alpha_acc, w.l1, rast, a.inv_n,
                         w.grad_alpha_acc, w.tiles, list_capacity, rs, sst, block_shape_log2(c));
-    if (rc || (rc = mark(5, st))) return rc;
+    if (rc) return rc;
+    if (side && (rc = accum_backward(sst))) return rc;
+    if ((rc = mark(5, st))) return rc;
 
     // edge gradients to clip-space positions
     edge_step_kernel<<<(unsigned)num_tiles, kEdgeThreads, 0, st>>>(
         c.B, views, c.V, c.T, tiles_tables(w.tiles, c.B, c.T, num_tiles, list_capacity), tri, a.color, w.grad_color,
         rast, w.grad_pos);
     if ((rc = mark(6, st))) return rc;
-    if (side && (rc = join_from(side, 1, st))) return rc;  // the adjoints read the opacity gradients
-    // adjoints of sigmoid + level accumulation, and of the projection
-    if (c.T > 0 && tab) {
-#define DSB_ACCUM_TAB_BWD(CC, CPP)                                                                                 \
-    do {                                                                                                           \
-        if ((rc = tab_smem_attr<accum_tab_backward_kernel<CC, CPP>>(tsm_bwd))) return rc;                          \
-        accum_tab_backward_kernel<CC, CPP><<<tgrid_bwd, kTabWarps * 32, tsm_bwd, st>>>(                            \
-            c.T, c.min_level, c.max_level, S, ST, w.alpha_acc, w.grad_alpha_acc, w.feat_acc, w.grad_feat_acc,      \
-            grad_alpha_src, grad_feat_src, w.tab);                                                                 \
-    } while (0)
-        if (c.C == 8) DSB_ACCUM_TAB_BWD(8, 8);
-        else if (c.C == 7) DSB_ACCUM_TAB_BWD(7, 8);
-        else DSB_ACCUM_TAB_BWD(16, 16);
-#undef DSB_ACCUM_TAB_BWD
-    } else if (c.T > 0) {
-        accum_sigmoid_backward_kernel<<<tb, kPrepWarps * 32, 0, st>>>(c.T, c.min_level, c.max_level, c.max_level, S,
-                                                                      ST, 1, 1, w.alpha_acc, w.grad_alpha_acc,
-                                                                      grad_alpha_src);
-        accum_sigmoid_backward_kernel<<<tb, kPrepWarps * 32, 0, st>>>(c.T, c.min_level, c.max_level, c.max_level, S,
-                                                                      ST, c.C, CP, w.feat_acc, w.grad_feat_acc,
-                                                                      grad_feat_src);
-    }
+    if (side && (rc = join_from(side, 1, st))) return rc;
+    // (one stream: the phases in order, so that the profiling events time each alone)
+    if (!side && (rc = accum_backward(st))) return rc;
+    // adjoint of the projection
     if (c.V > 0) project_backward_kernel<<<blocks_for(c.V), kThreads, 0, st>>>(c.B, c.V, mvp, w.grad_pos, grad_verts);
     finish_kernel<<<1, 32, 0, st>>>(w.loss_sum, a.inv_n, loss, c.stochastic ? rng : nullptr, w.rec_counters, status);
     if ((rc = mark(7, st))) return rc;
