@@ -64,9 +64,18 @@ class Ref:
     """The reference's Python-level composites (rasterize.py, multires.py) over
     one build of its CUDA sources."""
 
-    def __init__(self, build: str = "fma"):
+    def __init__(self, build: str = "fma", sync: bool = True):
+        """sync=False leaves out the device synchronisation after each launch
+        (kept where the reference itself reads a count back), for timing the
+        reference's path as its Python layer runs it: the launchers and torch
+        share the legacy default stream, so the order holds without it."""
         self.build = build
         self.L = lib(build)
+        self.sync = sync
+
+    def _done(self) -> None:
+        if self.sync:
+            _sync(self.build)
 
     def compute_fragments(self, H: int, W: int, pos: torch.Tensor, tri: torch.Tensor) -> Tuple[torch.Tensor, torch.Tensor]:
         """rasterize.py:40-76"""
@@ -84,7 +93,7 @@ class Ref:
         po = torch.empty_like(fpix)
         ao = torch.empty_like(fattr)
         k = self.L.dsref_filter_valid_fragments(n, _p(fpix), _p(fattr), _p(po), _p(ao)) if n else 0
-        _sync(self.build)
+        self._done()
         self.last_rects, self.last_prefix = rects, prefix
         return po[:k].contiguous(), ao[:k].contiguous()
 
@@ -92,7 +101,7 @@ class Ref:
         out = torch.zeros(frag_attrs.shape[0], dtype=torch.float32, device=frag_attrs.device)
         if frag_attrs.shape[0]:
             self.L.dsref_multires_triangle_alpha(frag_attrs.shape[0], _p(frag_attrs), lo, hi, _p(alpha_src_2d), _p(out))
-        _sync(self.build)
+        self._done()
         return out
 
     def depth_test(self, B, H, W, frag_pix, frag_attrs, frag_alpha, thresh):
@@ -100,7 +109,7 @@ class Ref:
         if frag_pix.shape[0]:
             self.L.dsref_depth_test(B, H, W, frag_pix.shape[0], _p(frag_pix), _p(frag_attrs), _p(frag_alpha),
                                     _p(thresh), _p(rast))
-        _sync(self.build)
+        self._done()
         return rast
 
     def rasterize_alpha(self, H, W, pos, tri, level, alpha_src, thresh_fn=None):
@@ -118,21 +127,21 @@ class Ref:
         B, H, W, _ = rast.shape
         out = torch.zeros(B, H, W, feat.shape[2], dtype=torch.float32, device=rast.device)
         self.L.dsref_multires_triangle_color(B, H, W, _p(rast), lo, hi, feat.shape[2], _p(feat), _p(out))
-        _sync(self.build)
+        self._done()
         return out
 
     def multires_color_backward(self, rast, lo, hi, feat_shape, grad_out):
         B, H, W, _ = rast.shape
         g = torch.zeros(feat_shape, dtype=torch.float32, device=rast.device)
         self.L.dsref_backward_multires_triangle_color(B, H, W, _p(rast), lo, hi, feat_shape[2], _p(g), _p(grad_out))
-        _sync(self.build)
+        self._done()
         return g
 
     def encode_sh2(self, rast, inv_mvp):
         B, H, W, _ = rast.shape
         enc = torch.zeros(B, H, W, 9, dtype=torch.float32, device=rast.device)
         self.L.dsref_encode_view_dir_sh2(B, H, W, _p(rast), _p(inv_mvp), _p(enc))
-        _sync(self.build)
+        self._done()
         return enc
 
     def edge_grad(self, color, grad_color, rast, pos, tri):
@@ -140,7 +149,7 @@ class Ref:
         gp = torch.zeros_like(pos)
         self.L.dsref_backward_edge_grad(B, H, W, Cd, _p(color), _p(grad_color), _p(rast), pos.shape[1], _p(pos),
                                         _p(gp), _p(tri))
-        _sync(self.build)
+        self._done()
         return gp
 
     def opacity_aux(self, color, target, rast, pos, tri, level, alpha_src_2d):
@@ -156,19 +165,19 @@ class Ref:
         gas = torch.zeros_like(alpha_src_2d)
         if nf:
             self.L.dsref_backward_multires_triangle_alpha(nf, _p(fattr), level, level, _p(gas), _p(gfa))
-        _sync(self.build)
+        self._done()
         return gas, fpix, fattr, alpha, gfa
 
     def accumulate_forward(self, lo, hi, target, feat, S_target):
         T, _, Cd = feat.shape
         out = torch.zeros(T, S_target, Cd, dtype=torch.float32, device=feat.device)
         self.L.dsref_accumulate_to_level_forward(T, lo, hi, target, Cd, _p(feat), _p(out))
-        _sync(self.build)
+        self._done()
         return out
 
     def accumulate_backward(self, lo, hi, target, feat_shape, grad_out):
         T, _, Cd = feat_shape
         g = torch.zeros(feat_shape, dtype=torch.float32, device=grad_out.device)
         self.L.dsref_accumulate_to_level_backward(T, lo, hi, target, Cd, _p(g), _p(grad_out))
-        _sync(self.build)
+        self._done()
         return g
