@@ -495,7 +495,22 @@ struct WarpStage {
     TriVerts v[32];
     TriBox box[32];
     int t[32];
+    unsigned lanes[32];  // lanes of the block whose (valid) pixel lies inside the candidate's rect
 };
+
+// Lanes of the block whose pixel lies inside the pixel rect r (lane l =
+// pixel (l mod bw, l div bw) of the block).
+__device__ __forceinline__ unsigned rect_lanes(const TriBox& r, const BlockGeom& g) {
+    const int cx0 = max((int)r.x0 - g.wx0, 0), cx1 = min((int)r.x1 - g.wx0, g.bw);
+    const int cy0 = max((int)r.y0 - g.wy0, 0), cy1 = min((int)r.y1 - g.wy0, g.bh);
+    if (cx0 >= cx1 || cy0 >= cy1) return 0u;
+    const unsigned row = ((1u << cx1) - 1u) & ~((1u << cx0) - 1u);  // cx1 <= bw <= 16
+    // one bit per block row, at the row's first lane: 0xffffffff / (2^bw - 1)
+    const unsigned rows = g.bw == 8 ? 0x01010101u : (g.bw == 16 ? 0x00010001u : 0x11111111u);
+    const int hi = cy1 * g.bw;  // <= 32
+    const unsigned keep = (hi >= 32 ? ~0u : (1u << hi) - 1u) & ~((1u << (cy0 * g.bw)) - 1u);
+    return row * (rows & keep);  // the row bits repeated on the kept rows (no carries)
+}
 
 // Loads entries [g0, g0+32) of the work item's range, keeps those whose box
 // meets the block, whose depth bound passes `zcut` (zlo <= zcut) and whose
@@ -534,11 +549,13 @@ __device__ __forceinline__ int stage_group(const BlockGeom& g, int64_t g0, const
         c = !edges_reject_block(edges[ri], xa, xb, ya, yb);
     }
     const unsigned mask = __ballot_sync(0xffffffffu, c);
+    const unsigned valid = __ballot_sync(0xffffffffu, g.valid);
     if (c) {
         const int k = __popc(mask & ((1u << lane) - 1u));
         st.v[k] = verts[ri];
         st.box[k] = bx;
         st.t[k] = ri - g.b * T;
+        st.lanes[k] = rect_lanes(bx, g) & valid;
     }
     __syncwarp();
     return __popc(mask);
@@ -665,8 +682,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, DSB_RASTER_MIN_CTAS) raster
                 // lanes inside the rect whose winner does not lie in front of the triangle: zlo's
                 // margin exceeds the rounding of z + 2, so with zlo > bz every fragment's depth key
                 // lies strictly behind the winner's (neither a winner nor a record)
-                const bool near = g.valid && g.px >= r.x0 && g.px < r.x1 && g.py >= r.y0 && g.py < r.y1 &&
-                                  !(best != ~0ull && r.zlo > bz);
+                const bool near = ((st.lanes[k] >> lane) & 1u) && !(best != ~0ull && r.zlo > bz);
                 if (!__any_sync(0xffffffffu, near)) continue;  // warp-uniform
                 float A0, A1, A2, A;
                 edge_terms(ndc_y, ndc_x, p0, p1, p2, A0, A1, A2, A);
@@ -858,8 +874,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) aux_kernel(
                 const int t = st.t[k];
                 const float4 p0 = st.v[k].p0, p1 = st.v[k].p1, p2 = st.v[k].p2;
                 // lanes inside the rect whose surface does not lie in front of the triangle
-                const bool near = g.valid && g.px >= r.x0 && g.px < r.x1 && g.py >= r.y0 && g.py < r.y1 &&
-                                  !(tp >= 0 && r.zlo > zp);
+                const bool near = ((st.lanes[k] >> lane) & 1u) && !(tp >= 0 && r.zlo > zp);
                 if (!__any_sync(0xffffffffu, near)) continue;  // warp-uniform
                 float A0, A1, A2, A;
                 edge_terms(ndc_y, ndc_x, p0, p1, p2, A0, A1, A2, A);
