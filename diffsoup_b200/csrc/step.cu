@@ -175,7 +175,7 @@ __device__ inline void tab_scan(int* rows, int n) {
     }
 }
 
-// Builds the tables; `scratch` holds N ints and N floats during the build.
+// Builds the tables; `scratch` holds N ints, N floats and S ints during the build.
 __device__ void build_lattice_tab(const LatticeTab& L, int lo, int hi, int ST, int S, unsigned char* scratch) {
     const int NL = hi - lo + 1, NE = NL * 3, N = ST * NE;
     int* fidx = reinterpret_cast<int*>(scratch);
@@ -203,14 +203,10 @@ __device__ void build_lattice_tab(const LatticeTab& L, int lo, int hi, int ST, i
         L.frow[k + 1] = cnt;
     }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    for (int d = warp; d < S; d += nw) {  // backward row lengths
-        int cnt = 0;
-        for (int e0 = 0; e0 < N; e0 += 32) {
-            const int e = e0 + lane;
-            cnt += __popc(__ballot_sync(0xffffffffu, e < N && fidx[e] == d && fw[e] != 0.f));
-        }
-        if (lane == 0) L.brow[d + 1] = cnt;
-    }
+    for (int d = threadIdx.x; d < S; d += blockDim.x) L.brow[d + 1] = 0;  // backward row lengths
+    __syncthreads();
+    for (int e = threadIdx.x; e < N; e += blockDim.x)
+        if (fw[e] != 0.f) atomicAdd(&L.brow[fidx[e] + 1], 1);
     __syncthreads();
     if (warp == 0) tab_scan(L.frow, ST);
     if (warp == 1 % nw) tab_scan(L.brow, S);
@@ -220,14 +216,24 @@ __device__ void build_lattice_tab(const LatticeTab& L, int lo, int hi, int ST, i
         for (int n = 0; n < NE; ++n)
             if (fw[k * NE + n] != 0.f) L.fent[at++] = make_int2(fidx[k * NE + n], __float_as_int(fw[k * NE + n]));
     }
-    for (int d = warp; d < S; d += nw) {  // backward rows, in (target, level, corner) order
-        int at = L.brow[d];
+    if (warp == nw - 1) {  // backward rows, in (target, level, corner) order: one warp walks the pairs
+        int* cursor = reinterpret_cast<int*>(fw + N);  // per source: the next free slot of its row
+        for (int d = lane; d < S; d += 32) cursor[d] = L.brow[d];
+        __syncwarp();
         for (int e0 = 0; e0 < N; e0 += 32) {
             const int e = e0 + lane;
-            const bool hit = e < N && fidx[e] == d && fw[e] != 0.f;
-            const unsigned m = __ballot_sync(0xffffffffu, hit);
-            if (hit) L.bent[at + __popc(m & ((1u << lane) - 1u))] = make_int2(e / NE, __float_as_int(fw[e]));
-            at += __popc(m);
+            const bool hit = e < N && fw[e] != 0.f;
+            const int d = hit ? fidx[e] : -1;
+            const unsigned peers = __match_any_sync(0xffffffffu, d);  // the lanes with this source
+            const int leader = __ffs(peers) - 1;
+            int base = 0;
+            if (hit && lane == leader) {
+                base = cursor[d];
+                cursor[d] = base + __popc(peers);
+            }
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (hit) L.bent[base + __popc(peers & ((1u << lane) - 1u))] = make_int2(e / NE, __float_as_int(fw[e]));
+            __syncwarp();
         }
     }
     __syncthreads();
