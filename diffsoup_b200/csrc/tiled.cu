@@ -660,10 +660,15 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, DSB_RASTER_MIN_CTAS) raster
     const int items = num_tiles * kBlocksPerTile;
     for (int item = warp_next(work); item < items; item = warp_next(work)) {
         const BlockGeom g = block_geometry(item, B, views, T, offsets, sorted, capacity, bwl);
+        if (g.begin >= g.end) {  // no candidate: background (a quarter to a third of the blocks)
+            if (g.valid) reinterpret_cast<float4*>(rast)[g.pix] = make_float4(0.f, 0.f, 0.f, 0.f);
+            continue;
+        }
         const float ndc_x = pix_ndc(g.px, g.W), ndc_y = pix_ndc(g.py, g.H);
         const PhiloxPixel php = philox_pixel(seed, iter, (uint32_t)g.b, (uint32_t)(g.py * g.W + g.px));
         unsigned long long best = ~0ull;
         float bb0 = 0.f, bb1 = 0.f, bz = 0.f;
+        float bz_cut = INFINITY;  // the winner's depth, +inf while the lane has none
         int nrec = 0;
         // max over the warp of the lanes' winning depth (+inf while a valid lane has none)
         float warp_far = warp_max(g.valid ? INFINITY : -INFINITY);
@@ -682,7 +687,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, DSB_RASTER_MIN_CTAS) raster
                 // lanes inside the rect whose winner does not lie in front of the triangle: zlo's
                 // margin exceeds the rounding of z + 2, so with zlo > bz every fragment's depth key
                 // lies strictly behind the winner's (neither a winner nor a record)
-                const bool near = ((st.lanes[k] >> lane) & 1u) && !(best != ~0ull && r.zlo > bz);
+                const bool near = ((st.lanes[k] >> lane) & 1u) && !(r.zlo > bz_cut);
                 if (!__any_sync(0xffffffffu, near)) continue;  // warp-uniform
                 float A0, A1, A2, A;
                 edge_terms(ndc_y, ndc_x, p0, p1, p2, A0, A1, A2, A);
@@ -710,7 +715,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32, DSB_RASTER_MIN_CTAS) raster
                                                           ? alpha >= 1.f || !(alpha < philox_uniform_tri(php, seed, t))
                                                           : !(alpha < thr_const);
                                     if (pass) {
-                                        best = key; bb0 = b0; bb1 = b1; bz = depth;
+                                        best = key; bb0 = b0; bb1 = b1; bz = depth; bz_cut = depth;
                                         improved = true;
                                     }
                                 }
