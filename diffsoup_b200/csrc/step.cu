@@ -499,6 +499,9 @@ __global__ void __launch_bounds__(kEdgeThreads, DSB_EDGE_MIN_CTAS) edge_step_ker
     double* __restrict__ grad_pos) {
     __shared__ EdgeHalo h;
     const int tile = blockIdx.x;
+    // no triangle may cover a pixel centre of the tile (its list is empty): every pixel is background,
+    // and background pixels contribute nothing as the centre of a pair
+    if (tab.offsets[tile] == tab.offsets[tile + 1]) return;
     const int b = tile_view(views, B, tile);
     const ds_view_desc vd = views[b];
     const int tl = tile - vd.tile_base;

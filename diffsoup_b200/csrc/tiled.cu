@@ -1033,7 +1033,7 @@ static int aux_launch(int B, const ds_view_desc* views, int num_tiles, int T, in
 
 TileTables tiles_tables(void* workspace, int B, int T, int num_tiles, int64_t list_capacity) {
     const TileWs w = carve(workspace, B, T, num_tiles, list_capacity, nullptr);
-    return TileTables{w.boxes, w.verts, w.ndc};
+    return TileTables{w.boxes, w.verts, w.ndc, w.offsets};
 }
 
 int tiles_aux_impl(int B, const ds_view_desc* views, int num_tiles, int T, int level, int S, const float* alpha_src,

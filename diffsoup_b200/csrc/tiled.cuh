@@ -35,6 +35,7 @@ struct TileTables {
     const TriBox* boxes;
     const TriVerts* verts;
     const TriNdc* ndc;
+    const int64_t* offsets;  // [num_tiles + 1] list ranges: a tile whose range is empty has no covered pixel
 };
 
 TileTables tiles_tables(void* workspace, int B, int T, int num_tiles, int64_t list_capacity);
