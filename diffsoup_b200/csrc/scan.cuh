@@ -2,7 +2,8 @@
 //
 // Three launches, no host synchronisation (graph-capturable): block sums,
 // one-block scan of the block sums, and a rescan that adds each block's
-// offset.  Sums are carried in int64 so totals never wrap.
+// offset; short scans in one launch (scan_one_cta_kernel).  Sums are carried
+// in int64 so totals never wrap.
 #pragma once
 
 #include "common.cuh"
@@ -108,6 +109,51 @@ int device_scan(const In* in, int64_t n, Out* out, bool inclusive, void* ws, cud
     scan_partials_kernel<<<1, kScanThreads, 0, st>>>(partials, nb);
     scan_apply_kernel<In, Out><<<(unsigned)nb, kScanThreads, 0, st>>>(in, n, partials, out, inclusive);
     return check_launch("device_scan");
+}
+
+// Short scans in one launch: a single CTA of kScanOneThreads threads, each
+// summing up to kScanOneItems consecutive counts, then re-reading them (from
+// L1) to write their offsets.  Up to 4 items a thread this beats the three
+// launches (the 2,500 tiles of one 800x800 view); at 20 (8 such views) the
+// threads' serial loads make it slower than them.
+constexpr int kScanOneThreads = 1024;
+constexpr int kScanOneItems = 4;
+constexpr int64_t kScanOneMax = (int64_t)kScanOneThreads * kScanOneItems;
+
+// out[i] = sum of in[0..i) for i < n and out[n] = the total (n <= kScanOneMax);
+// zero[0..n) is cleared on the way (a per-item cursor of the next pass; may
+// be null).
+static __global__ void __launch_bounds__(kScanOneThreads) scan_one_cta_kernel(const int* __restrict__ in, int n,
+                                                                              int64_t* __restrict__ out,
+                                                                              int* __restrict__ zero) {
+    __shared__ int64_t warp_tot[kScanOneThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int per = (n + kScanOneThreads - 1) / kScanOneThreads;  // <= kScanOneItems
+    const int i0 = threadIdx.x * per, i1 = min(i0 + per, n);
+    int64_t s = 0;
+    for (int i = i0; i < i1; ++i) s += in[i];
+    int64_t x = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_tot[warp] = x;
+    __syncthreads();
+    int64_t base = 0, total = 0;
+#pragma unroll 8
+    for (int w = 0; w < kScanOneThreads / 32; ++w) {
+        const int64_t t = warp_tot[w];
+        if (w < warp) base += t;
+        total += t;
+    }
+    int64_t run = base + x - s;
+    for (int i = i0; i < i1; ++i) {
+        out[i] = run;
+        run += in[i];
+        if (zero) zero[i] = 0;
+    }
+    if (threadIdx.x == 0) out[n] = total;
 }
 
 }  // namespace dsb

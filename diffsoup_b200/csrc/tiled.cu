@@ -954,17 +954,23 @@ int ds_tiles_bin(int B, const ds_view_desc* views, int num_tiles, int V, const f
     if (rc) return rc;
     cudaStream_t st = (cudaStream_t)stream;
     TileWs w = carve(workspace, B, T, num_tiles, list_capacity, nullptr);
+    // up to kScanOneMax tiles, one launch scans the counts, writes the total and clears the fill cursors
+    const bool one_cta = num_tiles <= kScanOneMax;
     DS_CUDA(cudaMemsetAsync(w.counts, 0, (size_t)num_tiles * sizeof(int), st));
-    DS_CUDA(cudaMemsetAsync(w.cursor, 0, (size_t)num_tiles * sizeof(int), st));
+    if (!one_cta) DS_CUDA(cudaMemsetAsync(w.cursor, 0, (size_t)num_tiles * sizeof(int), st));
     const int64_t n = (int64_t)B * T;
     if (n > 0)
         bin_setup_kernel<<<blocks_for(n), kThreads, 0, st>>>(B, views, V, pos, T, tri, w.boxes, w.verts, w.ndc,
                                                               w.edges, w.counts);
-    int64_t* total_dev = nullptr;
-    rc = device_scan<int, int64_t>(w.counts, num_tiles, w.offsets, false, w.scan, st, &total_dev);
-    if (rc) return rc;
-    // offsets[num_tiles] = total number of entries
-    DS_CUDA(cudaMemcpyAsync(w.offsets + num_tiles, total_dev, sizeof(int64_t), cudaMemcpyDeviceToDevice, st));
+    if (one_cta) {
+        scan_one_cta_kernel<<<1, kScanOneThreads, 0, st>>>(w.counts, num_tiles, w.offsets, w.cursor);
+    } else {
+        int64_t* total_dev = nullptr;
+        rc = device_scan<int, int64_t>(w.counts, num_tiles, w.offsets, false, w.scan, st, &total_dev);
+        if (rc) return rc;
+        // offsets[num_tiles] = total number of entries
+        DS_CUDA(cudaMemcpyAsync(w.offsets + num_tiles, total_dev, sizeof(int64_t), cudaMemcpyDeviceToDevice, st));
+    }
     if (n > 0)
         bin_fill_kernel<<<blocks_for(n), kThreads, 0, st>>>(B, views, T, w.boxes, w.verts, w.ndc, w.offsets, w.cursor,
                                                             w.fill,
