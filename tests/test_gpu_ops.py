@@ -158,6 +158,27 @@ def test_tiled_rasterizer_matches_oracle(config, seed, kw):
     assert (bits(rs) == bits(ref_s)).all()
 
 
+@pytest.mark.parametrize("hw", [
+    [(1000, 1000)],            # 3,969 tiles: scanned in one launch, the last busy thread holds one count
+    [(1024, 1024)],            # 4,096 tiles: one launch, 4 counts in every thread
+    [(1024, 1024), (16, 16)],  # 4,097 tiles: the three-launch scan
+])
+def test_tile_count_scans_bin_alike(hw):
+    """Both scans of the per-tile counts (one launch up to 4,096 tiles, three
+    launches above) give the tile lists of view 0 its oracle ID buffer."""
+    sc, lvl, alpha = _scene_inputs(1, 4)
+    pos = np.repeat(sc.clip_positions()[:1], len(hw), axis=0)
+    bins = tiles.bin_views(T_(pos), T_(sc.tri), hw, reuse=False)
+    assert bins.num_tiles == sum(((h + 15) // 16) * ((w + 15) // 16) for h, w in hw)
+    rast = torch.empty(bins.num_pixels, 4, device=DEV)
+    tiles.rasterize(bins, lvl, T_(alpha), rast, thr_mode=0, thr_const=0.5)
+    H, W = hw[0]
+    ref, nf = cpu.rasterize_alpha(H, W, pos[:1], sc.tri, lvl, alpha, stochastic=False)
+    assert nf > 0
+    got = rast.cpu().numpy()[: H * W].reshape(1, H, W, 4)
+    assert (bits(got) == bits(ref)).all()
+
+
 def test_tiled_rasterizer_uneven_views_and_overflow():
     sc, lvl, alpha = _scene_inputs(3, 1, num_tris=3000, num_views=4)
     hw = [(v.height, v.width) for v in sc.views]
