@@ -118,25 +118,6 @@ __device__ __forceinline__ void add_mid_contrib(float mx, float my, const float4
     a.any = true;
 }
 
-// The contribution of add_mid_contrib given the point's barycentrics and
-// interpolated clip z, w.
-__device__ __forceinline__ void add_contrib_at(float b0, float b1, float cz, float cw, float mx, float my, float gx,
-                                               float gy, float gz, bool use_z, EdgeAccum& a) {
-    const float b2 = 1.f - b0 - b1;
-    const float cx = mx * cw, cy = my * cw;
-    const float iw = 1.f / cw, iw2 = iw * iw;
-    const float gsum = use_z ? gx * cx + gy * cy + gz * cz : gx * cx + gy * cy;
-    const float bb[3] = {b0, b1, b2};
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        a.g[k * 4 + 0] += bb[k] * gx * iw;
-        a.g[k * 4 + 1] += bb[k] * gy * iw;
-        if (use_z) a.g[k * 4 + 2] += bb[k] * gz * iw;
-        a.g[k * 4 + 3] += -bb[k] * gsum * iw2;
-    }
-    a.any = true;
-}
-
 // Edge-gradient estimator of one pixel (rasterize.cu:663-892).  Pixel
 // buffers are addressed as base + y*W + x with `base` the view's first pixel;
 // posb holds the view's clip positions.  Returns the pixel's triangle (or -1)
